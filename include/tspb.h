@@ -1,0 +1,148 @@
+/*
+ * tspb.h - C ABI of libtspb.so, the B200 (sm_100a) kernels behind the memetic-GA
+ * hot path of lucasgaldinos/tsp_gpu_clean.
+ *
+ * Conventions (every entry point):
+ *   - plain device pointers and sizes; no framework types;
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream);
+ *   - work is enqueued asynchronously on `stream`; the return value is a host-side
+ *     status (TSPB_OK or a TSPB_ERR_* code) covering argument checks and the launch;
+ *   - per-item device-side failures (a tour that is not a permutation, an index out
+ *     of range) are written to the optional `status` device array, one int32 per
+ *     item, 0 meaning success; the item is then left unchanged;
+ *   - node ids are int32 in [0, dim); distance matrices are int32, row-major with
+ *     `dist_stride` elements per row; coordinates are float64 (x, y) pairs.
+ *
+ * Reference file:line citations are relative to the reference project root.
+ */
+#ifndef TSPB_H
+#define TSPB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TSPB_OK 0
+#define TSPB_ERR_ARG 1            /* bad size, null pointer, unknown mode */
+#define TSPB_ERR_CUDA 2           /* a CUDA launch or query failed */
+#define TSPB_ERR_NOT_PERMUTATION 3 /* an input tour repeats or misses a node */
+#define TSPB_ERR_RANGE 4          /* a value exceeds what the kernel's integer math covers */
+#define TSPB_ERR_UNSUPPORTED 5    /* configuration outside the kernels' scope */
+#define TSPB_ERR_WORKSPACE 6      /* caller workspace smaller than tspb_*_workspace_bytes */
+#define TSPB_ERR_BUDGET 7         /* a tour hit the device watchdog before converging */
+
+#define TSPB_MODE_BEST 0       /* steepest move per pass; also the "batch" mode */
+#define TSPB_MODE_FIRST 1      /* first improving move in scan order */
+#define TSPB_MODE_MULTI_MOVE 2 /* every disjoint improving move, steepest first */
+
+/* Library version and build facts. */
+int tspb_version(void);
+
+/* Human-readable text for a TSPB_* status code (static storage). */
+const char* tspb_status_string(int status);
+
+/* Bytes of global scratch `tspb_two_opt` needs for this shape (0 when none). */
+size_t tspb_two_opt_workspace_bytes(int32_t num_tours, int32_t n, int32_t k, int32_t mode, int32_t block_threads);
+
+/*
+ * Batched 2-opt local search, one CTA per tour, in place on `tours` (num_tours x n).
+ * Replaces: LocalSearchCPUTourTwoOpt._refine / improve_batch
+ *   (src/algorithms/strategies/local_search/two_opt.py:565-628) with the pair order of
+ *   _pair_blocks (:303-367), the gains of _pair_deltas (:204-261) and the acceptance
+ *   rules _step_best (:386-440), _step_first (:442-489), _step_multi_move (:491-563);
+ *   and the GPU launch loop of LocalSearchGPUTourTwoOpt._improve_grid (:831-899).
+ * Cyclic TSP topology. `cand` (n x k, k-NN table) selects candidate mode; NULL selects
+ * the exhaustive scan. `cand_dist` (n x k, optional) holds d(a, cand[a][r]).
+ * Distances come from `dist` when non-NULL, else are rebuilt from `coords` in FP64
+ * with TSPLIB EUC_2D rounding. `max_iterations` bounds the passes per tour.
+ * `stats` (optional, num_tours x 4 int64): passes, pairs evaluated by the reference
+ * scan (oracle-equivalent deltas), reversals applied, gains computed by the kernel.
+ */
+int tspb_two_opt(int32_t* tours, int32_t num_tours, int32_t n,
+                 const int32_t* dist, int64_t dist_stride, const double* coords,
+                 const int32_t* cand, const int32_t* cand_dist, int32_t k,
+                 int32_t mode, int64_t max_iterations, int32_t block_threads,
+                 int64_t* stats, int32_t* status,
+                 void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * cand_dist[a*k + r] = d(a, cand[a*k + r]) for the n x k table (entries outside [0, n)
+ * give 0). Replaces the D[a, c] gathers of _pair_deltas (two_opt.py:242) with a table
+ * built once per instance.
+ */
+int tspb_candidate_distances(const int32_t* cand, int32_t n, int32_t k,
+                             const int32_t* dist, int64_t dist_stride, const double* coords,
+                             int32_t* cand_dist, void* stream);
+
+/*
+ * Closed-tour cost per row (sum of n edges incl. the closing edge when return_to_depot),
+ * written as float64. Replaces evaluate_tour_cpu
+ *   (src/algorithms/strategies/evaluation/tour_cost.py:17-29) and tour_cost_kernel
+ *   (src/algorithms/strategies/evaluation/kernels/tour_cost.cu:21-63).
+ */
+int tspb_tour_cost(const int32_t* tours, int32_t num_tours, int32_t n,
+                   const int32_t* dist, int64_t dist_stride, const double* coords,
+                   int32_t return_to_depot, double* costs, void* stream);
+
+/*
+ * Tournament selection: winners[p] = first argmin of fitness over cand[p*k .. p*k+k).
+ * Replaces SelectionCPUTournament.select_batch
+ *   (src/algorithms/strategies/selection/tournament_selection.py:98-128) and
+ *   tournament_selection_kernel (.../selection/kernels/tournament_selection.cu:11-39).
+ */
+int tspb_tournament(const double* fitness, int32_t pop_size, const int32_t* cand,
+                    int32_t num_parents, int32_t k, int32_t* winners, void* stream);
+
+/* out[r, :] = src[rows[r], :] for r < num_rows (row gather of an int32 matrix). */
+int tspb_gather_rows(const int32_t* src, int32_t src_rows, int32_t n, const int32_t* rows,
+                     int32_t num_rows, int32_t* out, void* stream);
+
+/*
+ * PMX crossover of pairs (2q, 2q+1) sharing cuts (first[q], second[q]); the odd tail
+ * row is copied. Open permutations (bounds [0, n)). Replaces
+ *   CrossoverCPUPermPartiallyMapped._apply_pmx / crossover_batch
+ *   (src/algorithms/strategies/crossover/pmx_crossover.py:49-105, 128-171) and
+ *   pmx_crossover_kernel (.../crossover/kernels/pmx_crossover.cu:19-154).
+ */
+int tspb_pmx(const int32_t* parents, int32_t num_routes, int32_t n,
+             const int32_t* cut_first, const int32_t* cut_second,
+             int32_t* children, int32_t* status, void* stream);
+
+/*
+ * Inversion mutation in place: row r reversed over [min(p1,p2), max(p1,p2)] when
+ * u[r] < rate. Replaces MutationCPUPermInversion.mutate_batch
+ *   (src/algorithms/strategies/mutation/inversion_mutation.py:65-99) and
+ *   inversion_mutation_kernel (.../mutation/kernels/inversion_mutation.cu:11-44).
+ */
+int tspb_inversion(int32_t* routes, int32_t num_routes, int32_t n, const double* u,
+                   double rate, const int32_t* pos1, const int32_t* pos2, void* stream);
+
+/*
+ * (mu + lambda) survival: order[0..keep) = indices of the `keep` smallest values of
+ * fitness[0..count) by (fitness, index), i.e. a stable ascending sort. Replaces
+ * GeneticAlgorithm._select_survivors_assessed for feasible tours
+ *   (src/algorithms/metaheuristics/genetic_algorithm.py:618-706, lexsort :682-689).
+ */
+int tspb_stable_rank(const double* fitness, int32_t count, int32_t keep, int32_t* order, void* stream);
+
+/*
+ * Permutation check: bad[r] = 0 when row r is a permutation of 0..n-1, else 1.
+ */
+int tspb_validate_perm(const int32_t* tours, int32_t num_tours, int32_t n, int32_t* bad, void* stream);
+
+/*
+ * Dense EUC_2D matrix from FP64 coordinates: nint(sqrt(dx*dx + dy*dy)) with separate
+ * IEEE multiplies and add (no FMA), zero diagonal. Replaces compute_distance_matrix
+ *   (src/distances/matrix.py:84-86, 214-273) and gpu_euc_2d
+ *   (src/distances/kernels/pairwise_device.cuh:58-60).
+ */
+int tspb_euc2d_matrix(const double* coords, int32_t n, int32_t* dist, int64_t dist_stride, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TSPB_H */

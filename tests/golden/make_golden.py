@@ -1,0 +1,303 @@
+"""Generate the golden fixtures by running the reference's own CPU strategies.
+
+Run in a container that holds the reference checkout:
+
+    python tests/golden/make_golden.py /path/to/tsp_gpu_clean
+
+The reference imports `converter.utils.cost` from its git-only dependency
+`routing-data` (v0.3.0), which is not installable offline; the hot path never
+calls it, so this script writes a throwaway stand-in package into a temporary
+directory first. Nothing from the reference is copied: the fixtures hold only
+inputs and the outputs the reference produced for them.
+
+Outputs (NumPy `.npz`, committed next to this script):
+- `two_opt_small.npz`  2-opt best/first/multi_move, exhaustive and k-NN, n = 4..150,
+                       plus integer-lattice tie cases and duplicate-candidate tables;
+- `two_opt_c2.npz`     four tours of the 1000-city, 20-cluster instance refined to a
+                       local optimum in best and first mode, with pass and pair counts;
+- `ops.npz`            tournament selection, PMX, inversion, tour cost, candidate
+                       lists and the EUC_2D matrix on seeded inputs;
+- `ga.npz`             full GA runs (the 100-city memetic run for 50 generations, a
+                       3-generation 2000-city/512-tour run with 64 elites, and small
+                       runs for every local-search stage), recorded per generation.
+"""
+
+from __future__ import annotations
+
+import hashlib
+import os
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+
+_STUB = '''
+def nint(x):
+    return int(x + 0.5)
+def _unavailable(*args, **kwargs):
+    raise NotImplementedError("routing-data is not installed")
+att = ceil_2d = euclidean_2d = euclidean_3d = manhattan_2d = manhattan_3d = _unavailable
+maximum_2d = maximum_3d = xray1 = _unavailable
+'''
+
+
+def _setup(ref_root: str) -> None:
+  tmp = tempfile.mkdtemp(prefix="golden_stub_")
+  pkg = os.path.join(tmp, "converter", "utils")
+  os.makedirs(pkg)
+  open(os.path.join(tmp, "converter", "__init__.py"), "w").close()
+  open(os.path.join(pkg, "__init__.py"), "w").close()
+  with open(os.path.join(pkg, "cost.py"), "w") as fh:
+    fh.write(_STUB)
+  sys.path.insert(0, tmp)
+  sys.path.insert(0, os.path.join(ref_root, "src"))
+  sys.path.insert(0, REPO)
+
+
+def digest(a: np.ndarray) -> str:
+  return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def lattice_matrix(n: int) -> np.ndarray:
+  side = int(np.ceil(np.sqrt(n)))
+  coords = np.array([[x, y] for x in range(side) for y in range(side)][:n], dtype=float)
+  diff = coords[:, None, :] - coords[None, :, :]
+  d = np.floor(np.sqrt((diff**2).sum(axis=2)) + 0.5).astype(np.int32)
+  np.fill_diagonal(d, 0)
+  return d
+
+
+def main(ref_root: str) -> None:
+  _setup(ref_root)
+  from algorithms import GeneticAlgorithm
+  from algorithms.pipeline_steps import EliteOnlyLocalSearchStep, PeriodicLocalSearchStep, PostInitLocalSearchStep
+  from algorithms.strategies import (
+    CrossoverCPUPermPartiallyMapped,
+    EvaluationCPUCost,
+    InitializationCPUTourNearestNeighbor,
+    LocalSearchCPUTourTwoOpt,
+    MutationCPUPermInversion,
+    SelectionCPUTournament,
+  )
+  from data_models.problem import Problem
+  from protocols.problem_context import ProblemContext
+
+  from tsp_gpu_clean_b200 import instances
+
+  def coord_problem(coords, name="synthetic"):
+    return Problem(name=name, dimension=len(coords), problem_type="TSP", edge_type="EUC_2D",
+                   coordinates=np.asarray(coords, dtype=np.float64), distances=None)
+
+  def matrix_problem(d, name="explicit"):
+    return Problem(name=name, dimension=d.shape[0], problem_type="TSP", edge_type="EXPLICIT",
+                   coordinates=None, distances=d)
+
+  # ------------------------------------------------------------------ 2-opt small
+  out: dict[str, np.ndarray] = {}
+  case = 0
+  t0 = time.time()
+  for n in (4, 5, 6, 8, 10, 17, 40, 100, 150):
+    coords = instances.uniform_instance(n, 1000 + n)
+    prob = coord_problem(coords)
+    for k in (None, 3, 20):
+      for mode in ("best", "first", "multi_move"):
+        for iters in (1, 3, 10, 100000):
+          ctx = ProblemContext(prob, xp=np, seed=0)
+          tours = instances.random_tours(n, 4, 7 * n + (k or 0) + 31 * iters % 97)
+          ls = LocalSearchCPUTourTwoOpt(max_iterations=iters, mode=mode, candidate_k=k)
+          res = ls.improve_batch(tours.copy(), ctx)
+          key = f"c{case}"
+          out[key + "_coords"] = coords
+          out[key + "_meta"] = np.array([n, -1 if k is None else k, ("best", "first", "multi_move").index(mode), iters])
+          out[key + "_in"] = tours
+          out[key + "_out"] = np.asarray(res, dtype=np.int32)
+          if k is not None:
+            out[key + "_cand"] = ctx.get_cpu_candidate_list(k)
+          case += 1
+  # integer lattice: many tied gains (explicit matrices, candidate tables recorded)
+  for n in (9, 16, 25, 36):
+    d = lattice_matrix(n)
+    prob = matrix_problem(d)
+    for k in (None, 3):
+      for mode in ("best", "first", "multi_move"):
+        ctx = ProblemContext(prob, xp=np, seed=0)
+        tours = instances.random_tours(n, 4, 31 * n + (k or 0))
+        res = LocalSearchCPUTourTwoOpt(max_iterations=10, mode=mode, candidate_k=k).improve_batch(tours.copy(), ctx)
+        key = f"c{case}"
+        out[key + "_dist"] = d
+        out[key + "_meta"] = np.array([n, -1 if k is None else k, ("best", "first", "multi_move").index(mode), 10])
+        out[key + "_in"] = tours
+        out[key + "_out"] = np.asarray(res, dtype=np.int32)
+        if k is not None:
+          out[key + "_cand"] = ctx.get_cpu_candidate_list(k)
+        case += 1
+  # user-supplied candidate tables with repeated neighbours (duplicates are kept)
+  for n in (12, 40):
+    coords = instances.uniform_instance(n, 555 + n)
+    prob = coord_problem(coords)
+    base = ProblemContext(prob, xp=np, seed=0).get_cpu_candidate_list(6)
+    dup = np.concatenate([base[:, :3], base[:, :3]], axis=1).astype(np.int32)
+    for mode in ("best", "first", "multi_move"):
+      ctx = ProblemContext(prob, xp=np, seed=0, candidate_cache={6: dup})
+      tours = instances.random_tours(n, 4, 99 + n)
+      res = LocalSearchCPUTourTwoOpt(max_iterations=100000, mode=mode, candidate_k=6).improve_batch(tours.copy(), ctx)
+      key = f"c{case}"
+      out[key + "_coords"] = coords
+      out[key + "_meta"] = np.array([n, 6, ("best", "first", "multi_move").index(mode), 100000])
+      out[key + "_in"] = tours
+      out[key + "_out"] = np.asarray(res, dtype=np.int32)
+      out[key + "_cand"] = dup
+      case += 1
+  out["num_cases"] = np.array(case)
+  np.savez_compressed(os.path.join(HERE, "two_opt_small.npz"), **out)
+  print(f"two_opt_small: {case} cases in {time.time() - t0:.1f}s")
+
+  # ------------------------------------------------------------------ 2-opt C2 subset
+  t0 = time.time()
+  counts = {"pairs": 0, "passes": 0}
+  orig_blocks = LocalSearchCPUTourTwoOpt._pair_blocks
+
+  def counting_blocks(self, *a, **kw):
+    counts["passes"] += 1
+    for i_idx, j_idx in orig_blocks(self, *a, **kw):
+      counts["pairs"] += int(i_idx.size)
+      yield i_idx, j_idx
+
+  LocalSearchCPUTourTwoOpt._pair_blocks = counting_blocks
+  coords, tours = instances.c2_workload(tours=4)
+  prob = coord_problem(coords, "c2")
+  c2: dict[str, np.ndarray] = {"coords": coords, "tours_in": tours}
+  for mode in ("best", "first"):
+    outs, stats = [], []
+    for t in range(len(tours)):
+      ctx = ProblemContext(prob, xp=np, seed=0)
+      counts["pairs"] = counts["passes"] = 0
+      r = LocalSearchCPUTourTwoOpt(max_iterations=10**9, mode=mode, candidate_k=20).improve_batch(tours[t : t + 1].copy(), ctx)
+      outs.append(np.asarray(r)[0])
+      stats.append((counts["passes"], counts["pairs"]))
+    c2[f"{mode}_out"] = np.stack(outs)
+    c2[f"{mode}_stats"] = np.array(stats, dtype=np.int64)
+  c2["cand20"] = ProblemContext(prob, xp=np, seed=0).get_cpu_candidate_list(20)
+  LocalSearchCPUTourTwoOpt._pair_blocks = orig_blocks
+  np.savez_compressed(os.path.join(HERE, "two_opt_c2.npz"), **c2)
+  print(f"two_opt_c2 in {time.time() - t0:.1f}s: {c2['best_stats'].tolist()} {c2['first_stats'].tolist()}")
+
+  # ------------------------------------------------------------------ operators
+  t0 = time.time()
+  ops: dict[str, np.ndarray] = {}
+  for tag, n, pop_size, rate in (("a", 52, 129, 0.05), ("b", 100, 128, 0.5), ("c", 1000, 64, 1.0), ("d", 7, 10, 0.0)):
+    coords = instances.uniform_instance(n, 4242 + n)
+    prob = coord_problem(coords)
+    ctx = ProblemContext(prob, xp=np, seed=123 + n)
+    pop = instances.random_tours(n, pop_size, 17 + n)
+    ev = EvaluationCPUCost()
+    fit = np.asarray(ev.assess_batch(pop, ctx).objectives)
+    sel = SelectionCPUTournament(k=5, seed=1).select_batch(pop, fit, pop_size, ctx)
+    pmx = CrossoverCPUPermPartiallyMapped(seed=1).crossover_batch(sel, ctx)
+    inv = MutationCPUPermInversion(seed=1).mutate_batch(pmx, rate, ctx)
+    ops[f"{tag}_coords"] = coords
+    ops[f"{tag}_meta"] = np.array([n, pop_size, 123 + n])
+    ops[f"{tag}_rate"] = np.array(rate)
+    ops[f"{tag}_pop"] = pop
+    ops[f"{tag}_fit"] = fit
+    ops[f"{tag}_sel"] = np.asarray(sel)
+    ops[f"{tag}_pmx"] = np.asarray(pmx)
+    ops[f"{tag}_inv"] = np.asarray(inv)
+    ops[f"{tag}_rng_state"] = np.array([ctx.rng.bit_generator.state["state"]["state"] % (1 << 63)], dtype=np.int64)
+  # EUC_2D matrix and k-NN tables, including exact .5 distances
+  coords = instances.uniform_instance(300, 77)
+  coords[:4] = [[0.0, 0.0], [0.5, 0.0], [1.5, 2.0], [3.0, 4.0]]
+  prob = coord_problem(coords)
+  ctx = ProblemContext(prob, xp=np, seed=0)
+  ops["dist_coords"] = coords
+  ops["dist_matrix"] = ctx.get_cpu_distances()
+  ops["dist_cand5"] = ctx.get_cpu_candidate_list(5)
+  ops["dist_cand20"] = ctx.get_cpu_candidate_list(20)
+  big = instances.uniform_instance(5000, 78)
+  ops["big_coords"] = big
+  ops["big_digest"] = np.frombuffer(bytes.fromhex(digest(ProblemContext(coord_problem(big), xp=np, seed=0).get_cpu_distances())), dtype=np.uint8)
+  np.savez_compressed(os.path.join(HERE, "ops.npz"), **ops)
+  print(f"ops in {time.time() - t0:.1f}s")
+
+  # ------------------------------------------------------------------ GA runs
+  class Recorder:
+    stage_anchor = "post_survival"
+
+    def __init__(self):
+      self.digests: list[str] = []
+      self.fitness: list[np.ndarray] = []
+
+    def run(self, state, timer):
+      self.digests.append(digest(np.asarray(state.population, dtype=np.int32)))
+      self.fitness.append(np.asarray(state.fitness, dtype=np.float64).copy())
+
+  ga_out: dict[str, np.ndarray] = {}
+
+  def run_ga(tag, coords, pop_size, gens, elite, stage="none", post_init=True, periodic=None, ls_iters=10,
+             mutation_rate=0.05, patience=10**9, seed=42):
+    t = time.time()
+    prob = coord_problem(coords)
+    ctx = ProblemContext(prob, xp=np, seed=seed)
+    ls = LocalSearchCPUTourTwoOpt(mode="best", max_iterations=ls_iters, candidate_k=20)
+    ev = EvaluationCPUCost()
+    rec = Recorder()
+    steps = []
+    if post_init:
+      steps.append(PostInitLocalSearchStep(local_search=ls, evaluation=ev))
+    if periodic is not None:
+      steps.append(PeriodicLocalSearchStep(local_search=ls, interval=periodic[0], target=periodic[1],
+                                           re_evaluate=ev if periodic[1] == "population" else None))
+    if elite:
+      steps.append(EliteOnlyLocalSearchStep(local_search=ls, evaluation=ev, elite_count=elite))
+    steps.append(rec)
+    init = InitializationCPUTourNearestNeighbor(k=5, seed=42)
+    captured = {}
+    orig_init = init.initialize
+
+    def cap_init(*a, **kw):
+      res = orig_init(*a, **kw)
+      captured["pop"] = np.asarray(res).copy()
+      return res
+
+    init.initialize = cap_init
+    ga = GeneticAlgorithm(population_size=pop_size, mutation_rate=mutation_rate, seed=42, initialization=init,
+                          selection=SelectionCPUTournament(k=5, seed=42), crossover=CrossoverCPUPermPartiallyMapped(seed=42),
+                          mutation=MutationCPUPermInversion(seed=42), local_search=ls, evaluation=ev,
+                          local_search_stage=stage, pipeline=steps)
+    best, stats = ga.evolve(context=ctx, customers=list(range(len(coords))), max_generations=gens, patience=patience)
+    ga_out[f"{tag}_coords"] = coords
+    ga_out[f"{tag}_meta"] = np.array([pop_size, gens, elite or 0, int(post_init), ls_iters, seed,
+                                      -1 if periodic is None else periodic[0],
+                                      -1 if periodic is None else (0 if periodic[1] == "offspring" else 1)])
+    ga_out[f"{tag}_stage"] = np.array(stage)
+    ga_out[f"{tag}_rate"] = np.array(mutation_rate)
+    if captured["pop"].size <= 200_000:
+      ga_out[f"{tag}_init"] = captured["pop"]
+    ga_out[f"{tag}_init_digest"] = np.array(digest(captured["pop"].astype(np.int32)))
+    ga_out[f"{tag}_best"] = np.asarray(best, dtype=np.int32)
+    ga_out[f"{tag}_history"] = np.asarray(stats["convergence_history"], dtype=np.float64)
+    ga_out[f"{tag}_gens"] = np.array(stats["generations_completed"])
+    ga_out[f"{tag}_digests"] = np.array(rec.digests)
+    ga_out[f"{tag}_fitness"] = np.stack(rec.fitness) if rec.fitness else np.zeros((0, pop_size))
+    ga_out[f"{tag}_rng"] = np.array([ctx.rng.bit_generator.state["state"]["state"] % (1 << 63)], dtype=np.int64)
+    print(f"ga {tag}: {time.time() - t:.1f}s best={stats['best_fitness']} gens={stats['generations_completed']}")
+
+  run_ga("c1", instances.uniform_instance(100, 42), 128, 50, 16)
+  run_ga("c1default", instances.uniform_instance(100, 42), 128, 50, 16, patience=None)
+  run_ga("pm", instances.uniform_instance(52, 5), 32, 5, 0, stage="post_mutation", post_init=False, ls_iters=3)
+  run_ga("pc", instances.uniform_instance(52, 6), 33, 5, 0, stage="post_crossover", post_init=False, ls_iters=3)
+  run_ga("pe", instances.uniform_instance(52, 7), 32, 5, 4, stage="post_evaluation", post_init=True, ls_iters=3)
+  run_ga("px", instances.uniform_instance(52, 8), 32, 6, 0, stage="post_evolution", post_init=False, ls_iters=5)
+  run_ga("pp", instances.uniform_instance(60, 9), 32, 6, 0, periodic=(2, "population"), post_init=False)
+  run_ga("po", instances.uniform_instance(60, 10), 32, 6, 0, periodic=(3, "offspring"), post_init=False)
+  run_ga("c3", instances.uniform_instance(2000, 2000), 512, 3, 64, post_init=False)
+  ga_out["tags"] = np.array(["c1", "c1default", "pm", "pc", "pe", "px", "pp", "po", "c3"])
+  np.savez_compressed(os.path.join(HERE, "ga.npz"), **ga_out)
+
+
+if __name__ == "__main__":
+  main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

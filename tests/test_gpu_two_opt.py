@@ -1,0 +1,180 @@
+"""2-opt on the B200 through the C ABI, bit-exact against the oracle and the golden vectors.
+
+Covers every reference 2-opt parity case (`test_unit_two_opt_vectorized_scan.py`,
+`test_unit_two_opt_boundaries.py` of the reference): modes best/first/multi_move/batch,
+exhaustive and k-NN neighbourhoods, tie-heavy integer lattices, duplicated candidates,
+short tours, zero iterations, untouched inputs, and tours run to a local optimum on
+the 1000-city clustered instance with the oracle's pass and pair counts.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import iter_two_opt_cases
+from oracle import distances as odist
+from oracle import two_opt as otwo
+from tsp_gpu_clean_b200 import instances
+
+pytestmark = pytest.mark.gpu
+
+
+class CoordDist:
+  """EUC_2D lookups `D[a, c]` computed on demand (no n x n matrix on the host)."""
+
+  def __init__(self, coords):
+    self.coords = np.asarray(coords, dtype=np.float64)
+    self.shape = (len(coords), len(coords))
+
+  def __getitem__(self, idx):
+    a, c = idx
+    diff = self.coords[np.asarray(a)] - self.coords[np.asarray(c)]
+    return (np.sqrt(diff[..., 0] * diff[..., 0] + diff[..., 1] * diff[..., 1]) + 0.5).astype(np.int64).astype(np.int32)
+
+
+@pytest.fixture(scope="module")
+def b200():
+  import torch
+
+  if not torch.cuda.is_available():
+    pytest.skip("no CUDA device")
+  from tsp_gpu_clean_b200.build import build_library
+
+  build_library()
+  from tsp_gpu_clean_b200.problem import Problem, ProblemContext
+  from tsp_gpu_clean_b200.strategies.local_search import LocalSearchB200TourTwoOpt
+
+  return Problem, ProblemContext, LocalSearchB200TourTwoOpt
+
+
+def _ctx(b200, D=None, coords=None, cand=None, k=None):
+  Problem, ProblemContext, _ = b200
+  prob = Problem.from_coordinates(coords) if coords is not None else Problem.from_matrix(D)
+  cache = {k: cand} if cand is not None else None
+  return ProblemContext(prob, seed=0, candidate_cache=cache)
+
+
+def test_golden_small_cases(b200, golden):
+  data = golden("two_opt_small.npz")
+  LS = b200[2]
+  for c, n, k, mode, iters, D, cand, tin, tout in iter_two_opt_cases(data):
+    coords = data.get(f"c{c}_coords")
+    ctx = _ctx(b200, D=D if coords is None else None, coords=coords, cand=cand, k=k)
+    for m in ([mode, "batch"] if mode == "best" else [mode]):
+      before = tin.copy()
+      got = LS(max_iterations=iters, mode=m, candidate_k=k).improve_batch(tin, ctx)
+      assert np.array_equal(tin, before), "input mutated"
+      assert np.array_equal(got, tout), f"case {c}: n={n} k={k} mode={m} iters={iters}"
+
+
+@pytest.mark.parametrize("mode", ["best", "first"])
+def test_golden_c2_local_optimum_with_counts(b200, golden, mode):
+  data = golden("two_opt_c2.npz")
+  ctx = _ctx(b200, coords=data["coords"], cand=data["cand20"], k=20)
+  ls = b200[2](max_iterations=10**9, mode=mode, candidate_k=20)
+  got = ls.improve_batch(data["tours_in"], ctx)
+  assert np.array_equal(got, data[f"{mode}_out"])
+  assert np.array_equal(ls.last_stats[:, 0], data[f"{mode}_stats"][:, 0]), "passes"
+  assert np.array_equal(ls.last_stats[:, 1], data[f"{mode}_stats"][:, 1]), "oracle-equivalent pairs"
+
+
+@pytest.mark.parametrize("mode", ["best", "first", "multi_move"])
+@pytest.mark.parametrize("iters", [1, 10, 10**9])
+def test_random_tours_vs_oracle(b200, mode, iters):
+  coords = instances.clustered_instance(300, 10, 30.0, 11)
+  tours = instances.random_tours(300, 12, 12)
+  ctx = _ctx(b200, coords=coords)
+  D = odist.euc2d_matrix(coords)
+  cand = ctx.get_cpu_candidate_list(20)
+  ls = b200[2](max_iterations=iters, mode=mode, candidate_k=20)
+  got = ls.improve_batch(tours, ctx)
+  want, st = otwo.improve_batch(tours, D, cand, mode, iters)
+  assert np.array_equal(got, want)
+  assert np.array_equal(ls.last_stats[:, :3], st)
+
+
+@pytest.mark.parametrize("mode", ["best", "first", "multi_move"])
+def test_exhaustive_vs_oracle(b200, mode):
+  coords = instances.uniform_instance(120, 3)
+  tours = instances.random_tours(120, 6, 4)
+  ctx = _ctx(b200, coords=coords)
+  D = odist.euc2d_matrix(coords)
+  ls = b200[2](max_iterations=10**9, mode=mode, candidate_k=None)
+  got = ls.improve_batch(tours, ctx)
+  want, st = otwo.improve_batch(tours, D, None, mode, 10**9)
+  assert np.array_equal(got, want)
+  assert np.array_equal(ls.last_stats[:, :3], st)
+
+
+def test_exhaustive_first_pair_count_spans_cpu_blocks(b200):
+  # n = 800 has 318,801 pairs per scan: more than one 2^18 CPU block.
+  coords = instances.uniform_instance(800, 21)
+  tours = instances.random_tours(800, 2, 22)
+  ctx = _ctx(b200, coords=coords)
+  D = odist.euc2d_matrix(coords)
+  ls = b200[2](max_iterations=40, mode="first", candidate_k=None)
+  got = ls.improve_batch(tours, ctx)
+  want, st = otwo.improve_batch(tours, D, None, "first", 40)
+  assert np.array_equal(got, want)
+  assert np.array_equal(ls.last_stats[:, :3], st)
+
+
+@pytest.mark.parametrize("mode", ["best", "first", "multi_move"])
+def test_fp64_rebuilt_distances_match_matrix(b200, mode):
+  coords = instances.uniform_instance(500, 31)
+  tours = instances.random_tours(500, 8, 32)
+  ctx = _ctx(b200, coords=coords)
+  LS = b200[2]
+  a = LS(max_iterations=10**9, mode=mode, candidate_k=20).improve_batch(tours, ctx)
+  b = LS(max_iterations=10**9, mode=mode, candidate_k=20, max_matrix_dimension=100).improve_batch(tours, ctx)
+  assert np.array_equal(a, b)
+
+
+def test_large_tour_uses_workspace_arrays(b200):
+  # 20,000 cities: tour/pos/edge do not fit in shared memory and live in the workspace.
+  coords = instances.uniform_instance(20000, 41)
+  tours = instances.random_tours(20000, 2, 42)
+  ctx = _ctx(b200, coords=coords)
+  ls = b200[2](max_iterations=30, mode="best", candidate_k=8, max_matrix_dimension=1000)
+  got = ls.improve_batch(tours, ctx)
+  want, st = otwo.improve_batch(tours, CoordDist(coords), ctx.get_cpu_candidate_list(8), "best", 30)
+  assert np.array_equal(got, want)
+  assert np.array_equal(ls.last_stats[:, :3], st)
+
+
+def test_contracts(b200):
+  LS = b200[2]
+  coords = instances.uniform_instance(30, 1)
+  ctx = _ctx(b200, coords=coords)
+  t = instances.random_tours(30, 3, 2)
+  assert np.array_equal(LS(max_iterations=0).improve_batch(t, ctx), t)
+  short = np.array([[2, 0, 1], [0, 1, 2]], dtype=np.int32)
+  assert np.array_equal(LS(max_iterations=5).improve_batch(short, ctx), short)
+  one = LS(max_iterations=5, candidate_k=5).improve_batch(t[0], ctx)
+  assert one.shape == (30,)
+  with pytest.raises(ValueError):
+    LS(mode="naive")
+  with pytest.raises(ValueError):
+    LS(max_iterations=-1)
+  bad = t.copy()
+  bad[1, 3] = bad[1, 4]
+  from tsp_gpu_clean_b200.errors import NotPermutationError
+
+  with pytest.raises(NotPermutationError):
+    LS(max_iterations=5, candidate_k=5).improve_batch(bad, ctx)
+
+
+def test_device_resident_roundtrip(b200):
+  import torch
+
+  coords = instances.uniform_instance(200, 5)
+  tours = instances.random_tours(200, 8, 6)
+  ctx = _ctx(b200, coords=coords)
+  LS = b200[2]
+  host = LS(max_iterations=50, mode="best", candidate_k=20).improve_batch(tours, ctx)
+  dev_in = torch.from_numpy(tours).cuda()
+  dev = LS(max_iterations=50, mode="best", candidate_k=20).improve_batch(dev_in, ctx)
+  assert dev.is_cuda
+  assert np.array_equal(dev.cpu().numpy(), host)
+  assert np.array_equal(dev_in.cpu().numpy(), tours)

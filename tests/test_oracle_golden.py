@@ -1,0 +1,129 @@
+"""Pin the CPU oracle against golden vectors produced by the reference itself.
+
+The fixtures under `tests/golden/` were generated by `tests/golden/make_golden.py`,
+which runs the reference's CPU strategies. Every oracle function used as the
+checker of the CUDA path must reproduce them bit for bit.
+"""
+
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import iter_two_opt_cases
+from oracle import distances, ga, ga_ops, two_opt
+from tsp_gpu_clean_b200 import instances
+
+
+def test_two_opt_small_cases_match_reference(golden):
+  data = golden("two_opt_small.npz")
+  count = 0
+  for c, n, k, mode, iters, D, cand, tin, tout in iter_two_opt_cases(data):
+    cand_used = two_opt.resolve_candidates(cand, tin, n) if k is not None else None
+    got, _ = two_opt.improve_batch(tin, D, cand_used, mode, iters)
+    assert np.array_equal(got, tout), f"case {c}: n={n} k={k} mode={mode} iters={iters}"
+    count += 1
+  assert count == int(data["num_cases"])
+
+
+def test_candidate_tables_match_reference(golden):
+  data = golden("two_opt_small.npz")
+  for c, n, k, mode, iters, D, cand, tin, tout in iter_two_opt_cases(data):
+    if cand is None or f"c{c}_coords" not in data or cand.shape[1] != min(k, n - 1):
+      continue
+    if n >= 12 and k == 6:
+      continue  # hand-built duplicate tables
+    assert np.array_equal(distances.candidate_list(k, coords=data[f"c{c}_coords"]), cand), c
+
+
+@pytest.mark.parametrize("mode", ["best", "first"])
+def test_two_opt_c2_subset_matches_reference_with_counts(golden, mode):
+  data = golden("two_opt_c2.npz")
+  D = distances.euc2d_matrix(data["coords"])
+  cand = data["cand20"]
+  assert np.array_equal(distances.candidate_list(20, coords=data["coords"]), cand)
+  got, stats = two_opt.improve_batch(data["tours_in"][:1], D, cand, mode, 10**9)
+  assert np.array_equal(got, data[f"{mode}_out"][:1])
+  assert stats[0, 0] == data[f"{mode}_stats"][0, 0]  # passes
+  assert stats[0, 1] == data[f"{mode}_stats"][0, 1]  # pairs evaluated
+
+
+def test_c2_workload_generator_is_stable(golden):
+  data = golden("two_opt_c2.npz")
+  coords, tours = instances.c2_workload(tours=4)
+  assert np.array_equal(coords, data["coords"])
+  assert np.array_equal(tours, data["tours_in"])
+
+
+def test_distance_matrix_and_knn_match_reference(golden):
+  ops = golden("ops.npz")
+  D = distances.euc2d_matrix(ops["dist_coords"])
+  assert np.array_equal(D, ops["dist_matrix"])
+  assert D[0, 1] == 1 and D[1, 0] == 1  # sqrt(0.25)+0.5 == 1.0 exactly
+  assert np.array_equal(distances.candidate_list(5, coords=ops["dist_coords"]), ops["dist_cand5"])
+  assert np.array_equal(distances.candidate_list(20, distances=D), ops["dist_cand20"])
+  big = distances.euc2d_matrix(ops["big_coords"])
+  assert hashlib.sha256(big.tobytes()).digest() == ops["big_digest"].tobytes()
+
+
+@pytest.mark.parametrize("tag", ["a", "b", "c", "d"])
+def test_operators_match_reference(golden, tag):
+  ops = golden("ops.npz")
+  n, pop_size, seed = (int(v) for v in ops[f"{tag}_meta"])
+  rate = float(ops[f"{tag}_rate"])
+  D = distances.euc2d_matrix(ops[f"{tag}_coords"])
+  rng = np.random.default_rng(seed)
+  pop = ops[f"{tag}_pop"]
+  fit = ga_ops.tour_cost(pop, D)
+  assert np.array_equal(fit, ops[f"{tag}_fit"])
+  sel = ga_ops.tournament_select(rng, pop, fit, pop_size, 5)
+  assert np.array_equal(sel, ops[f"{tag}_sel"])
+  pmx = ga_ops.pmx_batch(rng, sel)
+  assert np.array_equal(pmx, ops[f"{tag}_pmx"])
+  inv = ga_ops.inversion_batch(rng, pmx, rate)
+  assert np.array_equal(inv, ops[f"{tag}_inv"])
+  assert rng.bit_generator.state["state"]["state"] % (1 << 63) == int(ops[f"{tag}_rng_state"][0])
+
+
+def _run_oracle_ga(g, tag, record=True):
+  coords = g[f"{tag}_coords"]
+  pop_size, gens, elite, post_init, ls_iters, seed, per_int, per_tgt = (int(v) for v in g[f"{tag}_meta"])
+  stage = str(g[f"{tag}_stage"])
+  D = distances.euc2d_matrix(coords)
+  cache = {}
+
+  def provider(k):
+    if k not in cache:
+      cache[k] = distances.candidate_list(k, coords=coords)
+    return cache[k]
+
+  cfg = ga.GAConfig(population_size=pop_size, mutation_rate=float(g[f"{tag}_rate"]), nn_k=5, tournament_k=5,
+                    local_search=ga.LocalSearchSpec("best", ls_iters, 20), local_search_stage=stage,
+                    post_init=bool(post_init), elite_count=elite or None,
+                    periodic=None if per_int < 0 else (per_int, "offspring" if per_tgt == 0 else "population"))
+  rng = np.random.default_rng(seed)
+  patience = None if tag == "c1default" else 10**9
+  return ga.OracleGA(D, provider, cfg, rng).evolve(gens, patience=patience, record=record), rng
+
+
+@pytest.mark.parametrize("tag", ["c1", "c1default", "pm", "pc", "pe", "px", "pp", "po"])
+def test_ga_runs_match_reference(golden, tag):
+  g = golden("ga.npz")
+  (best, pop, fit, stats, records), rng = _run_oracle_ga(g, tag)
+  assert np.array_equal(best, g[f"{tag}_best"])
+  assert np.array_equal(np.asarray(stats["convergence_history"]), g[f"{tag}_history"])
+  assert stats["generations_completed"] == int(g[f"{tag}_gens"])
+  digests = [r[0] for r in records]
+  assert digests == [str(d) for d in g[f"{tag}_digests"]]
+  assert np.array_equal(np.stack([r[1] for r in records]), g[f"{tag}_fitness"])
+  assert rng.bit_generator.state["state"]["state"] % (1 << 63) == int(g[f"{tag}_rng"][0])
+
+
+def test_nn_init_matches_reference(golden):
+  g = golden("ga.npz")
+  coords = g["c1_coords"]
+  rng = np.random.default_rng(42)
+  pop = ga_ops.nn_init(rng, np.arange(100), 128, distances.candidate_list(5, coords=coords))
+  assert np.array_equal(pop, g["c1_init"])

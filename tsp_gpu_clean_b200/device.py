@@ -1,0 +1,168 @@
+"""Device plumbing: the GPU probe, streams, pointers and the per-context operand cache.
+
+PyTorch is used only for device memory, streams and host<->device copies; every
+computation on the path runs in libtspb.so kernels.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import weakref
+from typing import Any
+
+import numpy as np
+
+from .errors import GPUUnavailableError, VRAMInsufficientError
+from .native import load_library
+
+try:  # torch is the allocator and stream provider; absent torch means no GPU path
+  import torch
+except Exception:  # pragma: no cover - exercised only without torch
+  torch = None  # type: ignore[assignment]
+
+
+def require_gpu():
+  """Return the torch module after checking the CUDA device and libtspb.so.
+
+  Mirrors `require_gpu` of the reference (`src/protocols/backend.py:235-244`): a
+  machine without a usable device raises instead of degrading to a CPU path.
+  """
+  load_library()
+  if torch is None or not torch.cuda.is_available():
+    raise GPUUnavailableError("no CUDA device is available; the B200 strategies do not fall back to the CPU")
+  return torch
+
+
+def is_device_array(x: Any) -> bool:
+  return torch is not None and isinstance(x, torch.Tensor) and x.is_cuda
+
+
+def stream_handle(stream=None) -> ctypes.c_void_p:
+  s = stream if stream is not None else torch.cuda.current_stream()
+  return ctypes.c_void_p(s.cuda_stream)
+
+
+def ptr(t) -> ctypes.c_void_p | None:
+  if t is None:
+    return None
+  return ctypes.c_void_p(t.data_ptr())
+
+
+def device_tensor(a: np.ndarray, dtype) -> "torch.Tensor":
+  """H2D copy of a host array (C-contiguous) to the current device."""
+  t = torch.from_numpy(np.ascontiguousarray(a))
+  return t.to(device="cuda", dtype=dtype)
+
+
+def check_free(required_bytes: int, what: str) -> None:
+  free, _ = torch.cuda.mem_get_info()
+  if required_bytes > free:
+    raise VRAMInsufficientError(f"Insufficient VRAM for {what}", required_bytes=required_bytes, available_bytes=free)
+
+
+class Workspace:
+  """Monotonically growing device scratch buffer (grows, never shrinks)."""
+
+  def __init__(self):
+    self.buf = None
+
+  def get(self, nbytes: int):
+    if nbytes <= 0:
+      return None
+    if self.buf is None or self.buf.numel() < nbytes:
+      check_free(nbytes, "2-opt workspace")
+      self.buf = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    return self.buf
+
+
+#: Largest |distance| for which the kernels' int32 gain arithmetic is exact.
+MAX_DISTANCE = (1 << 30) - 1
+
+
+class DeviceOperands:
+  """Device copies of one context's distances, coordinates and candidate tables.
+
+  Uploaded once and reused by every strategy bound to the same context, the way
+  the reference's `ProblemContext` owns its GPU caches (`problem_context.py:336-527`).
+  """
+
+  def __init__(self, context):
+    self.context = context
+    self.h2d_bytes = 0
+    self._dist = None
+    self._coords = None
+    self._cand: dict[int, tuple] = {}
+
+  def coords(self):
+    if self._coords is None:
+      c = self.context.get_cpu_coordinates()
+      if c is None:
+        raise ValueError("problem has no coordinates for on-the-fly distances")
+      c = np.ascontiguousarray(c, dtype=np.float64)
+      if c.ndim != 2 or c.shape[1] != 2:
+        raise ValueError("on-the-fly distances need (n, 2) EUC_2D coordinates")
+      span = float(np.abs(c).max()) if c.size else 0.0
+      if span * 2.0 * 1.5 >= MAX_DISTANCE:
+        raise ValueError("coordinates too large for exact int32 gains")
+      self._coords = device_tensor(c, torch.float64)
+      self.h2d_bytes += self._coords.numel() * 8
+    return self._coords
+
+  def dist(self):
+    if self._dist is None:
+      D = self.context.get_cpu_distances()
+      D = np.ascontiguousarray(D, dtype=np.int32)
+      if D.size and (int(D.max()) > MAX_DISTANCE or int(D.min()) < 0):
+        raise ValueError("distances outside [0, 2^30) are not supported by the int32 gain kernels")
+      check_free(D.nbytes, f"dense distance matrix (n={D.shape[0]})")
+      self._dist = device_tensor(D, torch.int32)
+      self.h2d_bytes += D.nbytes
+    return self._dist
+
+  def use_coords(self, n: int, max_matrix_dimension: int | None) -> bool:
+    threshold = max_matrix_dimension
+    if threshold is None:
+      threshold = int(getattr(self.context, "max_matrix_dimension", 10_000))
+    prob = self.context.problem
+    return (
+      n > threshold
+      and getattr(prob, "edge_type", "EUC_2D") == "EUC_2D"
+      and getattr(prob, "coordinates", None) is not None
+    )
+
+  def distance_args(self, n: int, max_matrix_dimension: int | None = None):
+    """`(dist_tensor_or_None, stride, coords_tensor_or_None)` for one launch."""
+    if self.use_coords(n, max_matrix_dimension):
+      return None, 0, self.coords()
+    d = self.dist()
+    return d, int(d.shape[1]), None
+
+  def candidates(self, k: int, table: np.ndarray, n: int, max_matrix_dimension: int | None = None):
+    """Device `(cand, cand_dist)` for a host k-NN table (cached per k and table identity)."""
+    key = int(k)
+    hit = self._cand.get(key)
+    if hit is not None and hit[0] is table:
+      return hit[1], hit[2]
+    from .native import call
+
+    tab = np.ascontiguousarray(table, dtype=np.int32)
+    d_cand = device_tensor(tab, torch.int32)
+    self.h2d_bytes += tab.nbytes
+    rows, kk = tab.shape
+    d_cd = torch.empty((rows, kk), dtype=torch.int32, device="cuda")
+    dist, stride, coords = self.distance_args(n, max_matrix_dimension)
+    if rows and kk:
+      call("tspb_candidate_distances", ptr(d_cand), rows, kk, ptr(dist), stride, ptr(coords), ptr(d_cd), stream_handle())
+    self._cand[key] = (table, d_cand, d_cd)
+    return d_cand, d_cd
+
+
+_operands: "weakref.WeakKeyDictionary[Any, DeviceOperands]" = weakref.WeakKeyDictionary()
+
+
+def operands_for(context) -> DeviceOperands:
+  ops = _operands.get(context)
+  if ops is None:
+    ops = DeviceOperands(context)
+    _operands[context] = ops
+  return ops

@@ -1,0 +1,91 @@
+"""ctypes binding of libtspb.so (the C ABI declared in include/tspb.h).
+
+The library is loaded from this package directory (built in-tree by
+`tsp_gpu_clean_b200.build`). There is no CPU fallback: when the library is
+missing or no CUDA device is present, callers get `GPUUnavailableError`.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+from .errors import GPUUnavailableError, KernelError, NotPermutationError
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libtspb.so")
+
+TSPB_OK = 0
+TSPB_ERR_ARG = 1
+TSPB_ERR_CUDA = 2
+TSPB_ERR_NOT_PERMUTATION = 3
+TSPB_ERR_RANGE = 4
+TSPB_ERR_UNSUPPORTED = 5
+TSPB_ERR_WORKSPACE = 6
+TSPB_ERR_BUDGET = 7
+
+MODE_CODES = {"best": 0, "batch": 0, "first": 1, "multi_move": 2}
+
+_p = ctypes.c_void_p
+_i32 = ctypes.c_int32
+_i64 = ctypes.c_int64
+_sz = ctypes.c_size_t
+_f64 = ctypes.c_double
+
+#: name -> (restype, argtypes); one entry per declaration in include/tspb.h.
+SIGNATURES: dict[str, tuple] = {
+  "tspb_version": (ctypes.c_int, []),
+  "tspb_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+  "tspb_two_opt_workspace_bytes": (_sz, [_i32, _i32, _i32, _i32, _i32]),
+  "tspb_two_opt": (ctypes.c_int, [_p, _i32, _i32, _p, _i64, _p, _p, _p, _i32, _i32, _i64, _i32, _p, _p, _p, _sz, _p]),
+  "tspb_candidate_distances": (ctypes.c_int, [_p, _i32, _i32, _p, _i64, _p, _p, _p]),
+  "tspb_tour_cost": (ctypes.c_int, [_p, _i32, _i32, _p, _i64, _p, _i32, _p, _p]),
+  "tspb_tournament": (ctypes.c_int, [_p, _i32, _p, _i32, _i32, _p, _p]),
+  "tspb_gather_rows": (ctypes.c_int, [_p, _i32, _i32, _p, _i32, _p, _p]),
+  "tspb_pmx": (ctypes.c_int, [_p, _i32, _i32, _p, _p, _p, _p, _p]),
+  "tspb_inversion": (ctypes.c_int, [_p, _i32, _i32, _p, _f64, _p, _p, _p]),
+  "tspb_stable_rank": (ctypes.c_int, [_p, _i32, _i32, _p, _p]),
+  "tspb_validate_perm": (ctypes.c_int, [_p, _i32, _i32, _p, _p]),
+  "tspb_euc2d_matrix": (ctypes.c_int, [_p, _i32, _p, _i64, _p]),
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+  """Load libtspb.so and bind every signature (no GPU needed to load)."""
+  global _lib
+  with _lock:
+    if _lib is not None:
+      return _lib
+    if not os.path.exists(path):
+      raise GPUUnavailableError(f"libtspb.so is not built at {path}; run `python -m tsp_gpu_clean_b200.build`")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+      fn = getattr(lib, name)
+      fn.restype = res
+      fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def status_text(code: int) -> str:
+  return load_library().tspb_status_string(int(code)).decode()
+
+
+def check(func: str, code: int) -> None:
+  """Raise for a non-zero host-side status of a libtspb call."""
+  if code == TSPB_OK:
+    return
+  if code == TSPB_ERR_NOT_PERMUTATION:
+    raise NotPermutationError(f"{func}: {status_text(code)}")
+  if code == TSPB_ERR_ARG:
+    raise ValueError(f"{func}: {status_text(code)}")
+  raise KernelError(func, code, status_text(code))
+
+
+def call(name: str, *args) -> None:
+  lib = load_library()
+  check(name, getattr(lib, name)(*args))
