@@ -1,0 +1,358 @@
+"""Benchmark: batched 2-opt to a local optimum on B200 (2-opt deltas/s).
+
+Workload (one step): 1024 random-permutation tours of a 1000-city, 20-cluster
+Gaussian-mixture EUC_2D instance (sigma 30, [0, 1000]^2, int32 matrix), refined to a
+local optimum with candidate_k=20, once in best mode and once in first mode. The
+metric counts the (i, j) pairs the reference's CPU scan evaluates on the same tours
+(oracle-equivalent 2-opt deltas), summed over every pass of every tour; the kernel
+reports that count itself and tests pin it to the oracle.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+- `value`: deltas/s with tours already resident in HBM, timed with CUDA events on
+  the launching stream, L2 flushed (256 MiB write) between timed steps.
+- `e2e`: the same metric through `LocalSearchB200TourTwoOpt.improve_batch` on host
+  NumPy tours (pinned H2D, kernel, D2H per call), timed with CUDA events.
+- `--impl reference`: the reference CPU path (the NumPy oracle restatement of
+  `LocalSearchCPUTourTwoOpt`) on the host cores, on a bounded sample of tours.
+- N > 1 (torchrun): every rank refines its own 1024 tours (weak scaling, no
+  collective on the data path); rank 0 prints the aggregate over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+  sys.path.insert(0, ROOT)
+
+from tsp_gpu_clean_b200 import instances  # noqa: E402
+
+METRIC = "2-opt deltas/s"
+UNIT = "deltas/s"
+MODES = ("best", "first")
+K_CAND = 20
+#: Algorithmic bytes per 2-opt delta: three int32 distances (d(a,c), d(b,d) and the
+#: two retired edges count as one cached read each side) = 12 B, plus the candidate,
+#: position and successor reads = 12 B.
+BYTES_PER_DELTA = 24
+L2_FLUSH_BYTES = 256 << 20
+
+
+def _peaks() -> dict:
+  path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+  if os.path.exists(path):
+    with open(path) as fh:
+      d = json.load(fh)
+    return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+  return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+# ----------------------------------------------------------------------------------- CPU
+def _cpu_worker(args):
+  """Refine one tour in both modes with the oracle; returns (pairs, seconds)."""
+  coords, tour = args
+  from oracle import distances, two_opt
+
+  D = distances.euc2d_matrix(coords)
+  cand = distances.candidate_list(K_CAND, coords=coords)
+  t0 = time.perf_counter()
+  pairs = 0
+  for mode in MODES:
+    _, st = two_opt.improve_batch(tour[None, :], D, cand, mode, 10**9)
+    pairs += int(st[0, 1])
+  return pairs, time.perf_counter() - t0
+
+
+def cpu_sample(pool, workers: int, seed_offset: int = 0) -> dict:
+  """Oracle deltas/s on `workers` tours in parallel (one tour per process)."""
+  coords, _ = instances.c2_workload(tours=1)
+  tours = instances.random_tours(instances.C2_N, workers, 777 + seed_offset)
+  t0 = time.perf_counter()
+  res = pool.map(_cpu_worker, [(coords, tours[i]) for i in range(workers)])
+  wall = time.perf_counter() - t0
+  pairs = sum(r[0] for r in res)
+  return {"value": pairs / wall, "pairs": pairs, "wall_s": wall, "tours": workers}
+
+
+# ------------------------------------------------------------------------------ clocks
+class ClockSampler:
+  FIELDS = "clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+  def __init__(self, device: int):
+    self.device = device
+    self.proc = None
+
+  def __enter__(self):
+    try:
+      self.proc = subprocess.Popen(
+        ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
+        stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+    except Exception:
+      self.proc = None
+    return self
+
+  def __exit__(self, *exc):
+    self.lines = []
+    if self.proc is not None:
+      self.proc.terminate()
+      try:
+        out, _ = self.proc.communicate(timeout=5)
+      except Exception:
+        self.proc.kill()
+        out = ""
+      self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+  def summary(self) -> dict:
+    sm, mx, reasons = [], 0.0, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for ln in getattr(self, "lines", []):
+      parts = [p.strip() for p in ln.split(",")]
+      if len(parts) < 6:
+        continue
+      try:
+        sm.append(float(parts[0]))
+        mx = max(mx, float(parts[1]))
+      except ValueError:
+        continue
+      for nm, v in zip(names, parts[2:6]):
+        if v.lower().startswith("active"):
+          reasons.add(nm)
+    return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+            "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------------- GPU
+def _dist_env():
+  world = int(os.environ.get("WORLD_SIZE", "1"))
+  rank = int(os.environ.get("RANK", "0"))
+  local = int(os.environ.get("LOCAL_RANK", "0"))
+  return world, rank, local
+
+
+def aggregate(units: float, elapsed_s: float, world: int):
+  """(sum of units over ranks, max elapsed over ranks); identity for one process."""
+  if world <= 1:
+    return units, elapsed_s
+  import torch
+  import torch.distributed as dist
+
+  dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+  u = torch.tensor([units], dtype=torch.float64, device=dev)
+  e = torch.tensor([elapsed_s], dtype=torch.float64, device=dev)
+  dist.all_reduce(u, op=dist.ReduceOp.SUM)
+  dist.all_reduce(e, op=dist.ReduceOp.MAX)
+  return float(u.item()), float(e.item())
+
+
+def run_gpu(args, pool) -> dict | None:
+  import torch
+  import torch.distributed as dist
+
+  from tsp_gpu_clean_b200 import native
+  from tsp_gpu_clean_b200.build import build_library
+  from tsp_gpu_clean_b200.device import operands_for, ptr, stream_handle
+  from tsp_gpu_clean_b200.problem import Problem, ProblemContext
+  from tsp_gpu_clean_b200.strategies.local_search import LocalSearchB200TourTwoOpt
+
+  world, rank, local = _dist_env()
+  torch.cuda.set_device(local)
+  if world > 1:
+    import datetime
+
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+  build_library()
+  lib = native.load_library()
+
+  coords, _ = instances.c2_workload(tours=1)
+  tours_np = instances.random_tours(instances.C2_N, args.tours, instances.C2_TOUR_SEED + 1000 * rank)
+  n = instances.C2_N
+  ctx = ProblemContext(Problem.from_coordinates(coords, "c2"), seed=0)
+  ops = operands_for(ctx)
+  dist_t, stride, _ = ops.distance_args(n)
+  tabs = ops.candidates(K_CAND, ctx.get_cpu_candidate_list(K_CAND), n)
+  k = tabs.k
+  rev_off = tabs.rev_off if args.kernel == "cached" else None
+  rev_idx = tabs.rev_idx if args.kernel == "cached" else None
+  packed = tabs.packed if args.kernel == "scan" else None
+  pristine = torch.from_numpy(tours_np).cuda()
+  work = torch.empty_like(pristine)
+  stats = {m: torch.zeros((args.tours, 4), dtype=torch.int64, device="cuda") for m in MODES}
+  status = torch.zeros(args.tours, dtype=torch.int32, device="cuda")
+  flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+  stream = torch.cuda.current_stream()
+  modes = MODES if args.mode == "both" else (args.mode,)
+
+  def step(ev_pairs):
+    for m in modes:
+      work.copy_(pristine)
+      ev_pairs[m][0].record(stream)
+      rc = lib.tspb_two_opt(ptr(work), args.tours, n, ptr(dist_t), stride, None, ptr(tabs.cand), ptr(tabs.cand_dist),
+                            ptr(rev_off), ptr(rev_idx), ptr(packed), k,
+                            native.MODE_CODES[m], 10**9, args.threads, ptr(stats[m]), ptr(status), None, 0,
+                            stream_handle())
+      native.check("tspb_two_opt", rc)
+      ev_pairs[m][1].record(stream)
+
+  def new_events():
+    return {m: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for m in modes}
+
+  for _ in range(args.warmup):
+    step(new_events())
+  torch.cuda.synchronize()
+  if int(status.max().item()) != 0:
+    raise RuntimeError("2-opt kernel reported a bad tour")
+
+  per_step = []
+  if world > 1:
+    dist.barrier()
+  torch.cuda.synchronize()
+  with ClockSampler(local) as clocks:
+    for _ in range(args.steps):
+      flush.fill_(1)
+      ev = new_events()
+      step(ev)
+      per_step.append(ev)
+    torch.cuda.synchronize()
+  if world > 1:
+    dist.barrier()
+  kernel_ms = {m: sum(e[m][0].elapsed_time(e[m][1]) for e in per_step) for m in modes}
+  total_ms = sum(kernel_ms.values())
+  st = {m: stats[m].cpu().numpy() for m in modes}
+  pairs_step = sum(int(st[m][:, 1].sum()) for m in modes)
+  eval_step = sum(int(st[m][:, 3].sum()) for m in modes)
+  units_all, elapsed = aggregate(pairs_step * args.steps, total_ms / 1e3, world)
+  value = units_all / elapsed
+
+  # end to end: the public strategy call on host tours (pinned H2D + kernel + D2H)
+  e2e_ms = 0.0
+  strategies = {m: LocalSearchB200TourTwoOpt(max_iterations=10**9, mode=m, candidate_k=K_CAND,
+                                              threads_per_block=args.threads) for m in modes}
+  for s_ in strategies.values():
+    s_.kernel = args.kernel
+  for m in modes:
+    strategies[m].improve_batch(tours_np, ctx)  # warm
+  torch.cuda.synchronize()
+  e2e_pairs = 0
+  for _ in range(args.steps):
+    for m in modes:
+      e0 = torch.cuda.Event(enable_timing=True)
+      e1 = torch.cuda.Event(enable_timing=True)
+      e0.record(stream)
+      out = strategies[m].improve_batch(tours_np, ctx)
+      e1.record(stream)
+      torch.cuda.synchronize()
+      e2e_ms += e0.elapsed_time(e1)
+      e2e_pairs += int(strategies[m].last_stats[:, 1].sum())
+  e2e_units, e2e_elapsed = aggregate(e2e_pairs, e2e_ms / 1e3, world)
+  del out
+
+  dominant = max(modes, key=lambda m: kernel_ms[m])
+  launches = args.steps * len(modes)
+  dom_ms = kernel_ms[dominant] / args.steps
+  dom_eval = int(st[dominant][:, 3].sum())
+  achieved_gbs = dom_eval * BYTES_PER_DELTA / (dom_ms / 1e3) / 1e9
+  peaks = _peaks()
+  res = {
+    "value": value,
+    "ms_per_step": total_ms / args.steps,
+    "kernel_ms_per_step": {m: kernel_ms[m] / args.steps for m in modes},
+    "pairs_per_step": pairs_step,
+    "evaluated_per_step": eval_step,
+    "passes_per_step": {m: int(st[m][:, 0].sum()) for m in modes},
+    "clocks": clocks.summary(),
+    "e2e": {"value": e2e_units / e2e_elapsed, "unit": UNIT,
+            "h2d_bytes_per_step": int(tours_np.nbytes * len(modes)),
+            "d2h_bytes_per_step": int(tours_np.nbytes * len(modes) + args.tours * 32 * len(modes))},
+    "gpu_launches": launches,
+    "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                 "frac": achieved_gbs / peaks["hbm_gbs"], "traffic": None,
+                 "kernel": f"two_opt_{args.kernel}_kernel<{dominant}>",
+                 "peak_source": peaks["source"],
+                 "basis": f"{BYTES_PER_DELTA} B per gain the kernel computed"},
+    "world": world,
+    "rank": rank,
+  }
+  if world > 1:
+    dist.destroy_process_group()
+  return res if rank == 0 else None
+
+
+def main(argv=None) -> int:
+  ap = argparse.ArgumentParser()
+  ap.add_argument("--gpus", type=int, default=1)
+  ap.add_argument("--steps", type=int, default=3)
+  ap.add_argument("--warmup", type=int, default=3)
+  ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+  ap.add_argument("--tours", type=int, default=instances.C2_TOURS)
+  ap.add_argument("--mode", default="both", choices=["both", "best", "first"])
+  ap.add_argument("--threads", type=int, default=128)
+  ap.add_argument("--kernel", default="scan", choices=["scan", "scan_unpacked", "cached"])
+  ap.add_argument("--cpu-workers", type=int, default=0, help="0: all host cores, capped at 64")
+  ap.add_argument("--no-cpu-baseline", action="store_true")
+  args = ap.parse_args(argv)
+  world, rank, _ = _dist_env()
+  workers = args.cpu_workers or min(os.cpu_count() or 1, 64)
+  config = {"workload": "2-opt to local optimum (best and first modes, candidate_k=20) on random tours of a "
+                        "1000-city 20-cluster EUC_2D instance",
+            "tours": args.tours, "n": instances.C2_N, "k": K_CAND, "modes": list(MODES if args.mode == "both" else (args.mode,)),
+            "l2": "flushed between timed steps (256 MiB write); the 4 MB matrix is L2-resident within a step",
+            "threads_per_cta": args.threads, "kernel": args.kernel}
+
+  if args.impl == "reference":
+    if rank != 0:
+      return 0
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(workers) as pool:
+      for w in range(args.warmup):
+        cpu_sample(pool, workers, seed_offset=w)
+      vals = [cpu_sample(pool, workers, seed_offset=100 + s) for s in range(args.steps)]
+    value = sum(v["pairs"] for v in vals) / sum(v["wall_s"] for v in vals)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sum(v["wall_s"] for v in vals) / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded)", "impl": "reference", "config": config,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port",
+                             "sample": f"{workers} tours per step (one per process), best then first mode to local optimum"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+  cpu = None
+  pool = None
+  if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    pool = mp.get_context("spawn").Pool(workers)  # before the first CUDA call
+  res = run_gpu(args, pool)
+  if pool is not None:
+    cpu = cpu_sample(pool, workers)
+    pool.close()
+    pool.join()
+  if res is None:
+    return 0
+  line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+          "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+          "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)", "config": config,
+          "clocks": res["clocks"], "e2e": res["e2e"], "gpu_launches": res["gpu_launches"],
+          "roofline": res["roofline"],
+          "detail": {"kernel_ms_per_step": res["kernel_ms_per_step"], "pairs_per_step": res["pairs_per_step"],
+                     "evaluated_per_step": res["evaluated_per_step"], "passes_per_step": res["passes_per_step"]}}
+  if cpu is not None:
+    line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": workers, "kind": "port",
+                            "sample": f"{cpu['tours']} tours (one per process), best then first mode to local optimum, "
+                                      f"{cpu['wall_s']:.1f} s wall"}
+  print(json.dumps(line))
+  return 0
+
+
+if __name__ == "__main__":
+  sys.exit(main())

@@ -56,6 +56,11 @@ size_t tspb_two_opt_workspace_bytes(int32_t num_tours, int32_t n, int32_t k, int
  *   and the GPU launch loop of LocalSearchGPUTourTwoOpt._improve_grid (:831-899).
  * Cyclic TSP topology. `cand` (n x k, k-NN table) selects candidate mode; NULL selects
  * the exhaustive scan. `cand_dist` (n x k, optional) holds d(a, cand[a][r]).
+ * Candidate best/first run the rescan kernel (block sizes 64, 128, 256 or 512) unless
+ * `rev_off`/`rev_idx` (from tspb_candidate_reverse_index) are given, which select the
+ * cached kernel: per-row keys and pair counts kept exactly across passes and refreshed
+ * only where a reversal can change them. `cand_packed` (optional, from
+ * tspb_candidate_pack) lets the rescan kernel read id and distance in one word.
  * Distances come from `dist` when non-NULL, else are rebuilt from `coords` in FP64
  * with TSPLIB EUC_2D rounding. `max_iterations` bounds the passes per tour.
  * `stats` (optional, num_tours x 4 int64): passes, pairs evaluated by the reference
@@ -63,7 +68,8 @@ size_t tspb_two_opt_workspace_bytes(int32_t num_tours, int32_t n, int32_t k, int
  */
 int tspb_two_opt(int32_t* tours, int32_t num_tours, int32_t n,
                  const int32_t* dist, int64_t dist_stride, const double* coords,
-                 const int32_t* cand, const int32_t* cand_dist, int32_t k,
+                 const int32_t* cand, const int32_t* cand_dist,
+                 const int32_t* rev_off, const int32_t* rev_idx, const uint32_t* cand_packed, int32_t k,
                  int32_t mode, int64_t max_iterations, int32_t block_threads,
                  int64_t* stats, int32_t* status,
                  void* workspace, size_t workspace_bytes, void* stream);
@@ -76,6 +82,23 @@ int tspb_two_opt(int32_t* tours, int32_t num_tours, int32_t n,
 int tspb_candidate_distances(const int32_t* cand, int32_t n, int32_t k,
                              const int32_t* dist, int64_t dist_stride, const double* coords,
                              int32_t* cand_dist, void* stream);
+
+/*
+ * Reverse k-NN index in CSR form: for node c, rev_idx[rev_off[c] .. rev_off[c+1]) lists
+ * the flat entries a*k + r with cand[a*k + r] == c (order within a list unspecified).
+ * rev_off has n + 1 entries, rev_idx n*k, scratch n int32. No reference counterpart:
+ * it serves the cached 2-opt kernel's refresh of gains whose second city moved.
+ */
+int tspb_candidate_reverse_index(const int32_t* cand, int32_t n, int32_t k, int32_t* rev_off,
+                                 int32_t* rev_idx, int32_t* scratch, void* stream);
+
+/*
+ * packed[e] = cand[e] | cand_dist[e] << 16 for the n x k table; *overflow (device int)
+ * becomes 1 when an id or distance does not fit 16 bits (the packed table must then not
+ * be used). No reference counterpart: a layout of the k-NN table for the 2-opt scan.
+ */
+int tspb_candidate_pack(const int32_t* cand, const int32_t* cand_dist, int32_t n, int32_t k,
+                        uint32_t* packed, int32_t* overflow, void* stream);
 
 /*
  * Closed-tour cost per row (sum of n edges incl. the closing edge when return_to_depot),

@@ -50,9 +50,9 @@ def test_status_strings_and_version(lib):
 
 def test_host_argument_checks_run_without_a_gpu(lib):
   # Argument validation returns before any CUDA call.
-  assert lib.tspb_two_opt(None, -1, 10, None, 0, None, None, None, 0, 0, 1, 256, None, None, None, 0, None) == 1
-  assert lib.tspb_two_opt(None, 0, 10, None, 0, None, None, None, 0, 0, 1, 256, None, None, None, 0, None) == 0
-  assert lib.tspb_two_opt(None, 1, 10, None, 0, None, None, None, 0, 7, 1, 256, None, None, None, 0, None) == 1
+  assert lib.tspb_two_opt(None, -1, 10, None, 0, None, None, None, None, None, None, 0, 0, 1, 256, None, None, None, 0, None) == 1
+  assert lib.tspb_two_opt(None, 0, 10, None, 0, None, None, None, None, None, None, 0, 0, 1, 256, None, None, None, 0, None) == 0
+  assert lib.tspb_two_opt(None, 1, 10, None, 0, None, None, None, None, None, None, 0, 7, 1, 256, None, None, None, 0, None) == 1
   assert lib.tspb_tournament(None, 0, None, 4, 0, None, None) == 1
   assert lib.tspb_stable_rank(None, 4, 5, None, None) == 1
 

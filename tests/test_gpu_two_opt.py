@@ -62,21 +62,43 @@ def test_golden_small_cases(b200, golden):
     coords = data.get(f"c{c}_coords")
     ctx = _ctx(b200, D=D if coords is None else None, coords=coords, cand=cand, k=k)
     for m in ([mode, "batch"] if mode == "best" else [mode]):
-      before = tin.copy()
-      got = LS(max_iterations=iters, mode=m, candidate_k=k).improve_batch(tin, ctx)
-      assert np.array_equal(tin, before), "input mutated"
-      assert np.array_equal(got, tout), f"case {c}: n={n} k={k} mode={m} iters={iters}"
+      for kern in (("scan", "scan_unpacked", "cached") if k is not None and m != "multi_move" else ("scan",)):
+        before = tin.copy()
+        ls = LS(max_iterations=iters, mode=m, candidate_k=k)
+        ls.kernel = kern
+        got = ls.improve_batch(tin, ctx)
+        assert np.array_equal(tin, before), "input mutated"
+        assert np.array_equal(got, tout), f"case {c}: n={n} k={k} mode={m} iters={iters} kernel={kern}"
 
 
+@pytest.mark.parametrize("kern", ["scan", "scan_unpacked", "cached"])
 @pytest.mark.parametrize("mode", ["best", "first"])
-def test_golden_c2_local_optimum_with_counts(b200, golden, mode):
+def test_golden_c2_local_optimum_with_counts(b200, golden, mode, kern):
   data = golden("two_opt_c2.npz")
   ctx = _ctx(b200, coords=data["coords"], cand=data["cand20"], k=20)
   ls = b200[2](max_iterations=10**9, mode=mode, candidate_k=20)
+  ls.kernel = kern
   got = ls.improve_batch(data["tours_in"], ctx)
   assert np.array_equal(got, data[f"{mode}_out"])
   assert np.array_equal(ls.last_stats[:, 0], data[f"{mode}_stats"][:, 0]), "passes"
   assert np.array_equal(ls.last_stats[:, 1], data[f"{mode}_stats"][:, 1]), "oracle-equivalent pairs"
+
+
+@pytest.mark.parametrize("kern", ["scan", "cached"])
+@pytest.mark.parametrize("threads", [64, 128, 256, 512])
+def test_kernel_block_sizes(b200, threads, kern):
+  coords = instances.clustered_instance(700, 12, 30.0, 13)
+  tours = instances.random_tours(700, 6, 14)
+  ctx = _ctx(b200, coords=coords)
+  D = odist.euc2d_matrix(coords)
+  cand = ctx.get_cpu_candidate_list(20)
+  for mode in ("best", "first"):
+    ls = b200[2](max_iterations=10**9, mode=mode, candidate_k=20, threads_per_block=threads)
+    ls.kernel = kern
+    got = ls.improve_batch(tours, ctx)
+    want, st = otwo.improve_batch(tours, D, cand, mode, 10**9)
+    assert np.array_equal(got, want)
+    assert np.array_equal(ls.last_stats[:, :3], st)
 
 
 @pytest.mark.parametrize("mode", ["best", "first", "multi_move"])

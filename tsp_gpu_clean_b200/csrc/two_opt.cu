@@ -21,37 +21,10 @@
 // workspace slice per tour.
 #include <algorithm>
 
-#include "common.cuh"
+#include "two_opt.cuh"
 
 namespace tspb {
 
-struct TwoOptArgs {
-  int32_t* tours;
-  int num_tours;
-  int n;
-  DistSrc ds;
-  const int32_t* cand;
-  const int32_t* cand_dist;
-  int k;
-  long long max_iter;
-  long long* stats;
-  int32_t* status;
-  unsigned char* ws;
-  size_t ws_tour_bytes;
-  size_t ws_keys_off;  // offset of the multi_move key buffer inside a tour's slice
-  int arrays_in_smem;
-};
-
-// Order-preserving u64 key: negative int32 gain in the high word, scan index low.
-__device__ __forceinline__ unsigned long long gain_key(int gain, unsigned idx) {
-  return ((unsigned long long)((unsigned)gain ^ 0x80000000u) << 32) | idx;
-}
-__device__ __forceinline__ int key_gain(unsigned long long key) {
-  return (int)((unsigned)(key >> 32) ^ 0x80000000u);
-}
-
-constexpr unsigned long long NO_KEY = ~0ull;
-constexpr unsigned NO_IDX = ~0u;
 constexpr long long EXH_BLOCK = 1LL << 18;  // exhaustive pairs per CPU block (two_opt.py:155)
 
 // Pairs of the exhaustive cyclic scan before row i (two_opt.py:188-196).
@@ -69,9 +42,6 @@ struct Smem {
   int stop;         // pass loop must end with an error status
 };
 
-// Watchdog: a tour that has not converged after this many SM cycles (about 35 s at
-// 1.9 GHz) ends with TSPB_ERR_BUDGET instead of running on.
-constexpr long long BUDGET_CYCLES = 1LL << 36;
 
 template <int MODE, bool CAND>
 __global__ void __launch_bounds__(1024) two_opt_kernel(const TwoOptArgs A) {
@@ -417,7 +387,7 @@ __global__ void __launch_bounds__(1024) two_opt_kernel(const TwoOptArgs A) {
   }
 }
 
-static int smem_optin() {
+int smem_optin() {
   static int cached = -1;
   if (cached < 0) {
     int dev = 0;
@@ -436,7 +406,7 @@ struct Layout {
   size_t ws_keys_off;
 };
 
-static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
 static unsigned long long next_pow2(unsigned long long v) {
   unsigned long long p = 1;
@@ -474,15 +444,32 @@ static int launch(const TwoOptArgs& a, int threads, size_t smem, cudaStream_t st
 
 using namespace tspb;
 
+// Per-tour global bytes of the cached kernel when its arrays do not fit in shared memory.
+static size_t cached_ws_tour_bytes(int n, int mode) {
+  const size_t need = two_opt_cached_tour_bytes(n, mode);
+  const size_t budget = (size_t)smem_optin() - 2048;
+  return need <= budget ? 0 : align256(need);
+}
+
 extern "C" size_t tspb_two_opt_workspace_bytes(int32_t num_tours, int32_t n, int32_t k, int32_t mode, int32_t block_threads) {
   (void)block_threads;
   if (num_tours <= 0 || n < 4) return 0;
   const Layout L = two_opt_layout(n, k, mode, k > 0);
-  return L.ws_tour_bytes * (size_t)num_tours;
+  size_t per = L.ws_tour_bytes;
+  if (k > 0 && mode != TSPB_MODE_MULTI_MOVE) {
+    const size_t c = cached_ws_tour_bytes(n, mode);
+    per = per > c ? per : c;
+    const size_t need = two_opt_scan_tour_bytes(n);
+    const size_t sc = need <= (size_t)smem_optin() - 2048 ? 0 : align256(need);
+    per = per > sc ? per : sc;
+  }
+  return per * (size_t)num_tours;
 }
 
 extern "C" int tspb_two_opt(int32_t* tours, int32_t num_tours, int32_t n, const int32_t* dist, int64_t dist_stride,
-                            const double* coords, const int32_t* cand, const int32_t* cand_dist, int32_t k, int32_t mode,
+                            const double* coords, const int32_t* cand, const int32_t* cand_dist,
+                            const int32_t* rev_off, const int32_t* rev_idx, const uint32_t* cand_packed, int32_t k,
+                            int32_t mode,
                             int64_t max_iterations, int32_t block_threads, int64_t* stats, int32_t* status,
                             void* workspace, size_t workspace_bytes, void* stream) {
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
@@ -500,6 +487,56 @@ extern "C" int tspb_two_opt(int32_t* tours, int32_t num_tours, int32_t n, const 
   if (dist != nullptr && dist_stride < n) return TSPB_ERR_ARG;
   int threads = block_threads > 0 ? block_threads : 256;
   if (threads % 32 != 0 || threads > 1024) return TSPB_ERR_ARG;
+  if (use_cand && mode != TSPB_MODE_MULTI_MOVE && (rev_off == nullptr || rev_idx == nullptr)) {
+    if (threads != 64 && threads != 128 && threads != 256 && threads != 512) return TSPB_ERR_ARG;
+    const size_t need = two_opt_scan_tour_bytes(n);
+    const size_t per = need <= (size_t)smem_optin() - 2048 ? 0 : align256(need);
+    if (per > 0 && (workspace == nullptr || workspace_bytes < per * (size_t)num_tours)) return TSPB_ERR_WORKSPACE;
+    if (cand_packed != nullptr && n > 65535) return TSPB_ERR_ARG;
+    TwoOptArgs c{};
+    c.tours = tours;
+    c.num_tours = num_tours;
+    c.n = n;
+    c.ds.dist = dist;
+    c.ds.stride = dist_stride;
+    c.ds.coords = reinterpret_cast<const double2*>(coords);
+    c.cand = cand;
+    c.cand_dist = cand_dist;
+    c.cand_packed = cand_packed;
+    c.k = k;
+    c.max_iter = max_iterations;
+    c.stats = reinterpret_cast<long long*>(stats);
+    c.status = status;
+    c.ws = reinterpret_cast<unsigned char*>(workspace);
+    c.ws_tour_bytes = per;
+    c.arrays_in_smem = per == 0 ? 1 : 0;
+    return launch_two_opt_scan(c, mode, threads, st);
+  }
+  if (use_cand && rev_off != nullptr && rev_idx != nullptr && mode != TSPB_MODE_MULTI_MOVE) {
+    if (threads != 64 && threads != 128 && threads != 256 && threads != 512) return TSPB_ERR_ARG;
+    if (k > 255) return TSPB_ERR_UNSUPPORTED;  // per-row counts are packed bytes
+    const size_t per = cached_ws_tour_bytes(n, mode);
+    if (per > 0 && (workspace == nullptr || workspace_bytes < per * (size_t)num_tours)) return TSPB_ERR_WORKSPACE;
+    TwoOptArgs c{};
+    c.tours = tours;
+    c.num_tours = num_tours;
+    c.n = n;
+    c.ds.dist = dist;
+    c.ds.stride = dist_stride;
+    c.ds.coords = reinterpret_cast<const double2*>(coords);
+    c.cand = cand;
+    c.cand_dist = cand_dist;
+    c.k = k;
+    c.max_iter = max_iterations;
+    c.stats = reinterpret_cast<long long*>(stats);
+    c.status = status;
+    c.ws = reinterpret_cast<unsigned char*>(workspace);
+    c.ws_tour_bytes = per;
+    c.arrays_in_smem = per == 0 ? 1 : 0;
+    c.rev_off = rev_off;
+    c.rev_idx = rev_idx;
+    return launch_two_opt_cached(c, mode, threads, st);
+  }
   const Layout L = two_opt_layout(n, use_cand ? k : 0, mode, use_cand);
   if (L.ws_tour_bytes > 0) {
     if (workspace == nullptr || workspace_bytes < L.ws_tour_bytes * (size_t)num_tours) return TSPB_ERR_WORKSPACE;

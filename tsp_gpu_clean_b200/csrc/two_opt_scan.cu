@@ -1,0 +1,294 @@
+// Candidate-mode 2-opt (best / first), full rescan per pass, latency-tuned for sm_100a.
+//
+// Same semantics as the reference scan (src/algorithms/strategies/local_search/two_opt.py:
+// pair order :347-367, gains :237-245, best :386-440, first :442-489, passes :565-595),
+// arranged so that one pass keeps as many independent loads in flight as possible:
+//
+// - the tour is held position- and node-indexed in shared memory: tour[p], pos[a],
+//   succ[a] and eout[a] = d(a, succ[a]); the gain of entry (i, r) with a = tour[i],
+//   c = N_k[a][r] is (d(a,c) - eout[a]) + (d(succ[a], succ[c]) - eout[c]);
+// - the k-NN table and d(a, c) come packed as one u32 per entry (c | d(a,c) << 16) when
+//   both fit 16 bits, so the whole per-instance table (80 KB at n=1000, k=20) stays in L1;
+// - each thread evaluates U entries per round with their loads issued back to back
+//   (k-NN word -> shared-memory lookups -> one L2 gather of d(succ[a], succ[c])).
+//
+// best keeps a per-thread (gain, i*k + r) minimum and reduces once per pass. first
+// publishes the smallest improving index of a round with a shared atomicMin; once set,
+// later rounds only count the pairs the reference still evaluates (validity, no gains).
+#include "two_opt.cuh"
+
+namespace tspb {
+
+struct ScanSmem {
+  unsigned long long red64[32];
+  long long redll[32];
+  unsigned first;
+  int bad;
+  int stop;
+};
+
+template <int THREADS>
+struct ScanMinBlocks {
+  static constexpr int value = THREADS == 64 ? 16 : THREADS == 128 ? 8 : THREADS == 256 ? 4 : 2;
+};
+
+template <int MODE, int THREADS, int U, bool PACKED>
+__global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value) two_opt_scan_kernel(const TwoOptArgs A) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  __shared__ ScanSmem S;
+  const int n = A.n, k = A.k, rows = n - 2;
+  const int tid = threadIdx.x;
+  const int t = blockIdx.x;
+  if (t >= A.num_tours) return;
+  int32_t* g_tour = A.tours + (long long)t * n;
+  unsigned char* base = A.arrays_in_smem ? dsm : A.ws + (size_t)t * A.ws_tour_bytes;
+  int* tour = reinterpret_cast<int*>(base);
+  int* pos = tour + n;
+  int* succ = pos + n;
+  int* eout = succ + n;
+  const DistSrc ds = A.ds;
+  const uint32_t* __restrict__ packed = A.cand_packed;
+  const int32_t* __restrict__ cand = A.cand;
+  const int32_t* __restrict__ cdist = A.cand_dist;
+  const int32_t* __restrict__ dist = A.ds.dist;
+  const unsigned stride = (unsigned)A.ds.stride;
+
+  if (tid == 0) {
+    S.bad = 0;
+    S.stop = 0;
+  }
+  for (int p = tid; p < n; p += THREADS) {
+    tour[p] = g_tour[p];
+    pos[p] = -1;
+  }
+  __syncthreads();
+  for (int p = tid; p < n; p += THREADS) {
+    const int v = tour[p];
+    if ((unsigned)v >= (unsigned)n || atomicExch(&pos[v], p) != -1) S.bad = 1;
+  }
+  __syncthreads();
+  if (S.bad) {
+    if (tid == 0) {
+      if (A.status) A.status[t] = TSPB_ERR_NOT_PERMUTATION;
+      if (A.stats)
+        for (int q = 0; q < 4; ++q) A.stats[(long long)t * 4 + q] = 0;
+    }
+    return;
+  }
+  for (int p = tid; p < n; p += THREADS) {
+    const int x = tour[p], y = tour[p + 1 == n ? 0 : p + 1];
+    succ[x] = y;
+    eout[x] = ds(x, y);
+  }
+  __syncthreads();
+
+  const int E = rows * k;
+  constexpr int STEP = THREADS * U;
+  const int sq = STEP / k, sr = STEP - (STEP / k) * k;
+  long long passes = 0, moves = 0, my_pairs = 0, my_eval = 0;
+  int err = TSPB_OK;
+  const long long t_start = clock64();
+
+  while (passes < A.max_iter) {
+    if (tid == 0) {
+      if (clock64() - t_start > BUDGET_CYCLES) S.stop = TSPB_ERR_BUDGET;
+      S.first = NO_IDX;
+    }
+    __syncthreads();
+    if (S.stop) {
+      err = S.stop;
+      break;
+    }
+    ++passes;
+    int bgain = 0;            // best: smallest gain of this thread (strictly below 0 to count)
+    unsigned bidx = NO_IDX;   // and its scan index (first in thread order wins ties)
+    int cnt = 0, evals = 0;
+    int ri[U], rr[U], ee[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      ee[u] = u * THREADS + tid;
+      ri[u] = ee[u] / k;
+      rr[u] = ee[u] - ri[u] * k;
+    }
+    bool found = false;  // first: an earlier round holds an improving pair (block-uniform)
+    for (int e0 = 0; e0 < E; e0 += STEP) {
+      int a[U], c[U], cd[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) a[u] = ee[u] < E ? tour[ri[u]] : -1;
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        c[u] = -1;
+        if (a[u] < 0) continue;
+        const unsigned ar = (unsigned)a[u] * (unsigned)k + (unsigned)rr[u];
+        if (PACKED) {
+          const uint32_t w = __ldg(packed + ar);
+          c[u] = (int)(w & 0xffffu);
+          cd[u] = (int)(w >> 16);
+        } else {
+          c[u] = __ldg(cand + ar);
+          cd[u] = cdist ? __ldg(cdist + ar) : -1;
+        }
+      }
+      bool ok[U];
+      int sa[U], sc[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        ok[u] = false;
+        if ((unsigned)c[u] >= (unsigned)n) continue;
+        const int i = ri[u];
+        // j in (i + 1, lim): one unsigned range test
+        ok[u] = (unsigned)(pos[c[u]] - (i + 2)) < (unsigned)(n - (i == 0) - (i + 2));
+        cnt += ok[u];
+        if (MODE == TSPB_MODE_FIRST && found) ok[u] = false;
+        if (ok[u]) {
+          sa[u] = succ[a[u]];
+          sc[u] = succ[c[u]];
+        }
+      }
+      int dbd[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (ok[u]) dbd[u] = dist ? __ldg(dist + ((unsigned)sa[u] * stride + (unsigned)sc[u])) : ds(sa[u], sc[u]);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (!ok[u]) continue;
+        ++evals;
+        const int dac = (PACKED || cd[u] >= 0) ? cd[u] : ds(a[u], c[u]);
+        const int gain = (dac - eout[a[u]]) + (dbd[u] - eout[c[u]]);
+        if (MODE == TSPB_MODE_BEST) {
+          if (gain < bgain) {
+            bgain = gain;
+            bidx = (unsigned)ee[u];
+          }
+        } else if (gain < 0) {
+          atomicMin(&S.first, (unsigned)ee[u]);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        ee[u] += STEP;
+        rr[u] += sr;
+        ri[u] += sq;
+        if (rr[u] >= k) {
+          rr[u] -= k;
+          ++ri[u];
+        }
+      }
+      if (MODE == TSPB_MODE_FIRST && !found) {
+        __syncthreads();
+        found = S.first != NO_IDX;
+      }
+    }
+    my_pairs += cnt;
+    my_eval += evals;
+    unsigned idx;
+    if (MODE == TSPB_MODE_BEST) {
+      const unsigned long long key = bidx == NO_IDX ? NO_KEY : gain_key(bgain, bidx);
+      const unsigned long long best = block_min(key, S.red64);
+      if (best == NO_KEY) break;
+      idx = (unsigned)best;
+    } else {
+      __syncthreads();
+      idx = S.first;
+      if (idx == NO_IDX) break;
+    }
+    const int bi = (int)(idx / (unsigned)k);
+    const int br = (int)(idx - (unsigned)bi * (unsigned)k);
+    const unsigned bar = (unsigned)tour[bi] * (unsigned)k + (unsigned)br;
+    const int ca = PACKED ? (int)(__ldg(packed + bar) & 0xffffu) : __ldg(cand + bar);
+    const int bj = pos[ca];
+    if (bi < 0 || bj <= bi + 1 || bj >= n) {
+      err = TSPB_ERR_RANGE;
+      break;
+    }
+    __syncthreads();
+    {
+      const int lo = bi + 1, hi = bj, half = (hi - lo + 1) >> 1;
+      for (int q = tid; q < half; q += THREADS) {
+        const int x = tour[lo + q], y = tour[hi - q];
+        tour[lo + q] = y;
+        tour[hi - q] = x;
+        pos[y] = lo + q;
+        pos[x] = hi - q;
+      }
+    }
+    __syncthreads();
+    for (int p = bi + tid; p <= bj; p += THREADS) {
+      const int x = tour[p], y = tour[p + 1 == n ? 0 : p + 1];
+      succ[x] = y;
+      eout[x] = ds(x, y);
+    }
+    __syncthreads();
+    ++moves;
+  }
+
+  __syncthreads();
+  for (int p = tid; p < n; p += THREADS) g_tour[p] = tour[p];
+  const long long tp = block_sum(my_pairs, S.redll);
+  const long long te = block_sum(my_eval, S.redll);
+  if (tid == 0) {
+    if (A.status) A.status[t] = err;
+    if (A.stats) {
+      long long* st = A.stats + (long long)t * 4;
+      st[0] = passes;
+      st[1] = tp;
+      st[2] = moves;
+      st[3] = te;
+    }
+  }
+}
+
+size_t two_opt_scan_tour_bytes(int n) { return (size_t)16 * n; }
+
+template <int MODE, int THREADS, int U>
+static int launch_scan(const TwoOptArgs& a, size_t smem, cudaStream_t st) {
+  auto kern = a.cand_packed ? two_opt_scan_kernel<MODE, THREADS, U, true> : two_opt_scan_kernel<MODE, THREADS, U, false>;
+  if (smem > 48 * 1024) TSPB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<a.num_tours, THREADS, smem, st>>>(a);
+  return tspb_launch_status();
+}
+
+template <int MODE>
+static int launch_scan_mode(const TwoOptArgs& a, int threads, size_t smem, cudaStream_t st) {
+  switch (threads) {
+    case 64: return launch_scan<MODE, 64, 4>(a, smem, st);
+    case 128: return launch_scan<MODE, 128, 4>(a, smem, st);
+    case 512: return launch_scan<MODE, 512, 2>(a, smem, st);
+    default: return launch_scan<MODE, 256, 4>(a, smem, st);
+  }
+}
+
+int launch_two_opt_scan(const TwoOptArgs& a, int mode, int threads, cudaStream_t st) {
+  const size_t smem = a.arrays_in_smem ? two_opt_scan_tour_bytes(a.n) : 0;
+  if (mode == TSPB_MODE_BEST) return launch_scan_mode<TSPB_MODE_BEST>(a, threads, smem, st);
+  return launch_scan_mode<TSPB_MODE_FIRST>(a, threads, smem, st);
+}
+
+__global__ void cand_pack_kernel(const int32_t* __restrict__ cand, const int32_t* __restrict__ cd, long long total,
+                                 uint32_t* __restrict__ out, int32_t* __restrict__ overflow) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= total) return;
+  const int c = __ldg(cand + e), d = __ldg(cd + e);
+  if ((unsigned)c > 0xffffu || (unsigned)d > 0xffffu) {
+    atomicOr(overflow, 1);
+    out[e] = 0xffffu;  // an id >= n: the entry is skipped
+    return;
+  }
+  out[e] = (uint32_t)c | ((uint32_t)d << 16);
+}
+
+}  // namespace tspb
+
+using namespace tspb;
+
+extern "C" int tspb_candidate_pack(const int32_t* cand, const int32_t* cand_dist, int32_t n, int32_t k, uint32_t* packed,
+                                   int32_t* overflow, void* stream) {
+  if (n < 0 || k < 0) return TSPB_ERR_ARG;
+  if (!overflow || (n > 0 && k > 0 && (!cand || !cand_dist || !packed))) return TSPB_ERR_ARG;
+  if (n > 65535) return TSPB_ERR_UNSUPPORTED;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  TSPB_CUDA_CHECK(cudaMemsetAsync(overflow, 0, sizeof(int32_t), st));
+  const long long total = (long long)n * k;
+  if (total > 0) cand_pack_kernel<<<(int)((total + 255) / 256), 256, 0, st>>>(cand, cand_dist, total, packed, overflow);
+  return tspb_launch_status();
+}

@@ -60,6 +60,35 @@ def check_free(required_bytes: int, what: str) -> None:
     raise VRAMInsufficientError(f"Insufficient VRAM for {what}", required_bytes=required_bytes, available_bytes=free)
 
 
+class PinnedStager:
+  """Reusable page-locked host buffers for H2D inputs and D2H results."""
+
+  def __init__(self):
+    self._bufs: dict[str, "torch.Tensor"] = {}
+
+  def _buf(self, slot: str, nbytes: int):
+    b = self._bufs.get(slot)
+    if b is None or b.numel() < nbytes:
+      b = torch.empty(max(nbytes, 1), dtype=torch.uint8, pin_memory=True)
+      self._bufs[slot] = b
+    return b
+
+  def upload(self, a: np.ndarray, dtype) -> "torch.Tensor":
+    a = np.ascontiguousarray(a)
+    b = self._buf("in", a.nbytes)
+    host = b[: a.nbytes].view(dtype).reshape(a.shape)
+    host.numpy()[...] = a
+    return host.to("cuda", non_blocking=True)
+
+  def download(self, t: "torch.Tensor") -> np.ndarray:
+    nbytes = t.numel() * t.element_size()
+    b = self._buf("out", nbytes)
+    host = b[:nbytes].view(t.dtype).reshape(t.shape)
+    host.copy_(t, non_blocking=True)
+    torch.cuda.current_stream().synchronize()
+    return host.numpy().copy()
+
+
 class Workspace:
   """Monotonically growing device scratch buffer (grows, never shrinks)."""
 
@@ -77,6 +106,21 @@ class Workspace:
 
 #: Largest |distance| for which the kernels' int32 gain arithmetic is exact.
 MAX_DISTANCE = (1 << 30) - 1
+
+
+class CandidateTables:
+  """Device k-NN table, its distances and its reverse index (CSR)."""
+
+  def __init__(self, cand, cand_dist, rev_off, rev_idx, packed=None):
+    self.cand = cand
+    self.cand_dist = cand_dist
+    self.rev_off = rev_off
+    self.rev_idx = rev_idx
+    self.packed = packed
+
+  @property
+  def k(self) -> int:
+    return int(self.cand.shape[1])
 
 
 class DeviceOperands:
@@ -138,11 +182,11 @@ class DeviceOperands:
     return d, int(d.shape[1]), None
 
   def candidates(self, k: int, table: np.ndarray, n: int, max_matrix_dimension: int | None = None):
-    """Device `(cand, cand_dist)` for a host k-NN table (cached per k and table identity)."""
+    """Device `CandidateTables` for a host k-NN table (cached per k and table identity)."""
     key = int(k)
     hit = self._cand.get(key)
     if hit is not None and hit[0] is table:
-      return hit[1], hit[2]
+      return hit[1]
     from .native import call
 
     tab = np.ascontiguousarray(table, dtype=np.int32)
@@ -150,11 +194,23 @@ class DeviceOperands:
     self.h2d_bytes += tab.nbytes
     rows, kk = tab.shape
     d_cd = torch.empty((rows, kk), dtype=torch.int32, device="cuda")
+    rev_off = torch.empty(rows + 1, dtype=torch.int32, device="cuda")
+    rev_idx = torch.empty(max(rows * kk, 1), dtype=torch.int32, device="cuda")
+    scratch = torch.empty(max(rows, 1), dtype=torch.int32, device="cuda")
     dist, stride, coords = self.distance_args(n, max_matrix_dimension)
     if rows and kk:
       call("tspb_candidate_distances", ptr(d_cand), rows, kk, ptr(dist), stride, ptr(coords), ptr(d_cd), stream_handle())
-    self._cand[key] = (table, d_cand, d_cd)
-    return d_cand, d_cd
+      call("tspb_candidate_reverse_index", ptr(d_cand), rows, kk, ptr(rev_off), ptr(rev_idx), ptr(scratch), stream_handle())
+    packed = None
+    if rows and kk and rows <= 0xFFFF:
+      packed = torch.empty((rows, kk), dtype=torch.int32, device="cuda")
+      overflow = torch.zeros(1, dtype=torch.int32, device="cuda")
+      call("tspb_candidate_pack", ptr(d_cand), ptr(d_cd), rows, kk, ptr(packed), ptr(overflow), stream_handle())
+      if int(overflow.item()) != 0:
+        packed = None
+    tables = CandidateTables(d_cand, d_cd, rev_off, rev_idx, packed)
+    self._cand[key] = (table, tables)
+    return tables
 
 
 _operands: "weakref.WeakKeyDictionary[Any, DeviceOperands]" = weakref.WeakKeyDictionary()

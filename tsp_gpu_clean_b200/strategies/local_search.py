@@ -21,10 +21,10 @@ from typing import Any
 import numpy as np
 
 from .. import native
-from ..device import Workspace, operands_for, ptr, require_gpu, stream_handle, torch
+from ..device import PinnedStager, Workspace, operands_for, ptr, require_gpu, stream_handle, torch
 from ..errors import NotPermutationError
 from ..phase_timer import time_strategy
-from ..routes import ensure_routes_batch, restore_shape, to_device_routes
+from ..routes import ensure_routes_batch, restore_shape
 from .base import StrategyBase
 
 MODES = frozenset({"best", "first", "multi_move", "batch"})
@@ -60,8 +60,13 @@ class LocalSearchB200TourTwoOpt(StrategyBase):
     self.threads_per_block = threads_per_block
     self.max_matrix_dimension = max_matrix_dimension
     self.collect_stats = True
+    #: candidate best/first kernel: "scan" (full rescan, packed k-NN words), "scan_unpacked"
+    #: (same kernel, separate id/distance arrays) or "cached" (exact incremental row keys).
+    #: All give identical results; the choice is a performance knob.
+    self.kernel = "scan"
     self.last_stats: np.ndarray | None = None
     self._workspace = Workspace()
+    self._stager = PinnedStager()
 
   def _warmup_impl(self, context: Any) -> None:
     self.improve_batch(self._warmup_batch(context, rows=1), context)
@@ -101,27 +106,34 @@ class LocalSearchB200TourTwoOpt(StrategyBase):
     ops = operands_for(context)
     before = ops.h2d_bytes
     dist, stride, coords = ops.distance_args(n, self.max_matrix_dimension)
-    cand = cand_dist = None
+    tabs = None
     k = 0
     if table is not None:
-      cand, cand_dist = ops.candidates(int(self.candidate_k), table, n, self.max_matrix_dimension)
-      k = int(cand.shape[1])
+      tabs = ops.candidates(int(self.candidate_k), table, n, self.max_matrix_dimension)
+      k = tabs.k
       if k == 0:
-        cand = cand_dist = None
+        tabs = None
     self.h2d_bytes += ops.h2d_bytes - before
 
     if on_device:
       d_tours = batch.to(torch.int32).contiguous().clone()
     else:
-      d_tours, _ = to_device_routes(host)
+      d_tours = self._stager.upload(host, torch.int32)
       self.h2d_bytes += host.nbytes
     mode = native.MODE_CODES[self.mode]
     ws_bytes = native.load_library().tspb_two_opt_workspace_bytes(num, n, k, mode, self.threads_per_block)
     ws = self._workspace.get(int(ws_bytes))
     stats = torch.empty((num, 4), dtype=torch.int64, device="cuda") if self.collect_stats else None
     status = torch.empty(num, dtype=torch.int32, device="cuda")
+    cand = tabs.cand if tabs is not None else None
+    cand_dist = tabs.cand_dist if tabs is not None else None
+    cached = tabs is not None and self.kernel == "cached"
+    rev_off = tabs.rev_off if cached else None
+    rev_idx = tabs.rev_idx if cached else None
+    packed = tabs.packed if tabs is not None and self.kernel == "scan" else None
     native.call(
-      "tspb_two_opt", ptr(d_tours), num, n, ptr(dist), stride, ptr(coords), ptr(cand), ptr(cand_dist), k, mode,
+      "tspb_two_opt", ptr(d_tours), num, n, ptr(dist), stride, ptr(coords), ptr(cand), ptr(cand_dist), ptr(rev_off),
+      ptr(rev_idx), ptr(packed), k, mode,
       int(self.max_iterations), int(self.threads_per_block), ptr(stats), ptr(status), ptr(ws), int(ws_bytes),
       stream_handle(),
     )
@@ -134,6 +146,6 @@ class LocalSearchB200TourTwoOpt(StrategyBase):
     self.last_stats = stats.cpu().numpy() if stats is not None else None
     if on_device:
       return restore_shape(d_tours, was_1d)
-    out = d_tours.cpu().numpy()
+    out = self._stager.download(d_tours)
     self.d2h_bytes += out.nbytes
     return restore_shape(out, was_1d)
