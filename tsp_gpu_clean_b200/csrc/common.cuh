@@ -30,13 +30,15 @@ __device__ __forceinline__ int euc2d(const double2 p, const double2 q) {
   return (int)(long long)__dadd_rn(__dsqrt_rn(s), 0.5);
 }
 
-// Distance source: a dense int32 matrix or on-the-fly FP64 coordinates.
+// Distance source: a dense int32 matrix or on-the-fly FP64 coordinates. Matrix reads
+// are random gathers with no reuse inside an SM, so they bypass L1 (ld.global.cg) and
+// leave L1 to the per-instance k-NN tables.
 struct DistSrc {
   const int32_t* dist;
   long long stride;
   const double2* coords;
   __device__ __forceinline__ int operator()(int a, int b) const {
-    if (dist != nullptr) return __ldg(dist + (long long)a * stride + b);
+    if (dist != nullptr) return __ldcg(dist + (long long)a * stride + b);
     return euc2d(__ldg(coords + a), __ldg(coords + b));
   }
 };

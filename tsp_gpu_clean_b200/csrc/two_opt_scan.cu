@@ -22,6 +22,7 @@ namespace tspb {
 struct ScanSmem {
   unsigned long long red64[32];
   long long redll[32];
+  long long total;  // first: valid entries of the current tour (kept exact across passes)
   unsigned first;
   int bad;
   int stop;
@@ -46,6 +47,7 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value) two_op
   int* pos = tour + n;
   int* succ = pos + n;
   int* eout = succ + n;
+  int* rcnt = eout + n;  // first: valid entries per row (position), n ints
   const DistSrc ds = A.ds;
   const uint32_t* __restrict__ packed = A.cand_packed;
   const int32_t* __restrict__ cand = A.cand;
@@ -56,6 +58,7 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value) two_op
   if (tid == 0) {
     S.bad = 0;
     S.stop = 0;
+    S.total = 0;
   }
   for (int p = tid; p < n; p += THREADS) {
     tour[p] = g_tour[p];
@@ -82,6 +85,36 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value) two_op
   }
   __syncthreads();
 
+  // Valid entries of row i (the pairs the reference scan evaluates for that row).
+  auto row_count = [&](int i) -> int {
+    const int a = tour[i];
+    const int lo = i + 2, span = n - (i == 0) - lo;
+    int c = 0;
+    for (int r0 = 0; r0 < k; r0 += 4) {
+      int cc[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const unsigned ar = (unsigned)a * (unsigned)k + (unsigned)(r0 + u);
+        cc[u] = r0 + u < k ? (PACKED ? (int)(__ldg(packed + ar) & 0xffffu) : __ldg(cand + ar)) : -1;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if ((unsigned)cc[u] < (unsigned)n) c += (unsigned)(pos[cc[u]] - lo) < (unsigned)span;
+    }
+    return c;
+  };
+  if (MODE == TSPB_MODE_FIRST) {
+    long long sum = 0;
+    for (int i = tid; i < n; i += THREADS) {
+      const int v = i < rows ? row_count(i) : 0;
+      rcnt[i] = v;
+      sum += v;
+    }
+    sum = warp_sum(sum);
+    if ((tid & 31) == 0) atomicAdd(reinterpret_cast<unsigned long long*>(&S.total), (unsigned long long)sum);
+    __syncthreads();
+  }
+
   const int E = rows * k;
   constexpr int STEP = THREADS * U;
   const int sq = STEP / k, sr = STEP - (STEP / k) * k;
@@ -100,6 +133,7 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value) two_op
       break;
     }
     ++passes;
+    if (MODE == TSPB_MODE_FIRST && tid == 0) my_pairs += S.total;
     int bgain = 0;            // best: smallest gain of this thread (strictly below 0 to count)
     unsigned bidx = NO_IDX;   // and its scan index (first in thread order wins ties)
     int cnt = 0, evals = 0;
@@ -110,7 +144,6 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value) two_op
       ri[u] = ee[u] / k;
       rr[u] = ee[u] - ri[u] * k;
     }
-    bool found = false;  // first: an earlier round holds an improving pair (block-uniform)
     for (int e0 = 0; e0 < E; e0 += STEP) {
       int a[U], c[U], cd[U];
 #pragma unroll
@@ -138,8 +171,7 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value) two_op
         const int i = ri[u];
         // j in (i + 1, lim): one unsigned range test
         ok[u] = (unsigned)(pos[c[u]] - (i + 2)) < (unsigned)(n - (i == 0) - (i + 2));
-        cnt += ok[u];
-        if (MODE == TSPB_MODE_FIRST && found) ok[u] = false;
+        if (MODE == TSPB_MODE_BEST) cnt += ok[u];
         if (ok[u]) {
           sa[u] = succ[a[u]];
           sc[u] = succ[c[u]];
@@ -148,7 +180,7 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value) two_op
       int dbd[U];
 #pragma unroll
       for (int u = 0; u < U; ++u)
-        if (ok[u]) dbd[u] = dist ? __ldg(dist + ((unsigned)sa[u] * stride + (unsigned)sc[u])) : ds(sa[u], sc[u]);
+        if (ok[u]) dbd[u] = dist ? __ldcg(dist + ((unsigned)sa[u] * stride + (unsigned)sc[u])) : ds(sa[u], sc[u]);
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         if (!ok[u]) continue;
@@ -174,9 +206,9 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value) two_op
           ++ri[u];
         }
       }
-      if (MODE == TSPB_MODE_FIRST && !found) {
+      if (MODE == TSPB_MODE_FIRST) {
         __syncthreads();
-        found = S.first != NO_IDX;
+        if (S.first != NO_IDX) break;
       }
     }
     my_pairs += cnt;
@@ -220,6 +252,21 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value) two_op
     }
     __syncthreads();
     ++moves;
+    if (MODE == TSPB_MODE_FIRST) {
+      // Only rows [bi, bj] (and row 0 when bj == n-1) can change their valid count.
+      const int r_hi = bj < rows - 1 ? bj : rows - 1;
+      const bool row0 = bj == n - 1 && bi > 0;
+      const int nr = r_hi - bi + 1 + (row0 ? 1 : 0);
+      long long d = 0;
+      for (int q = tid; q < nr; q += THREADS) {
+        const int i = q < r_hi - bi + 1 ? bi + q : 0;
+        const int v = row_count(i);
+        d += v - rcnt[i];
+        rcnt[i] = v;
+      }
+      d = warp_sum(d);
+      if ((tid & 31) == 0 && d != 0) atomicAdd(reinterpret_cast<unsigned long long*>(&S.total), (unsigned long long)d);
+    }
   }
 
   __syncthreads();
@@ -238,12 +285,33 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value) two_op
   }
 }
 
-size_t two_opt_scan_tour_bytes(int n) { return (size_t)16 * n; }
+size_t two_opt_scan_tour_bytes(int n) { return (size_t)20 * n; }
+
+// Shared-memory carveout (percent of the unified L1/shared array) that holds exactly the
+// CTAs this launch keeps resident per SM; the rest stays L1 for the k-NN tables. The
+// default lets the driver take the largest split, which leaves too little L1.
+static int carveout_percent(int num_tours, size_t smem_per_cta, int max_ctas_per_sm) {
+  static int sms = 0, smem_sm = 0;
+  if (sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  }
+  if (sms <= 0 || smem_sm <= 0) return -1;
+  int per_sm = (num_tours + sms - 1) / sms;
+  if (per_sm > max_ctas_per_sm) per_sm = max_ctas_per_sm;
+  const long long need = (long long)per_sm * (long long)(smem_per_cta + sizeof(ScanSmem) + 1024);
+  int pct = (int)((need * 100 + smem_sm - 1) / smem_sm);
+  return pct < 1 ? 1 : (pct > 100 ? 100 : pct);
+}
 
 template <int MODE, int THREADS, int U>
 static int launch_scan(const TwoOptArgs& a, size_t smem, cudaStream_t st) {
   auto kern = a.cand_packed ? two_opt_scan_kernel<MODE, THREADS, U, true> : two_opt_scan_kernel<MODE, THREADS, U, false>;
   if (smem > 48 * 1024) TSPB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int pct = carveout_percent(a.num_tours, smem, ScanMinBlocks<THREADS>::value);
+  if (pct > 0) TSPB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
   kern<<<a.num_tours, THREADS, smem, st>>>(a);
   return tspb_launch_status();
 }
