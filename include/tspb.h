@@ -75,6 +75,30 @@ int tspb_two_opt(int32_t* tours, int32_t num_tours, int32_t n,
                  void* workspace, size_t workspace_bytes, void* stream);
 
 /*
+ * multi_move 2-opt (same kernel and results as tspb_two_opt with TSPB_MODE_MULTI_MOVE)
+ * that allocates nothing: its scratch is a fixed TSPB_STATIC_SCRATCH_BYTES array compiled
+ * into the library, which every GPU that loads the library holds until exit. No
+ * counterpart in the reference. It is for callers that cannot call cudaMalloc, such as
+ * code running inside a host callback or a latency-critical loop that must stay off the
+ * allocator, or a plugin host that owns all device memory and passes in only the input
+ * and output buffers. The caller still provides tours, distances, candidates and the
+ * optional stats/status buffers.
+ *   - Returns TSPB_ERR_WORKSPACE when the shape needs more scratch than the array holds
+ *     (tspb_two_opt_workspace_bytes(num_tours, n, k, TSPB_MODE_MULTI_MOVE, threads) >
+ *     TSPB_STATIC_SCRATCH_BYTES); split the batch into smaller calls then.
+ *   - The first call on a device looks up the array's device address (set-up, once per
+ *     device, with that device current); make that first call before any stream capture.
+ *   - All calls share the array: calls whose kernels overlap on the GPU race on it and
+ *     must be serialised by the caller.
+ */
+#define TSPB_STATIC_SCRATCH_BYTES (32u << 20)
+int tspb_two_opt_multi_move_static(int32_t* tours, int32_t num_tours, int32_t n,
+                                   const int32_t* dist, int64_t dist_stride, const double* coords,
+                                   const int32_t* cand, const int32_t* cand_dist, int32_t k,
+                                   int64_t max_iterations, int32_t block_threads,
+                                   int64_t* stats, int32_t* status, void* stream);
+
+/*
  * cand_dist[a*k + r] = d(a, cand[a*k + r]) for the n x k table (entries outside [0, n)
  * give 0). Replaces the D[a, c] gathers of _pair_deltas (two_opt.py:242) with a table
  * built once per instance.

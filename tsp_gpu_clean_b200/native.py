@@ -40,6 +40,7 @@ SIGNATURES: dict[str, tuple] = {
   "tspb_two_opt_workspace_bytes": (_sz, [_i32, _i32, _i32, _i32, _i32]),
   "tspb_two_opt": (ctypes.c_int, [_p, _i32, _i32, _p, _i64, _p, _p, _p, _p, _p, _p, _i32, _i32, _i64, _i32, _p, _p, _p, _sz, _p]),
   "tspb_candidate_pack": (ctypes.c_int, [_p, _p, _i32, _i32, _p, _p, _p]),
+  "tspb_two_opt_multi_move_static": (ctypes.c_int, [_p, _i32, _i32, _p, _i64, _p, _p, _p, _i32, _i64, _i32, _p, _p, _p]),
   "tspb_candidate_reverse_index": (ctypes.c_int, [_p, _i32, _i32, _p, _p, _p, _p]),
   "tspb_candidate_distances": (ctypes.c_int, [_p, _i32, _i32, _p, _i64, _p, _p, _p]),
   "tspb_tour_cost": (ctypes.c_int, [_p, _i32, _i32, _p, _i64, _p, _i32, _p, _p]),
