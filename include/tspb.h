@@ -147,6 +147,12 @@ int tspb_tournament(const double* fitness, int32_t pop_size, const int32_t* cand
 int tspb_gather_rows(const int32_t* src, int32_t src_rows, int32_t n, const int32_t* rows,
                      int32_t num_rows, int32_t* out, void* stream);
 
+/* dst[rows[r], :] = src[r, :] for r < num_rows (rows outside [0, dst_rows) skipped).
+ * Replaces the elite scatter-back `state.population[elite_indices] = improved`
+ * (src/algorithms/pipeline_steps.py:183). */
+int tspb_scatter_rows(const int32_t* src, int32_t num_rows, int32_t n, const int32_t* rows, int32_t* dst,
+                      int32_t dst_rows, void* stream);
+
 /*
  * PMX crossover of pairs (2q, 2q+1) sharing cuts (first[q], second[q]); the odd tail
  * row is copied. Open permutations (bounds [0, n)). Replaces
@@ -174,6 +180,18 @@ int tspb_inversion(int32_t* routes, int32_t num_routes, int32_t n, const double*
  *   (src/algorithms/metaheuristics/genetic_algorithm.py:618-706, lexsort :682-689).
  */
 int tspb_stable_rank(const double* fitness, int32_t count, int32_t keep, int32_t* order, void* stream);
+
+/*
+ * GRASP nearest-neighbour initial population, one thread per row: row r starts from the
+ * SplitMix64 stream seeded with seeds[r] and walks the k-NN table of `cand` (cand_rows x k).
+ * `workspace` holds pop * (n + max_node + 1 + k) int32. Replaces
+ *   InitializationCPUTourNearestNeighbor.initialize / _nearest_neighbor_row_cpu
+ *   (src/algorithms/strategies/initialization/nearest_neighbor_init.py:31-132) and
+ *   nearest_neighbor_init_kernel (.../initialization/kernels/nearest_neighbor_init.cu:10-111).
+ */
+int tspb_nn_init(const int32_t* customers, int32_t n, const int32_t* cand, int32_t cand_rows, int32_t k,
+                 const uint64_t* seeds, int32_t pop, int32_t max_node, int32_t* workspace,
+                 size_t workspace_bytes, int32_t* out, void* stream);
 
 /*
  * Permutation check: bad[r] = 0 when row r is a permutation of 0..n-1, else 1.

@@ -1,0 +1,150 @@
+"""Population operators on the B200 against the reference's golden outputs and the oracle."""
+
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+import pytest
+
+from oracle import distances as odist
+from oracle import ga_ops
+from tsp_gpu_clean_b200 import instances
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch_mod():
+  import torch
+
+  if not torch.cuda.is_available():
+    pytest.skip("no CUDA device")
+  from tsp_gpu_clean_b200.build import build_library
+
+  build_library()
+  return torch
+
+
+def _ctx(coords, seed):
+  from tsp_gpu_clean_b200.problem import Problem, ProblemContext
+
+  return ProblemContext(Problem.from_coordinates(coords), seed=seed)
+
+
+@pytest.mark.parametrize("tag", ["a", "b", "c", "d"])
+@pytest.mark.parametrize("resident", [False, True])
+def test_operators_match_reference(torch_mod, golden, tag, resident):
+  from tsp_gpu_clean_b200.strategies import (
+    CrossoverB200PermPartiallyMapped,
+    EvaluationB200Cost,
+    MutationB200PermInversion,
+    SelectionB200Tournament,
+  )
+
+  ops = golden("ops.npz")
+  n, pop_size, seed = (int(v) for v in ops[f"{tag}_meta"])
+  ctx = _ctx(ops[f"{tag}_coords"], seed)
+  pop = ops[f"{tag}_pop"]
+  ev = EvaluationB200Cost(return_gpu=resident)
+  x = torch_mod.from_numpy(pop).cuda() if resident else pop
+  fit = ev.assess_batch(x, ctx, return_gpu=resident).objectives
+  assert np.array_equal(fit.cpu().numpy() if resident else fit, ops[f"{tag}_fit"])
+  sel = SelectionB200Tournament(k=5, seed=1).select_batch(x, fit, pop_size, ctx)
+  pmx = CrossoverB200PermPartiallyMapped(seed=1).crossover_batch(sel, ctx)
+  inv = MutationB200PermInversion(seed=1).mutate_batch(pmx, float(ops[f"{tag}_rate"]), ctx)
+  host = (lambda t: t.cpu().numpy()) if resident else (lambda t: t)
+  assert np.array_equal(host(sel), ops[f"{tag}_sel"])
+  assert np.array_equal(host(pmx), ops[f"{tag}_pmx"])
+  assert np.array_equal(host(inv), ops[f"{tag}_inv"])
+  assert ctx.rng.bit_generator.state["state"]["state"] % (1 << 63) == int(ops[f"{tag}_rng_state"][0])
+
+
+def test_pmx_and_inversion_random_vs_oracle(torch_mod):
+  from tsp_gpu_clean_b200 import native
+  from tsp_gpu_clean_b200.device import ptr, stream_handle
+
+  torch = torch_mod
+  rng = np.random.default_rng(5)
+  for n in (2, 3, 7, 64, 1000, 4099):
+    pop = instances.random_tours(n, 33, n)
+    pairs = ga_ops.sample_distinct_pairs(rng, 16, 0, n) if n >= 2 else None
+    want = ga_ops.pmx_apply(pop, pairs)
+    d = torch.from_numpy(pop).cuda()
+    out = torch.empty_like(d)
+    st = torch.zeros(33, dtype=torch.int32, device="cuda")
+    f = torch.from_numpy(pairs[:, 0].copy()).cuda()
+    s = torch.from_numpy(pairs[:, 1].copy()).cuda()
+    native.call("tspb_pmx", ptr(d), 33, n, ptr(f), ptr(s), ptr(out), ptr(st), stream_handle())
+    assert np.array_equal(out.cpu().numpy(), want), n
+    u = rng.random(33)
+    u[:5] = 0.0
+    p1 = rng.integers(0, n, 33).astype(np.int32)
+    p2 = rng.integers(0, n, 33).astype(np.int32)
+    want = ga_ops.inversion_apply(pop, 0.5, u, p1, p2)
+    d = torch.from_numpy(pop).cuda()
+    du, d1, d2 = torch.from_numpy(u).cuda(), torch.from_numpy(p1).cuda(), torch.from_numpy(p2).cuda()
+    native.call("tspb_inversion", ptr(d), 33, n, ptr(du), 0.5, ptr(d1), ptr(d2), stream_handle())
+    assert np.array_equal(d.cpu().numpy(), want), n
+
+
+def test_stable_rank_and_validation(torch_mod):
+  from tsp_gpu_clean_b200 import native
+  from tsp_gpu_clean_b200.device import ptr, stream_handle
+
+  torch = torch_mod
+  rng = np.random.default_rng(9)
+  for count in (1, 5, 256, 1024, 3000):
+    f = rng.integers(0, 20, count).astype(np.float64)  # heavy ties
+    keep = max(1, count // 2)
+    order = torch.empty(keep, dtype=torch.int32, device="cuda")
+    df = torch.from_numpy(f).cuda()
+    native.call("tspb_stable_rank", ptr(df), count, keep, ptr(order), stream_handle())
+    z = np.zeros_like(f)
+    assert np.array_equal(order.cpu().numpy(), np.lexsort(np.vstack([f, z, z]))[:keep])
+  tours = instances.random_tours(50, 6, 3)
+  tours[2, 5] = tours[2, 6]
+  tours[4, 0] = 50
+  bad = torch.empty(6, dtype=torch.int32, device="cuda")
+  dt = torch.from_numpy(tours).cuda()
+  native.call("tspb_validate_perm", ptr(dt), 6, 50, ptr(bad), stream_handle())
+  assert bad.cpu().numpy().tolist() == [0, 0, 1, 0, 1, 0]
+
+
+def test_euc2d_matrix_and_costs_match_reference(torch_mod, golden):
+  from tsp_gpu_clean_b200 import native
+  from tsp_gpu_clean_b200.device import ptr, stream_handle
+
+  torch = torch_mod
+  ops = golden("ops.npz")
+  for coords, expect in ((ops["dist_coords"], ops["dist_matrix"]), (ops["big_coords"], None)):
+    n = len(coords)
+    d = torch.empty((n, n), dtype=torch.int32, device="cuda")
+    dc = torch.from_numpy(np.ascontiguousarray(coords)).cuda()
+    native.call("tspb_euc2d_matrix", ptr(dc), n, ptr(d), n, stream_handle())
+    got = d.cpu().numpy()
+    if expect is not None:
+      assert np.array_equal(got, expect)
+    else:
+      assert hashlib.sha256(got.tobytes()).digest() == ops["big_digest"].tobytes()
+  # tour costs from the matrix and from rebuilt FP64 distances agree with the oracle
+  coords = ops["big_coords"]
+  tours = instances.random_tours(len(coords), 8, 4)
+  want = ga_ops.tour_cost(tours, odist.euc2d_matrix(coords))
+  from tsp_gpu_clean_b200.strategies import EvaluationB200Cost
+
+  ctx = _ctx(coords, 0)
+  assert np.array_equal(EvaluationB200Cost().evaluate_batch(tours, ctx), want)
+  assert np.array_equal(EvaluationB200Cost(max_matrix_dimension=100).evaluate_batch(tours, ctx), want)
+
+
+def test_nn_init_matches_reference(torch_mod, golden):
+  from tsp_gpu_clean_b200.strategies import InitializationB200TourNearestNeighbor
+
+  g = golden("ga.npz")
+  ctx = _ctx(g["c1_coords"], 42)
+  pop = InitializationB200TourNearestNeighbor(k=5, seed=42).initialize(list(range(100)), 128, ctx)
+  assert np.array_equal(pop, g["c1_init"])
+  ctx3 = _ctx(g["c3_coords"], 42)
+  pop3 = InitializationB200TourNearestNeighbor(k=5, seed=42, return_gpu=True).initialize(list(range(2000)), 512, ctx3)
+  assert hashlib.sha256(pop3.cpu().numpy().astype(np.int32).tobytes()).hexdigest() == str(g["c3_init_digest"])

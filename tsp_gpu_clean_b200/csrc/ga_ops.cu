@@ -75,6 +75,16 @@ __global__ void gather_rows_kernel(const int32_t* __restrict__ src, int src_rows
   }
 }
 
+// CTA per source row: dst[rows[r], :] = src[r, :] (the elite scatter-back).
+__global__ void scatter_rows_kernel(const int32_t* __restrict__ src, int n, const int32_t* __restrict__ rows, int dst_rows,
+                                    int32_t* __restrict__ dst) {
+  const int r = blockIdx.x;
+  const int dr = __ldg(rows + r);
+  if ((unsigned)dr >= (unsigned)dst_rows) return;
+  const long long s = (long long)r * n, d = (long long)dr * n;
+  for (int q = threadIdx.x; q < n; q += blockDim.x) dst[d + q] = __ldg(src + s + q);
+}
+
 // CTA per child. Child 2q+h takes p1 = parents[2q+h], p2 = parents[2q+1-h] and the
 // shared cuts; the mapping chains of values p2[c1..c2] that are not in p1[c1..c2] are
 // independent, so they run one per thread (_apply_pmx, pmx_crossover.py:49-105).
@@ -273,6 +283,15 @@ extern "C" int tspb_gather_rows(const int32_t* src, int32_t src_rows, int32_t n,
   if (num_rows == 0 || n == 0) return TSPB_OK;
   if (!src || !rows || !out) return TSPB_ERR_ARG;
   gather_rows_kernel<<<num_rows, 128, 0, reinterpret_cast<cudaStream_t>(stream)>>>(src, src_rows, n, rows, out);
+  return tspb_launch_status();
+}
+
+extern "C" int tspb_scatter_rows(const int32_t* src, int32_t num_rows, int32_t n, const int32_t* rows, int32_t* dst,
+                                 int32_t dst_rows, void* stream) {
+  if (num_rows < 0 || n < 0 || dst_rows < 0) return TSPB_ERR_ARG;
+  if (num_rows == 0 || n == 0) return TSPB_OK;
+  if (!src || !rows || !dst) return TSPB_ERR_ARG;
+  scatter_rows_kernel<<<num_rows, 128, 0, reinterpret_cast<cudaStream_t>(stream)>>>(src, n, rows, dst_rows, dst);
   return tspb_launch_status();
 }
 

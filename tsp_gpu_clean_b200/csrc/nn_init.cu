@@ -1,0 +1,102 @@
+// GRASP nearest-neighbour initial tours, one thread per row, bit-identical to the
+// reference's `_nearest_neighbor_row_cpu`
+// (src/algorithms/strategies/initialization/nearest_neighbor_init.py:31-99) with the
+// SplitMix64 stream of src/utils/splitmix64.py:38-51:
+//   - the start city is unvisited[bounded(rem)], swapped to the end of the unvisited list;
+//   - each next city is the first still-unvisited candidate met by an incremental
+//     Fisher-Yates shuffle of the current city's k-NN ranks (one bounded draw per rank
+//     tried), else a uniform unvisited city.
+// Each row needs n + (max_node + 1) + k ints of workspace (unvisited list, its inverse
+// map, the shuffled ranks).
+#include "common.cuh"
+
+namespace tspb {
+
+__device__ __forceinline__ unsigned long long splitmix64_bounded(unsigned long long& state, unsigned bound) {
+  state += 0x9E3779B97F4A7C15ull;
+  unsigned long long z = state;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z = z ^ (z >> 31);
+  return ((z >> 32) * (unsigned long long)bound) >> 32;
+}
+
+__global__ void nn_init_kernel(const int32_t* __restrict__ customers, int n, const int32_t* __restrict__ cand, int cand_rows,
+                               int k, const unsigned long long* __restrict__ seeds, int pop, int max_node,
+                               int32_t* __restrict__ ws, int32_t* __restrict__ out) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= pop) return;
+  const long long per = (long long)n + (max_node + 1) + k;
+  int32_t* unv = ws + (long long)row * per;
+  int32_t* pmap = unv + n;
+  int32_t* order = pmap + (max_node + 1);
+  int32_t* dst = out + (long long)row * n;
+  for (int q = 0; q <= max_node; ++q) pmap[q] = -1;
+  for (int q = 0; q < n; ++q) {
+    const int c = __ldg(customers + q);
+    unv[q] = c;
+    pmap[c] = q;
+  }
+  unsigned long long st = seeds[row];
+  int rem = n;
+  int s = (int)splitmix64_bounded(st, (unsigned)rem);
+  int cur = unv[s];
+  dst[0] = cur;
+  int last = rem - 1;
+  int ln = unv[last];
+  unv[s] = ln;
+  unv[last] = cur;
+  pmap[ln] = s;
+  pmap[cur] = last;
+  rem = last;
+  for (int step = 1; step < n; ++step) {
+    int chosen = -1;
+    if (cur >= 0 && cur < cand_rows && k > 0) {
+      for (int i = 0; i < k; ++i) order[i] = i;
+      const int32_t* crow = cand + (long long)cur * k;
+      for (int i = 0; i < k; ++i) {
+        const int j = i + (int)splitmix64_bounded(st, (unsigned)(k - i));
+        const int tmp = order[i];
+        order[i] = order[j];
+        order[j] = tmp;
+        const int nb = __ldg(crow + order[i]);
+        if (nb >= 0 && nb <= max_node) {
+          const int p = pmap[nb];
+          if (p >= 0 && p < rem) {
+            chosen = nb;
+            break;
+          }
+        }
+      }
+    }
+    if (chosen < 0) chosen = unv[(int)splitmix64_bounded(st, (unsigned)rem)];
+    dst[step] = chosen;
+    const int p = pmap[chosen];
+    last = rem - 1;
+    ln = unv[last];
+    unv[p] = ln;
+    unv[last] = chosen;
+    pmap[ln] = p;
+    pmap[chosen] = last;
+    rem = last;
+    cur = chosen;
+  }
+}
+
+}  // namespace tspb
+
+using namespace tspb;
+
+extern "C" int tspb_nn_init(const int32_t* customers, int32_t n, const int32_t* cand, int32_t cand_rows, int32_t k,
+                            const uint64_t* seeds, int32_t pop, int32_t max_node, int32_t* workspace,
+                            size_t workspace_bytes, int32_t* out, void* stream) {
+  if (n < 0 || pop < 0 || k < 0 || cand_rows < 0 || max_node < -1) return TSPB_ERR_ARG;
+  if (pop == 0 || n == 0) return TSPB_OK;
+  if (!customers || !seeds || !out || !workspace || (k > 0 && !cand)) return TSPB_ERR_ARG;
+  const size_t need = (size_t)pop * ((size_t)n + (size_t)(max_node + 1) + (size_t)k) * sizeof(int32_t);
+  if (workspace_bytes < need) return TSPB_ERR_WORKSPACE;
+  const int threads = 64;
+  nn_init_kernel<<<(pop + threads - 1) / threads, threads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+      customers, n, cand, cand_rows, k, reinterpret_cast<const unsigned long long*>(seeds), pop, max_node, workspace, out);
+  return tspb_launch_status();
+}

@@ -47,10 +47,12 @@ SIGNATURES: dict[str, tuple] = {
   "tspb_tournament": (ctypes.c_int, [_p, _i32, _p, _i32, _i32, _p, _p]),
   "tspb_gather_rows": (ctypes.c_int, [_p, _i32, _i32, _p, _i32, _p, _p]),
   "tspb_pmx": (ctypes.c_int, [_p, _i32, _i32, _p, _p, _p, _p, _p]),
+  "tspb_scatter_rows": (ctypes.c_int, [_p, _i32, _i32, _p, _p, _i32, _p]),
   "tspb_inversion": (ctypes.c_int, [_p, _i32, _i32, _p, _f64, _p, _p, _p]),
   "tspb_stable_rank": (ctypes.c_int, [_p, _i32, _i32, _p, _p]),
   "tspb_validate_perm": (ctypes.c_int, [_p, _i32, _i32, _p, _p]),
   "tspb_euc2d_matrix": (ctypes.c_int, [_p, _i32, _p, _i64, _p]),
+  "tspb_nn_init": (ctypes.c_int, [_p, _i32, _p, _i32, _i32, _p, _i32, _i32, _p, _sz, _p, _p]),
 }
 
 _lock = threading.Lock()
