@@ -75,6 +75,20 @@ int tspb_two_opt(int32_t* tours, int32_t num_tours, int32_t n,
                  void* workspace, size_t workspace_bytes, void* stream);
 
 /*
+ * tspb_two_opt that becomes a no-op on the device when *skip (device int32) is non-zero
+ * at launch time: tours, stats and status are then left untouched. Lets a captured CUDA
+ * graph of GA generations stop refining once the run's stop flag is set. No reference
+ * counterpart (the reference loop stops on the host).
+ */
+int tspb_two_opt_gated(const int32_t* skip, int32_t* tours, int32_t num_tours, int32_t n,
+                       const int32_t* dist, int64_t dist_stride, const double* coords,
+                       const int32_t* cand, const int32_t* cand_dist,
+                       const int32_t* rev_off, const int32_t* rev_idx, const uint32_t* cand_packed, int32_t k,
+                       int32_t mode, int64_t max_iterations, int32_t block_threads,
+                       int64_t* stats, int32_t* status,
+                       void* workspace, size_t workspace_bytes, void* stream);
+
+/*
  * multi_move 2-opt (same kernel and results as tspb_two_opt with TSPB_MODE_MULTI_MOVE)
  * that allocates nothing: its scratch is a fixed TSPB_STATIC_SCRATCH_BYTES array compiled
  * into the library, which every GPU that loads the library holds until exit. No
@@ -192,6 +206,42 @@ int tspb_stable_rank(const double* fitness, int32_t count, int32_t keep, int32_t
 int tspb_nn_init(const int32_t* customers, int32_t n, const int32_t* cand, int32_t cand_rows, int32_t k,
                  const uint64_t* seeds, int32_t pop, int32_t max_node, int32_t* workspace,
                  size_t workspace_bytes, int32_t* out, void* stream);
+
+/*
+ * One GA generation as graph-capturable steps. The random draws of all generations are
+ * pre-drawn on the host in the reference's order and passed as a tape; `gen` (device
+ * int) selects generation g's slice and is advanced by tspb_generation_track, `stopped`
+ * (device int, set by the tracker when patience runs out) turns later steps into no-ops.
+ *
+ * tspb_generation_offspring: fused tournament selection, PMX crossover of pairs
+ *   (2q, 2q+1), inversion mutation and closed-tour length of every child (CTA per child).
+ *   Tape layout per generation: tourn [P][kt], cut_a/cut_b [P/2], u/inv_a/inv_b [P].
+ *   Replaces SelectionCPUTournament.select_batch (tournament_selection.py:98-128),
+ *   CrossoverCPUPermPartiallyMapped.crossover_batch (pmx_crossover.py:128-171),
+ *   MutationCPUPermInversion.mutate_batch (inversion_mutation.py:65-99) and the offspring
+ *   EvaluationStep (genetic_algorithm.py:174-199) of one generation.
+ * tspb_generation_survival: stable (fitness, index) survival of [pop; off] into new_pop /
+ *   new_fit, and tie_flags[g] = 1 when the elite-th and (elite+1)-th survivors tie.
+ *   Replaces SurvivalStep / _select_survivors_assessed (genetic_algorithm.py:216-251, 618-706).
+ * tspb_generation_elite_cost: fitness of rows [0, k) after the elite 2-opt
+ *   (EliteOnlyLocalSearchStep re-evaluation, pipeline_steps.py:172-184).
+ * tspb_generation_track: best-so-far with the strict 1e-6 rule, history[g+1], patience
+ *   (genetic_algorithm.py:876-910).
+ */
+int tspb_generation_offspring(const int32_t* pop, const double* fit, int32_t P, int32_t n, int32_t kt,
+                              const int32_t* tape_tourn, const int32_t* tape_cut_a, const int32_t* tape_cut_b,
+                              const double* tape_u, const int32_t* tape_inv_a, const int32_t* tape_inv_b,
+                              double rate, const int32_t* dist, int64_t dist_stride, const double* coords,
+                              const int32_t* gen, const int32_t* stopped, int32_t* off, double* off_fit,
+                              void* stream);
+int tspb_generation_survival(const int32_t* pop, const double* fit, const int32_t* off, const double* off_fit,
+                             int32_t P, int32_t n, int32_t elite, const int32_t* gen, const int32_t* stopped,
+                             int32_t* order, int32_t* new_pop, double* new_fit, int32_t* tie_flags, void* stream);
+int tspb_generation_elite_cost(const int32_t* pop, int32_t k, int32_t n, const int32_t* dist, int64_t dist_stride,
+                               const double* coords, const int32_t* stopped, double* fit, void* stream);
+int tspb_generation_track(const double* fit, const int32_t* pop, int32_t P, int32_t n, int32_t* gen,
+                          int32_t* stopped, int32_t* stall, int64_t patience, double* best_cost,
+                          int32_t* best_tour, double* history, int32_t* done_gens, void* stream);
 
 /*
  * Permutation check: bad[r] = 0 when row r is a permutation of 0..n-1, else 1.

@@ -1,0 +1,330 @@
+// One GA generation on the device, for graph capture: the fused offspring kernel
+// (tournament selection, PMX crossover, inversion mutation, tour-length reduction), the
+// (mu + lambda) survival gather, and best-so-far tracking with early stop.
+//
+// The random draws of every generation are pre-drawn on the host from the run's
+// generator in the reference's order (tournament (P, k) -> PMX cut pairs (P/2) ->
+// inversion u (P) -> inversion position pairs (P)) and uploaded once as a tape; the
+// kernels read generation g's slice through a device counter that the tracking kernel
+// advances, so one captured graph replays every generation unchanged. A device flag set
+// by the tracker (patience exhausted) turns the remaining generations into no-ops.
+//
+// Reference semantics reproduced bit for bit:
+//   SelectionCPUTournament.select_batch    (tournament_selection.py:98-128)
+//   CrossoverCPUPermPartiallyMapped         (pmx_crossover.py:49-171, open permutations)
+//   MutationCPUPermInversion.mutate_batch   (inversion_mutation.py:65-99)
+//   evaluate_tour_cpu                       (tour_cost.py:17-29)
+//   _select_survivors_assessed              (genetic_algorithm.py:618-706)
+//   best tracking / patience                (genetic_algorithm.py:876-910)
+#include "common.cuh"
+
+namespace tspb {
+
+struct GenTape {
+  const int32_t* tourn;   // [G][P][kt]
+  const int32_t* cut_a;   // [G][P/2]
+  const int32_t* cut_b;   // [G][P/2]
+  const double* u;        // [G][P]
+  const int32_t* inv_a;   // [G][P]
+  const int32_t* inv_b;   // [G][P]
+};
+
+__device__ __forceinline__ int tournament_winner(const double* fit, const int32_t* c, int kt, int pop) {
+  int best = c[0];
+  if ((unsigned)best >= (unsigned)pop) best = 0;
+  double bf = fit[best];
+  for (int q = 1; q < kt; ++q) {
+    const int v = c[q];
+    if ((unsigned)v >= (unsigned)pop) continue;
+    const double f = fit[v];
+    if (f < bf) {
+      bf = f;
+      best = v;
+    }
+  }
+  return best;
+}
+
+// CTA per child row. Shared memory: inv_p2[n], child[n], in_seg bits.
+__global__ void __launch_bounds__(256) offspring_kernel(const int32_t* __restrict__ pop, const double* __restrict__ fit,
+                                                        int P, int n, int kt, GenTape tape, const int* __restrict__ gen,
+                                                        const int* __restrict__ stopped, double rate, DistSrc ds,
+                                                        int32_t* __restrict__ off, double* __restrict__ off_fit) {
+  if (*stopped) return;
+  extern __shared__ int sm[];
+  int* inv_p2 = sm;
+  int* child = sm + n;
+  unsigned* in_seg = reinterpret_cast<unsigned*>(sm + 2 * n);
+  __shared__ int w[2];
+  __shared__ long long red[32];
+  const int g = *gen;
+  const int row = blockIdx.x, tid = threadIdx.x, T = blockDim.x;
+  const int pairs = P >> 1;
+  const int q = row >> 1, h = row & 1;
+  const bool paired = row < 2 * pairs;
+  if (tid < 2) {
+    const int sel = paired ? 2 * q + (tid == 0 ? h : 1 - h) : row;
+    w[tid] = tournament_winner(fit, tape.tourn + ((long long)g * P + sel) * kt, kt, P);
+  }
+  __syncthreads();
+  const int32_t* p1 = pop + (long long)w[0] * n;
+  const int32_t* p2 = pop + (long long)w[1] * n;
+  if (!paired || n < 2) {
+    for (int p = tid; p < n; p += T) child[p] = __ldg(p1 + p);
+  } else {
+    int c1 = tape.cut_a[(long long)g * pairs + q], c2 = tape.cut_b[(long long)g * pairs + q];
+    if (c1 > c2) {
+      const int tmp = c1;
+      c1 = c2;
+      c2 = tmp;
+    }
+    const int words = (n + 31) >> 5;
+    for (int p = tid; p < n; p += T) child[p] = -1;
+    for (int wd = tid; wd < words; wd += T) in_seg[wd] = 0u;
+    __syncthreads();
+    for (int p = tid; p < n; p += T) {
+      inv_p2[__ldg(p2 + p)] = p;
+      if (p >= c1 && p <= c2) {
+        const int v1 = __ldg(p1 + p);
+        child[p] = v1;
+        atomicOr(&in_seg[v1 >> 5], 1u << (v1 & 31));
+      }
+    }
+    __syncthreads();
+    const int seg_len = c2 - c1 + 1;
+    for (int idx = c1 + tid; idx <= c2; idx += T) {
+      const int val = __ldg(p2 + idx);
+      if (in_seg[val >> 5] & (1u << (val & 31))) continue;
+      int pos = idx, steps = 0;
+      while (pos >= c1 && pos <= c2 && steps <= seg_len) {
+        pos = inv_p2[__ldg(p1 + pos)];
+        ++steps;
+      }
+      if (pos < c1 || pos > c2) child[pos] = val;
+    }
+    __syncthreads();
+    for (int p = tid; p < n; p += T)
+      if (child[p] == -1) child[p] = __ldg(p2 + p);
+  }
+  __syncthreads();
+  // inversion mutation of this child
+  const long long gi = (long long)g * P + row;
+  if (tape.u[gi] < rate) {
+    const int a = tape.inv_a[gi], b = tape.inv_b[gi];
+    const int lo = a < b ? a : b, hi = a < b ? b : a;
+    if (lo >= 0 && hi < n) {
+      const int half = (hi - lo + 1) >> 1;
+      for (int t = tid; t < half; t += T) {
+        const int x = child[lo + t], y = child[hi - t];
+        child[lo + t] = y;
+        child[hi - t] = x;
+      }
+    }
+  }
+  __syncthreads();
+  // write out and reduce the closed-tour length (exact int64, one float64 at the end)
+  int32_t* dst = off + (long long)row * n;
+  long long acc = 0;
+  for (int p = tid; p < n; p += T) {
+    const int v = child[p];
+    dst[p] = v;
+    acc += ds(v, child[p + 1 == n ? 0 : p + 1]);
+  }
+  acc = block_sum(acc, red);
+  if (tid == 0) off_fit[row] = n <= 1 ? 0.0 : (double)acc;
+}
+
+// Stable rank of the 2P combined fitness (old population first), keep P.
+__global__ void survival_rank_kernel(const double* __restrict__ fa, const double* __restrict__ fb, int P,
+                                     const int* __restrict__ stopped, int32_t* __restrict__ order) {
+  if (*stopped) return;
+  __shared__ double tile[256];
+  const int count = 2 * P;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const double fi = i < count ? (i < P ? fa[i] : fb[i - P]) : 0.0;
+  int rank = 0;
+  for (int base = 0; base < count; base += blockDim.x) {
+    const int j = base + threadIdx.x;
+    if (j < count) tile[threadIdx.x] = j < P ? fa[j] : fb[j - P];
+    __syncthreads();
+    const int lim = min((int)blockDim.x, count - base);
+    if (i < count)
+      for (int t = 0; t < lim; ++t) {
+        const double fj = tile[t];
+        rank += (fj < fi) || (fj == fi && base + t < i);
+      }
+    __syncthreads();
+  }
+  if (i < count && rank < P) order[rank] = i;
+}
+
+// CTA per survivor: new_pop[r] = combined[order[r]]; flags a fitness tie across the elite edge.
+__global__ void survival_gather_kernel(const int32_t* __restrict__ pop, const double* __restrict__ fit,
+                                       const int32_t* __restrict__ off, const double* __restrict__ off_fit, int P, int n,
+                                       const int32_t* __restrict__ order, const int* __restrict__ stopped,
+                                       const int* __restrict__ gen, int elite, int32_t* __restrict__ new_pop,
+                                       double* __restrict__ new_fit, int32_t* __restrict__ tie_flags) {
+  if (*stopped) return;
+  const int r = blockIdx.x;
+  const int o = order[r];
+  const int32_t* src = o < P ? pop + (long long)o * n : off + (long long)(o - P) * n;
+  int32_t* dst = new_pop + (long long)r * n;
+  if ((n & 3) == 0 && ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0) {
+    const int4* s4 = reinterpret_cast<const int4*>(src);
+    int4* d4 = reinterpret_cast<int4*>(dst);
+    for (int t = threadIdx.x; t < (n >> 2); t += blockDim.x) d4[t] = s4[t];
+  } else {
+    for (int t = threadIdx.x; t < n; t += blockDim.x) dst[t] = src[t];
+  }
+  if (threadIdx.x == 0) {
+    const double f = o < P ? fit[o] : off_fit[o - P];
+    new_fit[r] = f;
+    if (elite > 0 && elite < P && r == elite) {
+      const int oe = order[elite - 1];
+      const double fe = oe < P ? fit[oe] : off_fit[oe - P];
+      tie_flags[*gen] = fe == f ? 1 : 0;
+    }
+  }
+}
+
+// One CTA: argmin of fitness (first minimum), strict improvement by more than 1e-6 copies
+// the tour, history[g + 1] = best so far, patience, then the generation counter advances.
+__global__ void track_best_kernel(const double* __restrict__ fit, const int32_t* __restrict__ pop, int P, int n,
+                                  int* __restrict__ gen, int* __restrict__ stopped, int* __restrict__ stall,
+                                  long long patience, double* __restrict__ best_cost, int32_t* __restrict__ best_tour,
+                                  double* __restrict__ history, int32_t* __restrict__ done_gens) {
+  if (*stopped) return;
+  __shared__ double sv[32];
+  __shared__ int si[32];
+  __shared__ int improve;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  double bv = __longlong_as_double(0x7ff0000000000000LL);
+  int bi = P;
+  for (int i = tid; i < P; i += blockDim.x) {
+    const double f = fit[i];
+    if (f < bv || (f == bv && i < bi)) {
+      bv = f;
+      bi = i;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(FULL, bv, o);
+    const int oi = __shfl_xor_sync(FULL, bi, o);
+    if (ov < bv || (ov == bv && oi < bi)) {
+      bv = ov;
+      bi = oi;
+    }
+  }
+  if (lane == 0) {
+    sv[wid] = bv;
+    si[wid] = bi;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+      if (sv[w] < bv || (sv[w] == bv && si[w] < bi)) {
+        bv = sv[w];
+        bi = si[w];
+      }
+    si[0] = bi;
+    improve = bv < *best_cost - 1e-6;
+    if (improve) {
+      *best_cost = bv;
+      *stall = 0;
+    } else {
+      *stall += 1;
+    }
+    const int g = *gen;
+    history[g + 1] = *best_cost;
+    *done_gens = g + 1;
+    if (*stall >= patience) *stopped = 1;
+    *gen = g + 1;
+  }
+  __syncthreads();
+  if (improve) {
+    const int32_t* src = pop + (long long)si[0] * n;
+    for (int t = tid; t < n; t += blockDim.x) best_tour[t] = src[t];
+  }
+}
+
+// Rows [0, k) of the population get their fitness recomputed after the elite 2-opt.
+__global__ void elite_cost_kernel(const int32_t* __restrict__ pop, int k, int n, DistSrc ds,
+                                  const int* __restrict__ stopped, double* __restrict__ fit) {
+  if (*stopped) return;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= k) return;
+  const int32_t* t = pop + (long long)warp * n;
+  long long acc = 0;
+  for (int p = lane; p < n; p += 32) acc += ds(t[p], t[p + 1 == n ? 0 : p + 1]);
+  acc = warp_sum(acc);
+  if (lane == 0) fit[warp] = n <= 1 ? 0.0 : (double)acc;
+}
+
+}  // namespace tspb
+
+using namespace tspb;
+
+static DistSrc gen_ds(const int32_t* dist, int64_t stride, const double* coords) {
+  DistSrc d;
+  d.dist = dist;
+  d.stride = stride;
+  d.coords = reinterpret_cast<const double2*>(coords);
+  return d;
+}
+
+extern "C" int tspb_generation_offspring(const int32_t* pop, const double* fit, int32_t P, int32_t n, int32_t kt,
+                                         const int32_t* tape_tourn, const int32_t* tape_cut_a, const int32_t* tape_cut_b,
+                                         const double* tape_u, const int32_t* tape_inv_a, const int32_t* tape_inv_b,
+                                         double rate, const int32_t* dist, int64_t dist_stride, const double* coords,
+                                         const int32_t* gen, const int32_t* stopped, int32_t* off, double* off_fit,
+                                         void* stream) {
+  if (P < 1 || n < 1 || kt < 1) return TSPB_ERR_ARG;
+  if (!pop || !fit || !tape_tourn || !tape_u || !tape_inv_a || !tape_inv_b || !gen || !stopped || !off || !off_fit)
+    return TSPB_ERR_ARG;
+  if (P >= 2 && (!tape_cut_a || !tape_cut_b)) return TSPB_ERR_ARG;
+  if (!dist && !coords) return TSPB_ERR_ARG;
+  const size_t smem = (size_t)8 * n + (size_t)((n + 31) / 32) * 4;
+  if (smem > 200 * 1024) return TSPB_ERR_UNSUPPORTED;
+  if (smem > 48 * 1024)
+    TSPB_CUDA_CHECK(cudaFuncSetAttribute(offspring_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  GenTape tape{tape_tourn, tape_cut_a, tape_cut_b, tape_u, tape_inv_a, tape_inv_b};
+  offspring_kernel<<<P, 256, smem, reinterpret_cast<cudaStream_t>(stream)>>>(pop, fit, P, n, kt, tape, gen, stopped, rate,
+                                                                             gen_ds(dist, dist_stride, coords), off, off_fit);
+  return tspb_launch_status();
+}
+
+extern "C" int tspb_generation_survival(const int32_t* pop, const double* fit, const int32_t* off, const double* off_fit,
+                                        int32_t P, int32_t n, int32_t elite, const int32_t* gen, const int32_t* stopped,
+                                        int32_t* order, int32_t* new_pop, double* new_fit, int32_t* tie_flags,
+                                        void* stream) {
+  if (P < 1 || n < 1 || elite < 0) return TSPB_ERR_ARG;
+  if (!pop || !fit || !off || !off_fit || !gen || !stopped || !order || !new_pop || !new_fit) return TSPB_ERR_ARG;
+  if (elite > 0 && elite < P && !tie_flags) return TSPB_ERR_ARG;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  survival_rank_kernel<<<(2 * P + 255) / 256, 256, 0, st>>>(fit, off_fit, P, stopped, order);
+  survival_gather_kernel<<<P, 128, 0, st>>>(pop, fit, off, off_fit, P, n, order, stopped, gen, elite, new_pop, new_fit,
+                                           tie_flags);
+  return tspb_launch_status();
+}
+
+extern "C" int tspb_generation_elite_cost(const int32_t* pop, int32_t k, int32_t n, const int32_t* dist, int64_t dist_stride,
+                                          const double* coords, const int32_t* stopped, double* fit, void* stream) {
+  if (k < 0 || n < 1) return TSPB_ERR_ARG;
+  if (k == 0) return TSPB_OK;
+  if (!pop || !stopped || !fit || (!dist && !coords)) return TSPB_ERR_ARG;
+  elite_cost_kernel<<<(k * 32 + 255) / 256, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+      pop, k, n, gen_ds(dist, dist_stride, coords), stopped, fit);
+  return tspb_launch_status();
+}
+
+extern "C" int tspb_generation_track(const double* fit, const int32_t* pop, int32_t P, int32_t n, int32_t* gen,
+                                     int32_t* stopped, int32_t* stall, int64_t patience, double* best_cost,
+                                     int32_t* best_tour, double* history, int32_t* done_gens, void* stream) {
+  if (P < 1 || n < 1) return TSPB_ERR_ARG;
+  if (!fit || !pop || !gen || !stopped || !stall || !best_cost || !best_tour || !history || !done_gens) return TSPB_ERR_ARG;
+  track_best_kernel<<<1, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(fit, pop, P, n, gen, stopped, stall, patience,
+                                                                          best_cost, best_tour, history, done_gens);
+  return tspb_launch_status();
+}

@@ -54,6 +54,7 @@ __global__ void __launch_bounds__(1024) two_opt_kernel(const TwoOptArgs A) {
   const int lane = tid & 31, wid = tid >> 5, nwarps = T >> 5;
   const int t = blockIdx.x;
   if (t >= A.num_tours) return;
+  if (A.skip != nullptr && *A.skip != 0) return;
 
   int32_t* g_tour = A.tours + (long long)t * n;
   unsigned char* ws = A.ws ? A.ws + (size_t)t * A.ws_tour_bytes : nullptr;
@@ -466,12 +467,11 @@ extern "C" size_t tspb_two_opt_workspace_bytes(int32_t num_tours, int32_t n, int
   return per * (size_t)num_tours;
 }
 
-extern "C" int tspb_two_opt(int32_t* tours, int32_t num_tours, int32_t n, const int32_t* dist, int64_t dist_stride,
-                            const double* coords, const int32_t* cand, const int32_t* cand_dist,
-                            const int32_t* rev_off, const int32_t* rev_idx, const uint32_t* cand_packed, int32_t k,
-                            int32_t mode,
-                            int64_t max_iterations, int32_t block_threads, int64_t* stats, int32_t* status,
-                            void* workspace, size_t workspace_bytes, void* stream) {
+static int two_opt_impl(int32_t* tours, int32_t num_tours, int32_t n, const int32_t* dist, int64_t dist_stride,
+                        const double* coords, const int32_t* cand, const int32_t* cand_dist, const int32_t* rev_off,
+                        const int32_t* rev_idx, const uint32_t* cand_packed, int32_t k, int32_t mode,
+                        int64_t max_iterations, int32_t block_threads, int64_t* stats, int32_t* status,
+                        const int32_t* skip, void* workspace, size_t workspace_bytes, void* stream) {
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   if (num_tours < 0 || n < 0 || mode < 0 || mode > 2) return TSPB_ERR_ARG;
   if (num_tours == 0) return TSPB_OK;
@@ -510,6 +510,7 @@ extern "C" int tspb_two_opt(int32_t* tours, int32_t num_tours, int32_t n, const 
     c.ws = reinterpret_cast<unsigned char*>(workspace);
     c.ws_tour_bytes = per;
     c.arrays_in_smem = per == 0 ? 1 : 0;
+    c.skip = skip;
     return launch_two_opt_scan(c, mode, threads, st);
   }
   if (use_cand && rev_off != nullptr && rev_idx != nullptr && mode != TSPB_MODE_MULTI_MOVE) {
@@ -535,6 +536,7 @@ extern "C" int tspb_two_opt(int32_t* tours, int32_t num_tours, int32_t n, const 
     c.arrays_in_smem = per == 0 ? 1 : 0;
     c.rev_off = rev_off;
     c.rev_idx = rev_idx;
+    c.skip = skip;
     return launch_two_opt_cached(c, mode, threads, st);
   }
   const Layout L = two_opt_layout(n, use_cand ? k : 0, mode, use_cand);
@@ -558,6 +560,7 @@ extern "C" int tspb_two_opt(int32_t* tours, int32_t num_tours, int32_t n, const 
   a.ws_tour_bytes = L.ws_tour_bytes;
   a.ws_keys_off = L.ws_keys_off;
   a.arrays_in_smem = L.arrays_in_smem ? 1 : 0;
+  a.skip = skip;
   if (use_cand) {
     switch (mode) {
       case TSPB_MODE_BEST: return launch<TSPB_MODE_BEST, true>(a, threads, L.smem_bytes, st);
@@ -570,4 +573,23 @@ extern "C" int tspb_two_opt(int32_t* tours, int32_t num_tours, int32_t n, const 
     case TSPB_MODE_FIRST: return launch<TSPB_MODE_FIRST, false>(a, threads, L.smem_bytes, st);
     default: return launch<TSPB_MODE_MULTI_MOVE, false>(a, threads, L.smem_bytes, st);
   }
+}
+
+extern "C" int tspb_two_opt(int32_t* tours, int32_t num_tours, int32_t n, const int32_t* dist, int64_t dist_stride,
+                            const double* coords, const int32_t* cand, const int32_t* cand_dist, const int32_t* rev_off,
+                            const int32_t* rev_idx, const uint32_t* cand_packed, int32_t k, int32_t mode,
+                            int64_t max_iterations, int32_t block_threads, int64_t* stats, int32_t* status,
+                            void* workspace, size_t workspace_bytes, void* stream) {
+  return two_opt_impl(tours, num_tours, n, dist, dist_stride, coords, cand, cand_dist, rev_off, rev_idx, cand_packed, k,
+                      mode, max_iterations, block_threads, stats, status, nullptr, workspace, workspace_bytes, stream);
+}
+
+extern "C" int tspb_two_opt_gated(const int32_t* skip, int32_t* tours, int32_t num_tours, int32_t n, const int32_t* dist,
+                                  int64_t dist_stride, const double* coords, const int32_t* cand, const int32_t* cand_dist,
+                                  const int32_t* rev_off, const int32_t* rev_idx, const uint32_t* cand_packed, int32_t k,
+                                  int32_t mode, int64_t max_iterations, int32_t block_threads, int64_t* stats,
+                                  int32_t* status, void* workspace, size_t workspace_bytes, void* stream) {
+  if (skip == nullptr) return TSPB_ERR_ARG;
+  return two_opt_impl(tours, num_tours, n, dist, dist_stride, coords, cand, cand_dist, rev_off, rev_idx, cand_packed, k,
+                      mode, max_iterations, block_threads, stats, status, skip, workspace, workspace_bytes, stream);
 }

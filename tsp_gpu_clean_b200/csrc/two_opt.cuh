@@ -23,6 +23,7 @@ struct TwoOptArgs {
   const int32_t* rev_off;  // cached kernel: CSR offsets of the reverse k-NN index (n + 1)
   const int32_t* rev_idx;  // cached kernel: flat entries a * k + r grouped by candidate node
   const uint32_t* cand_packed;  // scan kernel: c | d(a, c) << 16 per entry (optional)
+  const int32_t* skip;          // optional device flag: non-zero makes the launch a no-op
 };
 
 // Order-preserving u64 key: negative int32 gain in the high word, scan index low.

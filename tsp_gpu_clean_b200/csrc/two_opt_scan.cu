@@ -41,6 +41,7 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value) two_op
   const int tid = threadIdx.x;
   const int t = blockIdx.x;
   if (t >= A.num_tours) return;
+  if (A.skip != nullptr && *A.skip != 0) return;
   int32_t* g_tour = A.tours + (long long)t * n;
   unsigned char* base = A.arrays_in_smem ? dsm : A.ws + (size_t)t * A.ws_tour_bytes;
   int* tour = reinterpret_cast<int*>(base);

@@ -1,0 +1,319 @@
+"""Device-resident memetic GA with every generation replayed from a captured CUDA graph.
+
+`FusedMemeticSolver.evolve` computes exactly what the reference's
+
+    GeneticAlgorithm(population_size=P, mutation_rate=rate,
+                     initialization=InitializationCPUTourNearestNeighbor(k=nn_k),
+                     selection=SelectionCPUTournament(k=tournament_k),
+                     crossover=CrossoverCPUPermPartiallyMapped(), mutation=MutationCPUPermInversion(),
+                     evaluation=EvaluationCPUCost(), local_search=LocalSearchCPUTourTwoOpt(...),
+                     local_search_stage="none",
+                     pipeline=[PostInitLocalSearchStep(...), EliteOnlyLocalSearchStep(..., elite_count=k)])
+    .evolve(context, customers, max_generations, patience=...)
+
+computes (`src/algorithms/metaheuristics/genetic_algorithm.py:789-965`,
+`src/algorithms/pipeline_steps.py:85-195`): same final population, fitness, best tour,
+convergence history and final RNG state.
+
+How: the row seeds and every generation's random draws are taken from `context.rng` in
+the reference's order before the loop (no draw depends on tour data) and uploaded as a
+tape. One generation is five launches - fused offspring (tournament + PMX + inversion +
+length), survival, elite 2-opt on survivor rows [0, k), elite re-cost, best tracking -
+captured once per population buffer parity into a CUDA graph and replayed in chunks.
+
+Elites: survivors come out sorted by (fitness, index), so `argsort(fitness)[:k]` is the
+first k rows unless the k-th and (k+1)-th fitness tie; then membership follows NumPy's
+unstable sort. The survival kernel flags such generations; a chunk that contains one is
+rolled back to its snapshot and that generation runs eagerly with the host `np.argsort`.
+Early stop: the tracking kernel sets a device stop flag when patience runs out; later
+launches (the 2-opt through `tspb_two_opt_gated`) become no-ops, and the RNG is rewound
+to its state after the last generation that ran.
+"""
+
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass
+from typing import Any
+
+import numpy as np
+
+from . import native
+from .device import operands_for, ptr, require_gpu, stream_handle, torch
+from .problem import resolve_rng
+from .routes import sample_distinct_pairs
+from .strategies.initialization import InitializationB200TourNearestNeighbor
+
+
+@dataclass
+class LocalSearchConfig:
+  mode: str = "best"
+  max_iterations: int = 10
+  candidate_k: int | None = 20
+  threads: int = 128
+
+
+class FusedMemeticSolver:
+  def __init__(self, population_size: int = 128, mutation_rate: float = 0.05, tournament_k: int = 5, nn_k: int = 5,
+               local_search: LocalSearchConfig | None = None, elite_count: int = 16, post_init: bool = True,
+               use_graph: bool = True, chunk: int = 16, max_matrix_dimension: int | None = None) -> None:
+    if population_size < 2:
+      raise ValueError("population_size must be >= 2")
+    self.P = population_size
+    self.rate = mutation_rate
+    self.kt = tournament_k
+    self.nn_k = nn_k
+    self.ls = local_search if local_search is not None else LocalSearchConfig()
+    self.elite = min(elite_count, population_size) if elite_count else 0
+    self.post_init = post_init
+    self.use_graph = use_graph
+    self.chunk = max(1, chunk)
+    self.max_matrix_dimension = max_matrix_dimension
+    self.kernel_launches = 0
+    self.last_timing: dict[str, float] = {}
+
+  # -------------------------------------------------------------------------- tape
+  def _draw_tape(self, rng: np.random.Generator, G: int, n: int):
+    P = self.P
+    tourn = np.empty((G, P, self.kt), dtype=np.int32)
+    cut_a = np.empty((G, P // 2), dtype=np.int32)
+    cut_b = np.empty((G, P // 2), dtype=np.int32)
+    u = np.empty((G, P), dtype=np.float64)
+    inv_a = np.empty((G, P), dtype=np.int32)
+    inv_b = np.empty((G, P), dtype=np.int32)
+    states = []
+    for g in range(G):
+      tourn[g] = rng.integers(0, P, size=(P, self.kt), dtype=np.int32)   # tournament_selection.py:113
+      pairs = sample_distinct_pairs(rng, P // 2, 0, n)                    # pmx_crossover.py:155
+      cut_a[g], cut_b[g] = pairs[:, 0], pairs[:, 1]
+      u[g] = rng.random(P)                                                # inversion_mutation.py:82
+      pos = sample_distinct_pairs(rng, P, 0, n)                           # route_helpers.py:214
+      inv_a[g], inv_b[g] = pos[:, 0], pos[:, 1]
+      states.append(rng.bit_generator.state)
+    return (tourn, cut_a, cut_b, u, inv_a, inv_b), states
+
+  # -------------------------------------------------------------------------- launches
+  def _two_opt(self, rows_ptr, num, skip=None):
+    ls = self.ls
+    lib = native.load_library()
+    mode = native.MODE_CODES[ls.mode]
+    rc = lib.tspb_two_opt_gated(ptr(skip if skip is not None else self.d_zero), rows_ptr, num, self.n, ptr(self.dist),
+                                self.stride, ptr(self.coords), ptr(self.cand), ptr(self.cand_dist), None, None,
+                                ptr(self.packed), self.k, mode, int(ls.max_iterations), int(ls.threads), None,
+                                ptr(self.ls_status), ptr(self.ws), self.ws_bytes, stream_handle())
+    native.check("tspb_two_opt_gated", rc)
+
+  def _generation(self, parity: int) -> None:
+    """Enqueue one generation reading buffer `parity`, writing buffer `1 - parity`."""
+    lib = native.load_library()
+    src, dst = self.pop[parity], self.pop[1 - parity]
+    fsrc, fdst = self.fit[parity], self.fit[1 - parity]
+    t = self.tape
+    sh = stream_handle()
+    native.check("offspring", lib.tspb_generation_offspring(
+      ptr(src), ptr(fsrc), self.P, self.n, self.kt, ptr(t[0]), ptr(t[1]), ptr(t[2]), ptr(t[3]), ptr(t[4]), ptr(t[5]),
+      float(self.rate), ptr(self.dist), self.stride, ptr(self.coords), ptr(self.gen), ptr(self.stopped), ptr(self.off),
+      ptr(self.off_fit), sh))
+    native.check("survival", lib.tspb_generation_survival(
+      ptr(src), ptr(fsrc), ptr(self.off), ptr(self.off_fit), self.P, self.n, self.elite, ptr(self.gen), ptr(self.stopped),
+      ptr(self.order), ptr(dst), ptr(fdst), ptr(self.ties), sh))
+    if self.elite:
+      self._two_opt(ptr(dst), self.elite, skip=self.stopped)
+      native.check("elite_cost", lib.tspb_generation_elite_cost(
+        ptr(dst), self.elite, self.n, ptr(self.dist), self.stride, ptr(self.coords), ptr(self.stopped), ptr(fdst), sh))
+    native.check("track", lib.tspb_generation_track(
+      ptr(fdst), ptr(dst), self.P, self.n, ptr(self.gen), ptr(self.stopped), ptr(self.stall), int(self.patience),
+      ptr(self.best_cost), ptr(self.best_tour), ptr(self.history), ptr(self.done), sh))
+    self.kernel_launches += 6 if self.elite else 4
+
+  def _generation_host_elites(self, parity: int) -> None:
+    """Generation with a fitness tie across the elite edge: elites from the host `np.argsort`."""
+    lib = native.load_library()
+    src, dst = self.pop[parity], self.pop[1 - parity]
+    fsrc, fdst = self.fit[parity], self.fit[1 - parity]
+    t = self.tape
+    sh = stream_handle()
+    native.check("offspring", lib.tspb_generation_offspring(
+      ptr(src), ptr(fsrc), self.P, self.n, self.kt, ptr(t[0]), ptr(t[1]), ptr(t[2]), ptr(t[3]), ptr(t[4]), ptr(t[5]),
+      float(self.rate), ptr(self.dist), self.stride, ptr(self.coords), ptr(self.gen), ptr(self.stopped), ptr(self.off),
+      ptr(self.off_fit), sh))
+    native.check("survival", lib.tspb_generation_survival(
+      ptr(src), ptr(fsrc), ptr(self.off), ptr(self.off_fit), self.P, self.n, self.elite, ptr(self.gen), ptr(self.stopped),
+      ptr(self.order), ptr(dst), ptr(fdst), ptr(self.ties), sh))
+    idx = np.argsort(fdst.cpu().numpy())[: self.elite].astype(np.int32)  # pipeline_steps.py:163
+    d_idx = torch.from_numpy(idx).cuda()
+    tmp = torch.empty((self.elite, self.n), dtype=torch.int32, device="cuda")
+    native.call("tspb_gather_rows", ptr(dst), self.P, self.n, ptr(d_idx), self.elite, ptr(tmp), sh)
+    self._two_opt(ptr(tmp), self.elite, skip=self.stopped)
+    costs = torch.empty(self.elite, dtype=torch.float64, device="cuda")
+    native.call("tspb_tour_cost", ptr(tmp), self.elite, self.n, ptr(self.dist), self.stride, ptr(self.coords), 1,
+                ptr(costs), sh)
+    native.call("tspb_scatter_rows", ptr(tmp), self.elite, self.n, ptr(d_idx), ptr(dst), self.P, sh)
+    fdst[d_idx.long()] = costs
+    native.check("track", lib.tspb_generation_track(
+      ptr(fdst), ptr(dst), self.P, self.n, ptr(self.gen), ptr(self.stopped), ptr(self.stall), int(self.patience),
+      ptr(self.best_cost), ptr(self.best_tour), ptr(self.history), ptr(self.done), sh))
+    torch.cuda.synchronize()
+
+  # -------------------------------------------------------------------------- evolve
+  def evolve(self, context: Any, customers: Any, max_generations: int, patience: int | None = None):
+    require_gpu()
+    t_start = time.perf_counter()
+    n = len(customers)
+    if n < 4 or n != int(context.dimension) or list(customers) != list(range(n)):
+      raise ValueError("FusedMemeticSolver needs the full tour customers = range(dimension) with dimension >= 4")
+    if patience is None:
+      patience = int(2 * math.sqrt(n))
+    self.n, self.patience = n, patience
+    P, G = self.P, int(max_generations)
+    rng = resolve_rng(context, None)
+    self.kernel_launches = 0
+
+    # initial population and fitness (draws the row seeds first, like the reference)
+    pop0 = InitializationB200TourNearestNeighbor(k=self.nn_k, return_gpu=True).initialize(list(customers), P, context)
+    ops = operands_for(context)
+    self.dist, self.stride, self.coords = ops.distance_args(n, self.max_matrix_dimension)
+    self.cand = self.cand_dist = self.packed = None
+    self.k = 0
+    ls = self.ls
+    if ls.candidate_k:
+      tabs = ops.candidates(int(ls.candidate_k), context.get_cpu_candidate_list(int(ls.candidate_k)), n,
+                            self.max_matrix_dimension)
+      self.cand, self.cand_dist, self.packed, self.k = tabs.cand, tabs.cand_dist, tabs.packed, tabs.k
+    lib = native.load_library()
+    rows_max = max(self.elite, P if self.post_init else 0, 1)
+    self.ws_bytes = int(lib.tspb_two_opt_workspace_bytes(rows_max, n, self.k, native.MODE_CODES[ls.mode], ls.threads))
+    self.ws = torch.empty(max(self.ws_bytes, 1), dtype=torch.uint8, device="cuda")
+    self.ls_status = torch.zeros(rows_max, dtype=torch.int32, device="cuda")
+    self.d_zero = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+    self.pop = [pop0.contiguous(), torch.empty_like(pop0)]
+    self.fit = [torch.empty(P, dtype=torch.float64, device="cuda") for _ in range(2)]
+    native.call("tspb_tour_cost", ptr(self.pop[0]), P, n, ptr(self.dist), self.stride, ptr(self.coords), 1,
+                ptr(self.fit[0]), stream_handle())
+    self.off = torch.empty_like(pop0)
+    self.off_fit = torch.empty(P, dtype=torch.float64, device="cuda")
+    self.order = torch.empty(P, dtype=torch.int32, device="cuda")
+    fit0 = self.fit[0].cpu().numpy()
+    i0 = int(np.argmin(fit0))
+    initial_best = float(fit0[i0])
+    self.best_cost = torch.tensor([initial_best], dtype=torch.float64, device="cuda")
+    self.best_tour = self.pop[0][i0].clone()
+    self.history = torch.zeros(G + 1, dtype=torch.float64, device="cuda")
+    self.history[0] = initial_best
+    self.gen = torch.zeros(1, dtype=torch.int32, device="cuda")
+    self.stopped = torch.zeros(1, dtype=torch.int32, device="cuda")
+    self.stall = torch.zeros(1, dtype=torch.int32, device="cuda")
+    self.done = torch.zeros(1, dtype=torch.int32, device="cuda")
+    self.ties = torch.zeros(max(G, 1), dtype=torch.int32, device="cuda")
+
+    tape_host, states = self._draw_tape(rng, G, n)
+    self.tape = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in tape_host]
+    torch.cuda.synchronize()
+    t_setup = time.perf_counter()
+
+    # generation 1 starts with the post-init refinement of the whole population
+    if self.post_init and G > 0:
+      self._two_opt(ptr(self.pop[0]), P)
+      native.call("tspb_tour_cost", ptr(self.pop[0]), P, n, ptr(self.dist), self.stride, ptr(self.coords), 1,
+                  ptr(self.fit[0]), stream_handle())
+      self.kernel_launches += 2
+
+    graphs = self._capture() if (self.use_graph and G > 0) else None
+    per_gen = 6 if self.elite else 4
+    self.kernel_launches = 2 if (self.post_init and G > 0) else 0
+    torch.cuda.synchronize()
+    t_loop = time.perf_counter()
+    g = 0
+    parity = 0
+    while g < G:
+      c = min(self.chunk, G - g)
+      snap = self._snapshot(parity)
+      for q in range(c):
+        if graphs is not None:
+          graphs[(parity + q) % 2].replay()
+          self.kernel_launches += per_gen
+        else:
+          self._generation((parity + q) % 2)
+      torch.cuda.synchronize()
+      ties = self.ties[g : g + c].cpu().numpy() if self.elite and self.elite < P else np.zeros(c, dtype=np.int32)
+      if ties.any():
+        t0 = int(np.argmax(ties != 0))
+        self._restore(snap, parity)
+        for q in range(t0):
+          if graphs is not None:
+            graphs[(parity + q) % 2].replay()
+            self.kernel_launches += per_gen
+          else:
+            self._generation((parity + q) % 2)
+        self._generation_host_elites((parity + t0) % 2)
+        self.kernel_launches += 8
+        c = t0 + 1
+      g += c
+      parity = (parity + c) % 2
+      if int(self.stopped.item()):
+        break
+    torch.cuda.synchronize()
+    t_end = time.perf_counter()
+    if int(self.ls_status.max().item()) != 0:
+      raise RuntimeError("2-opt kernel reported a bad tour inside the fused GA")
+
+    done = int(self.done.item())
+    if 0 < done < G:
+      rng.bit_generator.state = states[done - 1]
+    final_parity = done % 2 if done else 0
+    self.final_population = self.pop[final_parity]
+    self.final_fitness = self.fit[final_parity]
+    history = self.history[: done + 1].cpu().numpy().tolist()
+    best_cost = float(self.best_cost.item())
+    best_tour = self.best_tour.cpu().numpy().astype(np.int32)
+    self.last_timing = {"setup_s": t_setup - t_start, "loop_s": t_end - t_loop, "total_s": t_end - t_start,
+                        "generations": done}
+    stats = {
+      "initial_fitness": initial_best,
+      "best_fitness": best_cost,
+      "best_is_feasible": True,
+      "generations_completed": done,
+      "stopped_early": done < G,
+      "stop_reason": "no_improvements" if done < G else "max_generations",
+      "convergence_history": history,
+      "kernel_launches": self.kernel_launches,
+    }
+    return best_tour, stats
+
+  # -------------------------------------------------------------------------- graph, snapshots
+  def _capture(self):
+    # Warm every launch path outside capture with the stop flag set (all kernels no-op).
+    self.stopped.fill_(1)
+    self._generation(0)
+    self._generation(1)
+    torch.cuda.synchronize()
+    self.stopped.fill_(0)
+    graphs = []
+    stream = torch.cuda.Stream()
+    stream.wait_stream(torch.cuda.current_stream())
+    for parity in (0, 1):
+      g = torch.cuda.CUDAGraph()
+      with torch.cuda.graph(g, stream=stream, capture_error_mode="relaxed"):
+        self._generation(parity)
+      graphs.append(g)
+    torch.cuda.current_stream().wait_stream(stream)
+    torch.cuda.synchronize()
+    return graphs
+
+  def _snapshot(self, parity: int):
+    return (self.pop[parity].clone(), self.fit[parity].clone(), self.best_cost.clone(), self.best_tour.clone(),
+            self.stall.clone(), self.stopped.clone(), self.gen.clone(), self.done.clone())
+
+  def _restore(self, snap, parity: int) -> None:
+    pop, fit, bc, bt, stall, stopped, gen, done = snap
+    self.pop[parity].copy_(pop)
+    self.fit[parity].copy_(fit)
+    self.best_cost.copy_(bc)
+    self.best_tour.copy_(bt)
+    self.stall.copy_(stall)
+    self.stopped.copy_(stopped)
+    self.gen.copy_(gen)
+    self.done.copy_(done)
+    torch.cuda.synchronize()

@@ -39,6 +39,8 @@ SIGNATURES: dict[str, tuple] = {
   "tspb_status_string": (ctypes.c_char_p, [ctypes.c_int]),
   "tspb_two_opt_workspace_bytes": (_sz, [_i32, _i32, _i32, _i32, _i32]),
   "tspb_two_opt": (ctypes.c_int, [_p, _i32, _i32, _p, _i64, _p, _p, _p, _p, _p, _p, _i32, _i32, _i64, _i32, _p, _p, _p, _sz, _p]),
+  "tspb_two_opt_gated": (ctypes.c_int, [_p, _p, _i32, _i32, _p, _i64, _p, _p, _p, _p, _p, _p, _i32, _i32, _i64, _i32, _p,
+                                         _p, _p, _sz, _p]),
   "tspb_candidate_pack": (ctypes.c_int, [_p, _p, _i32, _i32, _p, _p, _p]),
   "tspb_two_opt_multi_move_static": (ctypes.c_int, [_p, _i32, _i32, _p, _i64, _p, _p, _p, _i32, _i64, _i32, _p, _p, _p]),
   "tspb_candidate_reverse_index": (ctypes.c_int, [_p, _i32, _i32, _p, _p, _p, _p]),
@@ -52,6 +54,11 @@ SIGNATURES: dict[str, tuple] = {
   "tspb_stable_rank": (ctypes.c_int, [_p, _i32, _i32, _p, _p]),
   "tspb_validate_perm": (ctypes.c_int, [_p, _i32, _i32, _p, _p]),
   "tspb_euc2d_matrix": (ctypes.c_int, [_p, _i32, _p, _i64, _p]),
+  "tspb_generation_offspring": (ctypes.c_int, [_p, _p, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _f64, _p, _i64, _p, _p,
+                                                _p, _p, _p, _p]),
+  "tspb_generation_survival": (ctypes.c_int, [_p, _p, _p, _p, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _p]),
+  "tspb_generation_elite_cost": (ctypes.c_int, [_p, _i32, _i32, _p, _i64, _p, _p, _p, _p]),
+  "tspb_generation_track": (ctypes.c_int, [_p, _p, _i32, _i32, _p, _p, _p, _i64, _p, _p, _p, _p, _p]),
   "tspb_nn_init": (ctypes.c_int, [_p, _i32, _p, _i32, _i32, _p, _i32, _i32, _p, _sz, _p, _p]),
 }
 
