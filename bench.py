@@ -288,6 +288,83 @@ def run_gpu(args, pool) -> dict | None:
   return res if rank == 0 else None
 
 
+GA_WORKLOADS = {
+  # name: (n, population, generations, elite, post_init, instance seed, description)
+  "ga100": (100, 128, 50, 16, True, 42, "memetic GA, 100 uniform cities, population 128, 50 generations, NN init k=5, "
+                                        "tournament 5, PMX, inversion 0.05, 2-opt best k=20 x10 post-init and on 16 elites"),
+  "ga1000": (1000, 512, 100, 64, False, 1000, "memetic GA, 1000 uniform cities, population 512, 100 generations, 64 elites "
+                                               "2-opt best k=20 x10, tournament 5, PMX, inversion 0.05"),
+  "ga2000": (2000, 512, 200, 64, False, 2000, "memetic GA, 2000 uniform cities, population 512, 200 generations, 64 elites "
+                                               "2-opt best k=20 x10, tournament 5, PMX, inversion 0.05"),
+}
+
+
+def _ga_cpu_gens_per_s(name: str, sample_gens: int) -> dict:
+  """Oracle GA (NumPy restatement of the reference GA) generations/s on one core."""
+  from oracle import distances as odist
+  from oracle import ga as oga
+
+  n, P, G, elite, post_init, seed, _ = GA_WORKLOADS[name]
+  coords = instances.uniform_instance(n, seed)
+  D = odist.euc2d_matrix(coords)
+  cache = {}
+
+  def provider(k):
+    if k not in cache:
+      cache[k] = odist.candidate_list(k, coords=coords)
+    return cache[k]
+
+  cfg = oga.GAConfig(population_size=P, mutation_rate=0.05, nn_k=5, tournament_k=5,
+                     local_search=oga.LocalSearchSpec("best", 10, 20), post_init=post_init, elite_count=elite)
+  provider(5), provider(20)
+  t0 = time.perf_counter()
+  oga.OracleGA(D, provider, cfg, np.random.default_rng(42)).evolve(0, patience=10**9)
+  t1 = time.perf_counter()
+  oga.OracleGA(D, provider, cfg, np.random.default_rng(42)).evolve(sample_gens, patience=10**9)
+  t2 = time.perf_counter()
+  loop = max((t2 - t1) - (t1 - t0), 1e-9)
+  return {"value": sample_gens / loop, "gens": sample_gens, "loop_s": loop}
+
+
+def run_ga_bench(args) -> dict:
+  import torch
+
+  from tsp_gpu_clean_b200.build import build_library
+  from tsp_gpu_clean_b200.fused import FusedMemeticSolver, LocalSearchConfig
+  from tsp_gpu_clean_b200.problem import Problem, ProblemContext
+
+  build_library()
+  n, P, G, elite, post_init, seed, desc = GA_WORKLOADS[args.workload]
+  coords = instances.uniform_instance(n, seed)
+
+  def run_once():
+    ctx = ProblemContext(Problem.from_coordinates(coords), seed=42)
+    solver = FusedMemeticSolver(population_size=P, mutation_rate=0.05, tournament_k=5, nn_k=5,
+                                local_search=LocalSearchConfig("best", 10, 20), elite_count=elite, post_init=post_init,
+                                chunk=args.chunk)
+    t0 = time.perf_counter()
+    best, stats = solver.evolve(ctx, list(range(n)), G, patience=10**9)
+    wall = time.perf_counter() - t0
+    return solver, stats, wall
+
+  for _ in range(args.warmup):
+    run_once()
+  torch.cuda.synchronize()
+  loop_ms, walls, launches, gens = [], [], 0, 0
+  with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+    for _ in range(args.steps):
+      solver, stats, wall = run_once()
+      loop_ms.append(solver.last_timing["loop_ms_device"])
+      walls.append(wall)
+      launches += solver.kernel_launches
+      gens += stats["generations_completed"]
+  value = gens / (sum(loop_ms) / 1e3)
+  return {"value": value, "ms_per_step": sum(loop_ms) / args.steps, "clocks": clocks.summary(),
+          "e2e": {"value": gens / sum(walls), "unit": "generations/s", "h2d_bytes_per_step": int(coords.nbytes),
+                  "d2h_bytes_per_step": int(n * 4 + (G + 1) * 8 + P * n * 4)},
+          "gpu_launches": launches, "desc": desc, "best": stats["best_fitness"]}
+
+
 def main(argv=None) -> int:
   ap = argparse.ArgumentParser()
   ap.add_argument("--gpus", type=int, default=1)
@@ -300,7 +377,12 @@ def main(argv=None) -> int:
   ap.add_argument("--kernel", default="scan", choices=["scan", "scan_unpacked", "cached"])
   ap.add_argument("--cpu-workers", type=int, default=0, help="0: all host cores, capped at 64")
   ap.add_argument("--no-cpu-baseline", action="store_true")
+  ap.add_argument("--workload", default="two_opt", choices=["two_opt", *GA_WORKLOADS])
+  ap.add_argument("--chunk", type=int, default=16, help="GA: generations replayed between host checks")
+  ap.add_argument("--cpu-gens", type=int, default=0, help="GA: generations in the CPU sample (0: workload default)")
   args = ap.parse_args(argv)
+  if args.workload != "two_opt":
+    return main_ga(args)
   world, rank, _ = _dist_env()
   workers = args.cpu_workers or min(os.cpu_count() or 1, 64)
   config = {"workload": "2-opt to local optimum (best and first modes, candidate_k=20) on random tours of a "
@@ -350,6 +432,39 @@ def main(argv=None) -> int:
     line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": workers, "kind": "port",
                             "sample": f"{cpu['tours']} tours (one per process), best then first mode to local optimum, "
                                       f"{cpu['wall_s']:.1f} s wall"}
+  print(json.dumps(line))
+  return 0
+
+
+def main_ga(args) -> int:
+  world, rank, _ = _dist_env()
+  n, P, G, elite, post_init, seed, desc = GA_WORKLOADS[args.workload]
+  sample = args.cpu_gens or {"ga100": 50, "ga1000": 6, "ga2000": 4}[args.workload]
+  config = {"workload": desc, "n": n, "population": P, "generations": G, "elite": elite,
+            "l2": "working set (matrix + population) below L2 for n <= 2000; not flushed between generations"}
+  if args.impl == "reference":
+    if rank != 0:
+      return 0
+    vals = [_ga_cpu_gens_per_s(args.workload, sample) for _ in range(max(1, args.steps))]
+    value = sum(v["gens"] for v in vals) / sum(v["loop_s"] for v in vals)
+    line = {"metric": "generations/s", "value": value, "unit": "generations/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value * G, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)", "impl": "reference",
+            "config": config,
+            "cpu_baseline": {"value": value, "unit": "generations/s", "cores": 1, "kind": "port",
+                             "sample": f"{sample} generations of the NumPy GA per step (init excluded)"},
+            "e2e": {"value": value, "unit": "generations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+  res = run_ga_bench(args)
+  line = {"metric": "generations/s", "value": res["value"], "unit": "generations/s", "n_gpus": 1, "steps": args.steps,
+          "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+          "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)", "config": config, "clocks": res["clocks"],
+          "e2e": res["e2e"], "gpu_launches": res["gpu_launches"], "detail": {"best_fitness": res["best"]}}
+  if not args.no_cpu_baseline:
+    cpu = _ga_cpu_gens_per_s(args.workload, sample)
+    line["cpu_baseline"] = {"value": cpu["value"], "unit": "generations/s", "cores": 1, "kind": "port",
+                            "sample": f"{sample} generations of the NumPy GA (init excluded), {cpu['loop_s']:.1f} s"}
   print(json.dumps(line))
   return 0
 

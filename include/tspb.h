@@ -221,7 +221,8 @@ int tspb_nn_init(const int32_t* customers, int32_t n, const int32_t* cand, int32
  *   MutationCPUPermInversion.mutate_batch (inversion_mutation.py:65-99) and the offspring
  *   EvaluationStep (genetic_algorithm.py:174-199) of one generation.
  * tspb_generation_survival: stable (fitness, index) survival of [pop; off] into new_pop /
- *   new_fit, and tie_flags[g] = 1 when the elite-th and (elite+1)-th survivors tie.
+ *   new_fit; when the elite-th and (elite+1)-th survivors tie it sets tie_flags[g] = 1
+ *   and *stopped = 2 (pause: the host decides the elite membership, then clears it).
  *   Replaces SurvivalStep / _select_survivors_assessed (genetic_algorithm.py:216-251, 618-706).
  * tspb_generation_elite_cost: fitness of rows [0, k) after the elite 2-opt
  *   (EliteOnlyLocalSearchStep re-evaluation, pipeline_steps.py:172-184).
@@ -235,7 +236,7 @@ int tspb_generation_offspring(const int32_t* pop, const double* fit, int32_t P, 
                               const int32_t* gen, const int32_t* stopped, int32_t* off, double* off_fit,
                               void* stream);
 int tspb_generation_survival(const int32_t* pop, const double* fit, const int32_t* off, const double* off_fit,
-                             int32_t P, int32_t n, int32_t elite, const int32_t* gen, const int32_t* stopped,
+                             int32_t P, int32_t n, int32_t elite, const int32_t* gen, int32_t* stopped,
                              int32_t* order, int32_t* new_pop, double* new_fit, int32_t* tie_flags, void* stream);
 int tspb_generation_elite_cost(const int32_t* pop, int32_t k, int32_t n, const int32_t* dist, int64_t dist_stride,
                                const double* coords, const int32_t* stopped, double* fit, void* stream);

@@ -158,10 +158,12 @@ __global__ void survival_rank_kernel(const double* __restrict__ fa, const double
   if (i < count && rank < P) order[rank] = i;
 }
 
-// CTA per survivor: new_pop[r] = combined[order[r]]; flags a fitness tie across the elite edge.
+// CTA per survivor: new_pop[r] = combined[order[r]]. A fitness tie across the elite edge
+// sets tie_flags[g] and pauses the run (*stopped = 2): the elite membership then follows
+// NumPy's unstable argsort, which the host decides before the run resumes.
 __global__ void survival_gather_kernel(const int32_t* __restrict__ pop, const double* __restrict__ fit,
                                        const int32_t* __restrict__ off, const double* __restrict__ off_fit, int P, int n,
-                                       const int32_t* __restrict__ order, const int* __restrict__ stopped,
+                                       const int32_t* __restrict__ order, int* __restrict__ stopped,
                                        const int* __restrict__ gen, int elite, int32_t* __restrict__ new_pop,
                                        double* __restrict__ new_fit, int32_t* __restrict__ tie_flags) {
   if (*stopped) return;
@@ -185,6 +187,13 @@ __global__ void survival_gather_kernel(const int32_t* __restrict__ pop, const do
       tie_flags[*gen] = fe == f ? 1 : 0;
     }
   }
+}
+
+// After the gather (never inside it: its own CTAs read the flag at entry), a tie across
+// the elite edge pauses the run for the host's elite decision.
+__global__ void survival_pause_kernel(const int32_t* __restrict__ tie_flags, const int* __restrict__ gen,
+                                      int* __restrict__ stopped) {
+  if (*stopped == 0 && tie_flags[*gen] != 0) *stopped = 2;
 }
 
 // One CTA: argmin of fitness (first minimum), strict improvement by more than 1e-6 copies
@@ -296,7 +305,7 @@ extern "C" int tspb_generation_offspring(const int32_t* pop, const double* fit, 
 }
 
 extern "C" int tspb_generation_survival(const int32_t* pop, const double* fit, const int32_t* off, const double* off_fit,
-                                        int32_t P, int32_t n, int32_t elite, const int32_t* gen, const int32_t* stopped,
+                                        int32_t P, int32_t n, int32_t elite, const int32_t* gen, int32_t* stopped,
                                         int32_t* order, int32_t* new_pop, double* new_fit, int32_t* tie_flags,
                                         void* stream) {
   if (P < 1 || n < 1 || elite < 0) return TSPB_ERR_ARG;
@@ -306,6 +315,7 @@ extern "C" int tspb_generation_survival(const int32_t* pop, const double* fit, c
   survival_rank_kernel<<<(2 * P + 255) / 256, 256, 0, st>>>(fit, off_fit, P, stopped, order);
   survival_gather_kernel<<<P, 128, 0, st>>>(pop, fit, off, off_fit, P, n, order, stopped, gen, elite, new_pop, new_fit,
                                            tie_flags);
+  if (elite > 0 && elite < P) survival_pause_kernel<<<1, 1, 0, st>>>(tie_flags, gen, stopped);
   return tspb_launch_status();
 }
 

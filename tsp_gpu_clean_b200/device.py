@@ -54,6 +54,22 @@ def device_tensor(a: np.ndarray, dtype) -> "torch.Tensor":
   return t.to(device="cuda", dtype=dtype)
 
 
+_SM_COUNT: int | None = None
+
+
+def auto_threads(num_tours: int) -> int:
+  """CTA size of a one-CTA-per-tour 2-opt launch: wide CTAs when the batch leaves SMs idle,
+  128-thread CTAs (eight resident per SM) when there are several tours per SM."""
+  global _SM_COUNT
+  if _SM_COUNT is None:
+    _SM_COUNT = int(torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count)
+  if num_tours <= _SM_COUNT:
+    return 512
+  if num_tours <= 4 * _SM_COUNT:
+    return 256
+  return 128
+
+
 def check_free(required_bytes: int, what: str) -> None:
   free, _ = torch.cuda.mem_get_info()
   if required_bytes > free:

@@ -23,8 +23,12 @@ captured once per population buffer parity into a CUDA graph and replayed in chu
 
 Elites: survivors come out sorted by (fitness, index), so `argsort(fitness)[:k]` is the
 first k rows unless the k-th and (k+1)-th fitness tie; then membership follows NumPy's
-unstable sort. The survival kernel flags such generations; a chunk that contains one is
-rolled back to its snapshot and that generation runs eagerly with the host `np.argsort`.
+unstable sort, which only the host can reproduce. Once duplicate tours fill the
+population such ties are common (46 of 50 generations of the 100-city run). The
+survival kernel pauses the run on a tie (device flag; every later launch of the chunk is
+a no-op); the host reads the fitness vector, takes `np.argsort`, runs that generation's
+elite step and resumes, with the replay chunk shrinking to one generation after a pause
+and doubling back while no tie occurs.
 Early stop: the tracking kernel sets a device stop flag when patience runs out; later
 launches (the 2-opt through `tspb_two_opt_gated`) become no-ops, and the RNG is rewound
 to its state after the last generation that ran.
@@ -40,7 +44,7 @@ from typing import Any
 import numpy as np
 
 from . import native
-from .device import operands_for, ptr, require_gpu, stream_handle, torch
+from .device import auto_threads, operands_for, ptr, require_gpu, stream_handle, torch
 from .problem import resolve_rng
 from .routes import sample_distinct_pairs
 from .strategies.initialization import InitializationB200TourNearestNeighbor
@@ -51,7 +55,7 @@ class LocalSearchConfig:
   mode: str = "best"
   max_iterations: int = 10
   candidate_k: int | None = 20
-  threads: int = 128
+  threads: int = 0  # 0: chosen per launch from the batch size
 
 
 class FusedMemeticSolver:
@@ -65,6 +69,7 @@ class FusedMemeticSolver:
     self.kt = tournament_k
     self.nn_k = nn_k
     self.ls = local_search if local_search is not None else LocalSearchConfig()
+    self.host_elite_generations = 0
     self.elite = min(elite_count, population_size) if elite_count else 0
     self.post_init = post_init
     self.use_graph = use_graph
@@ -98,9 +103,10 @@ class FusedMemeticSolver:
     ls = self.ls
     lib = native.load_library()
     mode = native.MODE_CODES[ls.mode]
+    threads = int(ls.threads) if ls.threads else auto_threads(num)
     rc = lib.tspb_two_opt_gated(ptr(skip if skip is not None else self.d_zero), rows_ptr, num, self.n, ptr(self.dist),
                                 self.stride, ptr(self.coords), ptr(self.cand), ptr(self.cand_dist), None, None,
-                                ptr(self.packed), self.k, mode, int(ls.max_iterations), int(ls.threads), None,
+                                ptr(self.packed), self.k, mode, int(ls.max_iterations), threads, None,
                                 ptr(self.ls_status), ptr(self.ws), self.ws_bytes, stream_handle())
     native.check("tspb_two_opt_gated", rc)
 
@@ -125,28 +131,21 @@ class FusedMemeticSolver:
     native.check("track", lib.tspb_generation_track(
       ptr(fdst), ptr(dst), self.P, self.n, ptr(self.gen), ptr(self.stopped), ptr(self.stall), int(self.patience),
       ptr(self.best_cost), ptr(self.best_tour), ptr(self.history), ptr(self.done), sh))
-    self.kernel_launches += 6 if self.elite else 4
+    self.kernel_launches += 7 if self.elite else 4
 
-  def _generation_host_elites(self, parity: int) -> None:
-    """Generation with a fitness tie across the elite edge: elites from the host `np.argsort`."""
+  def _host_elites(self, gen: int) -> None:
+    """Elite step of paused generation `gen`: membership from the host `np.argsort`."""
     lib = native.load_library()
-    src, dst = self.pop[parity], self.pop[1 - parity]
-    fsrc, fdst = self.fit[parity], self.fit[1 - parity]
-    t = self.tape
+    dst = self.pop[(gen + 1) % 2]
+    fdst = self.fit[(gen + 1) % 2]
     sh = stream_handle()
-    native.check("offspring", lib.tspb_generation_offspring(
-      ptr(src), ptr(fsrc), self.P, self.n, self.kt, ptr(t[0]), ptr(t[1]), ptr(t[2]), ptr(t[3]), ptr(t[4]), ptr(t[5]),
-      float(self.rate), ptr(self.dist), self.stride, ptr(self.coords), ptr(self.gen), ptr(self.stopped), ptr(self.off),
-      ptr(self.off_fit), sh))
-    native.check("survival", lib.tspb_generation_survival(
-      ptr(src), ptr(fsrc), ptr(self.off), ptr(self.off_fit), self.P, self.n, self.elite, ptr(self.gen), ptr(self.stopped),
-      ptr(self.order), ptr(dst), ptr(fdst), ptr(self.ties), sh))
+    self.stopped.zero_()
     idx = np.argsort(fdst.cpu().numpy())[: self.elite].astype(np.int32)  # pipeline_steps.py:163
     d_idx = torch.from_numpy(idx).cuda()
-    tmp = torch.empty((self.elite, self.n), dtype=torch.int32, device="cuda")
+    tmp = self.elite_tmp
     native.call("tspb_gather_rows", ptr(dst), self.P, self.n, ptr(d_idx), self.elite, ptr(tmp), sh)
-    self._two_opt(ptr(tmp), self.elite, skip=self.stopped)
-    costs = torch.empty(self.elite, dtype=torch.float64, device="cuda")
+    self._two_opt(ptr(tmp), self.elite)
+    costs = self.elite_costs
     native.call("tspb_tour_cost", ptr(tmp), self.elite, self.n, ptr(self.dist), self.stride, ptr(self.coords), 1,
                 ptr(costs), sh)
     native.call("tspb_scatter_rows", ptr(tmp), self.elite, self.n, ptr(d_idx), ptr(dst), self.P, sh)
@@ -154,7 +153,8 @@ class FusedMemeticSolver:
     native.check("track", lib.tspb_generation_track(
       ptr(fdst), ptr(dst), self.P, self.n, ptr(self.gen), ptr(self.stopped), ptr(self.stall), int(self.patience),
       ptr(self.best_cost), ptr(self.best_tour), ptr(self.history), ptr(self.done), sh))
-    torch.cuda.synchronize()
+    self.kernel_launches += 5
+    self.host_elite_generations += 1
 
   # -------------------------------------------------------------------------- evolve
   def evolve(self, context: Any, customers: Any, max_generations: int, patience: int | None = None):
@@ -183,7 +183,7 @@ class FusedMemeticSolver:
       self.cand, self.cand_dist, self.packed, self.k = tabs.cand, tabs.cand_dist, tabs.packed, tabs.k
     lib = native.load_library()
     rows_max = max(self.elite, P if self.post_init else 0, 1)
-    self.ws_bytes = int(lib.tspb_two_opt_workspace_bytes(rows_max, n, self.k, native.MODE_CODES[ls.mode], ls.threads))
+    self.ws_bytes = int(lib.tspb_two_opt_workspace_bytes(rows_max, n, self.k, native.MODE_CODES[ls.mode], 128))
     self.ws = torch.empty(max(self.ws_bytes, 1), dtype=torch.uint8, device="cuda")
     self.ls_status = torch.zeros(rows_max, dtype=torch.int32, device="cuda")
     self.d_zero = torch.zeros(1, dtype=torch.int32, device="cuda")
@@ -207,6 +207,8 @@ class FusedMemeticSolver:
     self.stall = torch.zeros(1, dtype=torch.int32, device="cuda")
     self.done = torch.zeros(1, dtype=torch.int32, device="cuda")
     self.ties = torch.zeros(max(G, 1), dtype=torch.int32, device="cuda")
+    self.elite_tmp = torch.empty((max(self.elite, 1), n), dtype=torch.int32, device="cuda")
+    self.elite_costs = torch.empty(max(self.elite, 1), dtype=torch.float64, device="cuda")
 
     tape_host, states = self._draw_tape(rng, G, n)
     self.tape = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in tape_host]
@@ -221,41 +223,41 @@ class FusedMemeticSolver:
       self.kernel_launches += 2
 
     graphs = self._capture() if (self.use_graph and G > 0) else None
-    per_gen = 6 if self.elite else 4
+    per_gen = 7 if self.elite else 4
     self.kernel_launches = 2 if (self.post_init and G > 0) else 0
     torch.cuda.synchronize()
     t_loop = time.perf_counter()
+    ev_start = torch.cuda.Event(enable_timing=True)
+    ev_end = torch.cuda.Event(enable_timing=True)
+    ev_start.record()
     g = 0
-    parity = 0
+    chunk = self.chunk
+    self.host_elite_generations = 0
     while g < G:
-      c = min(self.chunk, G - g)
-      snap = self._snapshot(parity)
+      c = min(chunk, G - g)
       for q in range(c):
         if graphs is not None:
-          graphs[(parity + q) % 2].replay()
+          graphs[(g + q) % 2].replay()
           self.kernel_launches += per_gen
         else:
-          self._generation((parity + q) % 2)
-      torch.cuda.synchronize()
-      ties = self.ties[g : g + c].cpu().numpy() if self.elite and self.elite < P else np.zeros(c, dtype=np.int32)
-      if ties.any():
-        t0 = int(np.argmax(ties != 0))
-        self._restore(snap, parity)
-        for q in range(t0):
-          if graphs is not None:
-            graphs[(parity + q) % 2].replay()
-            self.kernel_launches += per_gen
-          else:
-            self._generation((parity + q) % 2)
-        self._generation_host_elites((parity + t0) % 2)
-        self.kernel_launches += 8
-        c = t0 + 1
-      g += c
-      parity = (parity + c) % 2
-      if int(self.stopped.item()):
+          self._generation((g + q) % 2)
+      state = int(self.stopped.item())  # synchronises the chunk
+      if state == 2:  # paused on an elite-edge tie at generation gt
+        gt = int(self.gen.item())
+        self._host_elites(gt)
+        g = gt + 1
+        chunk = 1
+        if int(self.stopped.item()) == 1:
+          break
+        continue
+      if state == 1:
         break
+      g += c
+      chunk = min(2 * chunk, self.chunk)
+    ev_end.record()
     torch.cuda.synchronize()
     t_end = time.perf_counter()
+    loop_ms = ev_start.elapsed_time(ev_end)
     if int(self.ls_status.max().item()) != 0:
       raise RuntimeError("2-opt kernel reported a bad tour inside the fused GA")
 
@@ -269,7 +271,7 @@ class FusedMemeticSolver:
     best_cost = float(self.best_cost.item())
     best_tour = self.best_tour.cpu().numpy().astype(np.int32)
     self.last_timing = {"setup_s": t_setup - t_start, "loop_s": t_end - t_loop, "total_s": t_end - t_start,
-                        "generations": done}
+                        "loop_ms_device": loop_ms, "generations": done}
     stats = {
       "initial_fitness": initial_best,
       "best_fitness": best_cost,
@@ -279,6 +281,7 @@ class FusedMemeticSolver:
       "stop_reason": "no_improvements" if done < G else "max_generations",
       "convergence_history": history,
       "kernel_launches": self.kernel_launches,
+      "host_elite_generations": self.host_elite_generations,
     }
     return best_tour, stats
 
@@ -301,19 +304,3 @@ class FusedMemeticSolver:
     torch.cuda.current_stream().wait_stream(stream)
     torch.cuda.synchronize()
     return graphs
-
-  def _snapshot(self, parity: int):
-    return (self.pop[parity].clone(), self.fit[parity].clone(), self.best_cost.clone(), self.best_tour.clone(),
-            self.stall.clone(), self.stopped.clone(), self.gen.clone(), self.done.clone())
-
-  def _restore(self, snap, parity: int) -> None:
-    pop, fit, bc, bt, stall, stopped, gen, done = snap
-    self.pop[parity].copy_(pop)
-    self.fit[parity].copy_(fit)
-    self.best_cost.copy_(bc)
-    self.best_tour.copy_(bt)
-    self.stall.copy_(stall)
-    self.stopped.copy_(stopped)
-    self.gen.copy_(gen)
-    self.done.copy_(done)
-    torch.cuda.synchronize()

@@ -21,7 +21,7 @@ from typing import Any
 import numpy as np
 
 from .. import native
-from ..device import PinnedStager, Workspace, operands_for, ptr, require_gpu, stream_handle, torch
+from ..device import PinnedStager, Workspace, auto_threads, operands_for, ptr, require_gpu, stream_handle, torch
 from ..errors import NotPermutationError
 from ..phase_timer import time_strategy
 from ..routes import ensure_routes_batch, restore_shape
@@ -46,7 +46,7 @@ class LocalSearchB200TourTwoOpt(StrategyBase):
     max_iterations: int = 10,
     mode: str = "best",
     candidate_k: int | None = None,
-    threads_per_block: int = 256,
+    threads_per_block: int | None = None,
     max_matrix_dimension: int | None = None,
   ) -> None:
     super().__init__()
@@ -121,7 +121,8 @@ class LocalSearchB200TourTwoOpt(StrategyBase):
       d_tours = self._stager.upload(host, torch.int32)
       self.h2d_bytes += host.nbytes
     mode = native.MODE_CODES[self.mode]
-    ws_bytes = native.load_library().tspb_two_opt_workspace_bytes(num, n, k, mode, self.threads_per_block)
+    threads = int(self.threads_per_block) if self.threads_per_block else auto_threads(num)
+    ws_bytes = native.load_library().tspb_two_opt_workspace_bytes(num, n, k, mode, threads)
     ws = self._workspace.get(int(ws_bytes))
     stats = torch.empty((num, 4), dtype=torch.int64, device="cuda") if self.collect_stats else None
     status = torch.empty(num, dtype=torch.int32, device="cuda")
@@ -134,7 +135,7 @@ class LocalSearchB200TourTwoOpt(StrategyBase):
     native.call(
       "tspb_two_opt", ptr(d_tours), num, n, ptr(dist), stride, ptr(coords), ptr(cand), ptr(cand_dist), ptr(rev_off),
       ptr(rev_idx), ptr(packed), k, mode,
-      int(self.max_iterations), int(self.threads_per_block), ptr(stats), ptr(status), ptr(ws), int(ws_bytes),
+      int(self.max_iterations), threads, ptr(stats), ptr(status), ptr(ws), int(ws_bytes),
       stream_handle(),
     )
     self.kernel_launches += 1
