@@ -245,6 +245,43 @@ int tspb_generation_track(const double* fit, const int32_t* pop, int32_t P, int3
                           int32_t* best_tour, double* history, int32_t* done_gens, void* stream);
 
 /*
+ * k-nearest-neighbour table on the device (CTA per node): out[u][0..k) ordered by
+ * (distance, node id), self excluded, k <= 64. Counterpart of compute_candidate_list
+ *   (src/distances/matrix.py:140-211) with a fixed tie rule (lower id wins at the k-th
+ *   boundary) where the reference's argpartition leaves the winner unspecified; used for
+ *   bulk preprocessing, while the 2-opt strategies keep the context's host table.
+ */
+int tspb_knn(const int32_t* dist, int64_t dist_stride, const double* coords, int32_t n, int32_t k,
+             int32_t* out, void* stream);
+
+/*
+ * Learned candidate lists (no reference counterpart: the reference uses plain k-NN).
+ * Edge-scoring MLP 5 -> 64 -> 64 -> 1, FP32 master parameters used in BF16, FP32
+ * accumulation, tensor-core layers (mma.sync bf16). Parameter block of
+ * tspb_mlp_param_count() floats: W1[16][64] (rows >= 5 zero), b1[64], W2[64][64], b2[64],
+ * w3[64], b3.
+ * tspb_edge_features: x (n*pool_k rows of 16 bf16) for candidate edges (u, pool[u][s]):
+ *   d/s_u, s/pool_k, rank of u in pool[v] / pool_k, dx/s_u, dy/s_u, s_u = d(u, pool[u][-1]);
+ *   labels (optional) = 1 when v is next to u in the tour given by tour_pos (node -> position).
+ * tspb_mlp_infer: logits of num_edges rows.
+ * tspb_mlp_train_grad: adds d(mean BCE-with-logits)/dparams over the batch to grad and
+ *   the summed loss to *loss.
+ * tspb_mlp_adam: one Adam step on params from grad (grad is zeroed).
+ * tspb_select_topk: out[u][0..k) = pool entries of u with the highest scores.
+ */
+int tspb_mlp_param_count(void);
+int tspb_edge_features(const double* coords, int32_t n, const int32_t* pool, int32_t pool_k,
+                       const int32_t* dist, int64_t dist_stride, const int32_t* tour_pos, uint16_t* x,
+                       float* labels, void* stream);
+int tspb_mlp_infer(const float* params, const uint16_t* x, int64_t num_edges, float* logits, void* stream);
+int tspb_mlp_train_grad(const float* params, const uint16_t* x, const float* labels, int64_t num_edges,
+                        float* grad, float* loss, void* stream);
+int tspb_mlp_adam(float* params, float* grad, float* m, float* v, int32_t step, float lr, float beta1,
+                  float beta2, float eps, float weight_decay, void* stream);
+int tspb_select_topk(const int32_t* pool, const float* scores, int32_t n, int32_t pool_k, int32_t k,
+                     int32_t* out, void* stream);
+
+/*
  * Permutation check: bad[r] = 0 when row r is a permutation of 0..n-1, else 1.
  */
 int tspb_validate_perm(const int32_t* tours, int32_t num_tours, int32_t n, int32_t* bad, void* stream);

@@ -59,6 +59,14 @@ SIGNATURES: dict[str, tuple] = {
   "tspb_generation_survival": (ctypes.c_int, [_p, _p, _p, _p, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _p]),
   "tspb_generation_elite_cost": (ctypes.c_int, [_p, _i32, _i32, _p, _i64, _p, _p, _p, _p]),
   "tspb_generation_track": (ctypes.c_int, [_p, _p, _i32, _i32, _p, _p, _p, _i64, _p, _p, _p, _p, _p]),
+  "tspb_knn": (ctypes.c_int, [_p, _i64, _p, _i32, _i32, _p, _p]),
+  "tspb_mlp_param_count": (ctypes.c_int, []),
+  "tspb_edge_features": (ctypes.c_int, [_p, _i32, _p, _i32, _p, _i64, _p, _p, _p, _p]),
+  "tspb_mlp_infer": (ctypes.c_int, [_p, _p, _i64, _p, _p]),
+  "tspb_mlp_train_grad": (ctypes.c_int, [_p, _p, _p, _i64, _p, _p, _p]),
+  "tspb_mlp_adam": (ctypes.c_int, [_p, _p, _p, _p, _i32, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                   ctypes.c_float, _p]),
+  "tspb_select_topk": (ctypes.c_int, [_p, _p, _i32, _i32, _i32, _p, _p]),
   "tspb_nn_init": (ctypes.c_int, [_p, _i32, _p, _i32, _i32, _p, _i32, _i32, _p, _sz, _p, _p]),
 }
 
