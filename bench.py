@@ -365,6 +365,89 @@ def run_ga_bench(args) -> dict:
           "gpu_launches": launches, "desc": desc, "best": stats["best_fitness"]}
 
 
+def run_learned_bench(args) -> dict:
+  """Learned top-10 vs k-NN top-20 candidates for 2-opt at equal wall time.
+
+  Train: `args.train_instances` generated instances (n log-uniform in [200, 2000], half
+  uniform, half 10-50-cluster mixtures); labels are the edges of the best 2-opt local
+  optimum of nearest-neighbour starts (optionally GA-refined). Evaluate at n = 1000,
+  5000, 10000: both methods refine the same nearest-neighbour starts to a local optimum
+  (best mode); the learned method, being faster per start, keeps refining further starts
+  until it has used the k-NN method's device time. Gap = best length / best length found
+  by either method - 1.
+  """
+  import torch
+
+  from tsp_gpu_clean_b200 import learned
+  from tsp_gpu_clean_b200.build import build_library
+
+  build_library()
+  lc = learned.LearnedCandidates(pool_k=30, seed=0)
+  rng = np.random.default_rng(2024)
+  t0 = time.perf_counter()
+  xs, ys = [], []
+  for i in range(args.train_instances):
+    n = int(round(np.exp(rng.uniform(np.log(200), np.log(2000)))))
+    coords = (instances.uniform_instance(n, 10_000 + i) if i % 2 == 0
+              else instances.clustered_instance(n, int(rng.integers(10, 51)), 30.0, 10_000 + i))
+    inst = learned.device_instance(coords, 30)
+    tour = lc.label_tour(inst, starts=4, seed=i, ga_generations=args.ga_label_generations)
+    x, y = lc.training_edges(inst, tour)
+    xs.append(x)
+    ys.append(y)
+  torch.cuda.synchronize()
+  t_data = time.perf_counter() - t0
+  t_train = lc.fit(xs, ys, epochs=3, batch=1 << 16, lr=3e-3)
+  edges = sum(int(x.shape[0]) for x in xs)
+  del xs, ys
+
+  def timed(fn):
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    out = fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return out, e0.elapsed_time(e1) / 1e3
+
+  rows = []
+  for n in (1000, 5000, 10000):
+    for j in range(args.eval_instances):
+      seed = 90_000 + 100 * n + j
+      coords = instances.uniform_instance(n, seed) if j % 2 == 0 else instances.clustered_instance(n, 30, 30.0, seed)
+      inst = learned.device_instance(coords, 30)
+      starts = learned.nn_starts(inst, args.eval_starts, seed)
+      knn20 = inst.pool[:, :20].contiguous()
+      (t_k, _), time_k = timed(lambda: learned.two_opt_table(inst, starts, knn20, mode="best"))
+      best_k = learned.tour_lengths(inst, t_k).min()
+      tab, time_tab = timed(lambda: lc.table(inst, 10))
+      used = time_tab
+      best_l = np.inf
+      rounds = 0
+      while used < time_k or rounds == 0:
+        st = starts if rounds == 0 else learned.nn_starts(inst, args.eval_starts, seed + 7 * rounds)
+        (t_l, _), dt = timed(lambda: learned.two_opt_table(inst, st, tab, mode="best"))
+        used += dt
+        best_l = min(best_l, learned.tour_lengths(inst, t_l).min())
+        rounds += 1
+        if rounds >= 64:
+          break
+      ref = min(best_k, best_l)
+      rows.append({"n": n, "knn_gap": best_k / ref - 1, "learned_gap": best_l / ref - 1, "knn_s": time_k,
+                   "learned_s": used, "learned_rounds": rounds})
+  by_n = {}
+  for n in (1000, 5000, 10000):
+    rs = [r for r in rows if r["n"] == n]
+    by_n[str(n)] = {"learned_gap_pct": 100 * float(np.mean([r["learned_gap"] for r in rs])),
+                    "knn_gap_pct": 100 * float(np.mean([r["knn_gap"] for r in rs])),
+                    "knn_s": float(np.mean([r["knn_s"] for r in rs])),
+                    "learned_s": float(np.mean([r["learned_s"] for r in rs])),
+                    "learned_rounds": float(np.mean([r["learned_rounds"] for r in rs]))}
+  return {"value": 100 * float(np.mean([r["learned_gap"] for r in rows])),
+          "knn": 100 * float(np.mean([r["knn_gap"] for r in rows])), "by_n": by_n,
+          "train": {"instances": args.train_instances, "edges": edges, "data_s": t_data, "train_s": t_train,
+                    "final_loss": float(np.mean(lc.train_log[-20:]))}}
+
+
 def main(argv=None) -> int:
   ap = argparse.ArgumentParser()
   ap.add_argument("--gpus", type=int, default=1)
@@ -377,10 +460,25 @@ def main(argv=None) -> int:
   ap.add_argument("--kernel", default="scan", choices=["scan", "scan_unpacked", "cached"])
   ap.add_argument("--cpu-workers", type=int, default=0, help="0: all host cores, capped at 64")
   ap.add_argument("--no-cpu-baseline", action="store_true")
-  ap.add_argument("--workload", default="two_opt", choices=["two_opt", *GA_WORKLOADS])
+  ap.add_argument("--workload", default="two_opt", choices=["two_opt", "learned", *GA_WORKLOADS])
+  ap.add_argument("--train-instances", type=int, default=2000)
+  ap.add_argument("--eval-instances", type=int, default=4)
+  ap.add_argument("--eval-starts", type=int, default=8)
+  ap.add_argument("--ga-label-generations", type=int, default=0)
   ap.add_argument("--chunk", type=int, default=16, help="GA: generations replayed between host checks")
   ap.add_argument("--cpu-gens", type=int, default=0, help="GA: generations in the CPU sample (0: workload default)")
   args = ap.parse_args(argv)
+  if args.workload == "learned":
+    res = run_learned_bench(args)
+    print(json.dumps({"metric": "tour gap @ equal wall time, learned top-10 vs k-NN top-20", "value": res["value"],
+                      "unit": "% above best found", "n_gpus": 1, "higher_is_better": False, "data": "synthetic (seeded)",
+                      "dtype": "bf16 weights / fp32 accumulate; int32 tours", "knn_gap_pct": res["knn"],
+                      "by_n": res["by_n"], "train": res["train"],
+                      "config": {"workload": "learned candidates: train on generated instances n in [200, 2000], "
+                                             "evaluate n = 1000, 5000, 10000 (2-opt best, nearest-neighbour starts)",
+                                 "train_instances": args.train_instances, "eval_instances_per_n": args.eval_instances,
+                                 "starts": args.eval_starts}}))
+    return 0
   if args.workload != "two_opt":
     return main_ga(args)
   world, rank, _ = _dist_env()
