@@ -43,7 +43,9 @@ struct Smem {
 };
 
 
-template <int MODE, bool CAND>
+// SMEM: tour arrays in shared memory (addressed with shared-memory instructions), else in
+// the tour's global workspace slice.
+template <int MODE, bool CAND, bool SMEM>
 __global__ void __launch_bounds__(1024) two_opt_kernel(const TwoOptArgs A) {
   extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ Smem S;
@@ -58,11 +60,11 @@ __global__ void __launch_bounds__(1024) two_opt_kernel(const TwoOptArgs A) {
 
   int32_t* g_tour = A.tours + (long long)t * n;
   unsigned char* ws = A.ws ? A.ws + (size_t)t * A.ws_tour_bytes : nullptr;
-  unsigned char* arr = A.arrays_in_smem ? dsm : ws;
+  unsigned char* arr = SMEM ? dsm : ws;
   int* s_tour = reinterpret_cast<int*>(arr);
   int* s_pos = s_tour + n;
   int* s_edge = s_pos + n;
-  unsigned* occ = reinterpret_cast<unsigned*>(dsm + (A.arrays_in_smem ? (size_t)12 * n : 0));
+  unsigned* occ = reinterpret_cast<unsigned*>(dsm + (SMEM ? (size_t)12 * n : 0));
   unsigned long long* keys = MODE == TSPB_MODE_MULTI_MOVE ? reinterpret_cast<unsigned long long*>(ws + A.ws_keys_off) : nullptr;
   const DistSrc ds = A.ds;
   const int k = A.k;
@@ -435,7 +437,7 @@ static Layout two_opt_layout(int n, int k, int mode, bool cand) {
 
 template <int MODE, bool CAND>
 static int launch(const TwoOptArgs& a, int threads, size_t smem, cudaStream_t st) {
-  auto kern = two_opt_kernel<MODE, CAND>;
+  auto kern = a.arrays_in_smem ? two_opt_kernel<MODE, CAND, true> : two_opt_kernel<MODE, CAND, false>;
   if (smem > 48 * 1024) TSPB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   kern<<<a.num_tours, threads, smem, st>>>(a);
   return tspb_launch_status();
@@ -460,7 +462,7 @@ extern "C" size_t tspb_two_opt_workspace_bytes(int32_t num_tours, int32_t n, int
   if (k > 0 && mode != TSPB_MODE_MULTI_MOVE) {
     const size_t c = cached_ws_tour_bytes(n, mode);
     per = per > c ? per : c;
-    const size_t need = two_opt_scan_tour_bytes(n);
+    const size_t need = two_opt_scan_tour_bytes(n, mode);
     const size_t sc = need <= (size_t)smem_optin() - 2048 ? 0 : align256(need);
     per = per > sc ? per : sc;
   }
@@ -489,7 +491,7 @@ static int two_opt_impl(int32_t* tours, int32_t num_tours, int32_t n, const int3
   if (threads % 32 != 0 || threads > 1024) return TSPB_ERR_ARG;
   if (use_cand && mode != TSPB_MODE_MULTI_MOVE && (rev_off == nullptr || rev_idx == nullptr)) {
     if (threads != 64 && threads != 128 && threads != 256 && threads != 512) return TSPB_ERR_ARG;
-    const size_t need = two_opt_scan_tour_bytes(n);
+    const size_t need = two_opt_scan_tour_bytes(n, mode);
     const size_t per = need <= (size_t)smem_optin() - 2048 ? 0 : align256(need);
     if (per > 0 && (workspace == nullptr || workspace_bytes < per * (size_t)num_tours)) return TSPB_ERR_WORKSPACE;
     if (cand_packed != nullptr && n > 65535) return TSPB_ERR_ARG;

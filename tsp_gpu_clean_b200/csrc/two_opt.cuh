@@ -46,6 +46,7 @@ size_t align256(size_t v);
 int launch_two_opt_cached(const TwoOptArgs& a, int mode, int threads, cudaStream_t st);
 size_t two_opt_cached_tour_bytes(int n, int mode);
 int launch_two_opt_scan(const TwoOptArgs& a, int mode, int threads, cudaStream_t st);
-size_t two_opt_scan_tour_bytes(int n);
+size_t two_opt_scan_tour_bytes(int n, int mode);
+int carveout_for(int ctas_per_sm, size_t smem_per_cta);
 
 }  // namespace tspb

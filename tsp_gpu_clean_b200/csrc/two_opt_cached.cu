@@ -168,7 +168,9 @@ struct MinBlocks {
   static constexpr int value = THREADS == 64 ? 16 : THREADS == 128 ? 8 : THREADS == 256 ? 4 : 2;
 };
 
-template <int MODE, int THREADS>
+// SMEM: per-tour arrays in shared memory (shared-memory instructions), else in the tour's
+// global workspace slice.
+template <int MODE, int THREADS, bool SMEM>
 __global__ void __launch_bounds__(THREADS, MinBlocks<THREADS>::value) two_opt_cached_kernel(const TwoOptArgs A) {
   extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ CachedSmem S;
@@ -179,7 +181,7 @@ __global__ void __launch_bounds__(THREADS, MinBlocks<THREADS>::value) two_opt_ca
   if (A.skip != nullptr && *A.skip != 0) return;
 
   int32_t* g_tour = A.tours + (long long)t * n;
-  unsigned char* base = A.arrays_in_smem ? dsm : A.ws + (size_t)t * A.ws_tour_bytes;
+  unsigned char* base = SMEM ? dsm : A.ws + (size_t)t * A.ws_tour_bytes;
   NodeTour T{A.cand, A.cand_dist, A.rev_off, A.rev_idx, A.ds, n, k, rows};
   T.nkey = reinterpret_cast<unsigned long long*>(base);
   T.tour = reinterpret_cast<int*>(T.nkey + (MODE == TSPB_MODE_BEST ? n : 0));
@@ -494,7 +496,7 @@ size_t two_opt_cached_tour_bytes(int n, int mode) {
 
 template <int MODE, int THREADS>
 static int launch_cached(const TwoOptArgs& a, size_t smem, cudaStream_t st) {
-  auto kern = two_opt_cached_kernel<MODE, THREADS>;
+  auto kern = a.arrays_in_smem ? two_opt_cached_kernel<MODE, THREADS, true> : two_opt_cached_kernel<MODE, THREADS, false>;
   if (smem > 48 * 1024) TSPB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   kern<<<a.num_tours, THREADS, smem, st>>>(a);
   return tspb_launch_status();

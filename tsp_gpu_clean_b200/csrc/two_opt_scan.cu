@@ -1,315 +1,77 @@
-// Candidate-mode 2-opt (best / first), full rescan per pass, latency-tuned for sm_100a.
+// Candidate-mode 2-opt (best / first), full rescan per pass: one CTA per tour.
 //
-// Same semantics as the reference scan (src/algorithms/strategies/local_search/two_opt.py:
-// pair order :347-367, gains :237-245, best :386-440, first :442-489, passes :565-595),
-// arranged so that one pass keeps as many independent loads in flight as possible:
-//
-// - the tour is held position- and node-indexed in shared memory: tour[p], pos[a],
-//   succ[a] and eout[a] = d(a, succ[a]); the gain of entry (i, r) with a = tour[i],
-//   c = N_k[a][r] is (d(a,c) - eout[a]) + (d(succ[a], succ[c]) - eout[c]);
-// - the k-NN table and d(a, c) come packed as one u32 per entry (c | d(a,c) << 16) when
-//   both fit 16 bits, so the whole per-instance table (80 KB at n=1000, k=20) stays in L1;
-// - each thread evaluates U entries per round with their loads issued back to back
-//   (k-NN word -> shared-memory lookups -> one L2 gather of d(succ[a], succ[c])).
-//
-// best keeps a per-thread (gain, i*k + r) minimum and reduces once per pass. first
-// publishes the smallest improving index of a round with a shared atomicMin; once set,
-// later rounds only count the pairs the reference still evaluates (validity, no gains).
-#include "two_opt.cuh"
+// The per-tour body (scan_tour, two_opt_scan.cuh) follows the reference scan
+// (src/algorithms/strategies/local_search/two_opt.py:347-367, 386-489, 565-595); this file
+// holds the one-CTA-per-tour launch, its shared-memory carveout policy and the k-NN
+// packing kernel.
+#include "two_opt_scan.cuh"
 
 namespace tspb {
 
-struct ScanSmem {
-  unsigned long long red64[32];
-  long long redll[32];
-  long long total;  // first: valid entries of the current tour (kept exact across passes)
-  unsigned first;
-  int bad;
-  int stop;
-};
-
-template <int THREADS>
-struct ScanMinBlocks {
-  static constexpr int value = THREADS == 64 ? 16 : THREADS == 128 ? 8 : THREADS == 256 ? 4 : 2;
-};
-
-template <int MODE, int THREADS, int U, bool PACKED>
+// SMEM: the tour state lives in shared memory (the compiler then addresses it with
+// shared-memory instructions); otherwise in the per-tour global workspace slice.
+template <int MODE, int THREADS, int U, bool PACKED, bool SMEM>
 __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value) two_opt_scan_kernel(const TwoOptArgs A) {
   extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ ScanSmem S;
-  const int n = A.n, k = A.k, rows = n - 2;
-  const int tid = threadIdx.x;
   const int t = blockIdx.x;
   if (t >= A.num_tours) return;
   if (A.skip != nullptr && *A.skip != 0) return;
-  int32_t* g_tour = A.tours + (long long)t * n;
-  unsigned char* base = A.arrays_in_smem ? dsm : A.ws + (size_t)t * A.ws_tour_bytes;
-  int* tour = reinterpret_cast<int*>(base);
-  int* pos = tour + n;
-  int* succ = pos + n;
-  int* eout = succ + n;
-  int* rcnt = eout + n;  // first: valid entries per row (position), n ints
-  const DistSrc ds = A.ds;
-  const uint32_t* __restrict__ packed = A.cand_packed;
-  const int32_t* __restrict__ cand = A.cand;
-  const int32_t* __restrict__ cdist = A.cand_dist;
-  const int32_t* __restrict__ dist = A.ds.dist;
-  const unsigned stride = (unsigned)A.ds.stride;
-
-  if (tid == 0) {
-    S.bad = 0;
-    S.stop = 0;
-    S.total = 0;
-  }
-  for (int p = tid; p < n; p += THREADS) {
-    tour[p] = g_tour[p];
-    pos[p] = -1;
-  }
-  __syncthreads();
-  for (int p = tid; p < n; p += THREADS) {
-    const int v = tour[p];
-    if ((unsigned)v >= (unsigned)n || atomicExch(&pos[v], p) != -1) S.bad = 1;
-  }
-  __syncthreads();
-  if (S.bad) {
-    if (tid == 0) {
-      if (A.status) A.status[t] = TSPB_ERR_NOT_PERMUTATION;
-      if (A.stats)
-        for (int q = 0; q < 4; ++q) A.stats[(long long)t * 4 + q] = 0;
-    }
-    return;
-  }
-  for (int p = tid; p < n; p += THREADS) {
-    const int x = tour[p], y = tour[p + 1 == n ? 0 : p + 1];
-    succ[x] = y;
-    eout[x] = ds(x, y);
-  }
-  __syncthreads();
-
-  // Valid entries of row i (the pairs the reference scan evaluates for that row).
-  auto row_count = [&](int i) -> int {
-    const int a = tour[i];
-    const int lo = i + 2, span = n - (i == 0) - lo;
-    int c = 0;
-    for (int r0 = 0; r0 < k; r0 += 4) {
-      int cc[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const unsigned ar = (unsigned)a * (unsigned)k + (unsigned)(r0 + u);
-        cc[u] = r0 + u < k ? (PACKED ? (int)(__ldg(packed + ar) & 0xffffu) : __ldg(cand + ar)) : -1;
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-        if ((unsigned)cc[u] < (unsigned)n) c += (unsigned)(pos[cc[u]] - lo) < (unsigned)span;
-    }
-    return c;
-  };
-  if (MODE == TSPB_MODE_FIRST) {
-    long long sum = 0;
-    for (int i = tid; i < n; i += THREADS) {
-      const int v = i < rows ? row_count(i) : 0;
-      rcnt[i] = v;
-      sum += v;
-    }
-    sum = warp_sum(sum);
-    if ((tid & 31) == 0) atomicAdd(reinterpret_cast<unsigned long long*>(&S.total), (unsigned long long)sum);
-    __syncthreads();
-  }
-
-  const int E = rows * k;
-  constexpr int STEP = THREADS * U;
-  const int sq = STEP / k, sr = STEP - (STEP / k) * k;
-  long long passes = 0, moves = 0, my_pairs = 0, my_eval = 0;
-  int err = TSPB_OK;
-  const long long t_start = clock64();
-
-  while (passes < A.max_iter) {
-    if (tid == 0) {
-      if (clock64() - t_start > BUDGET_CYCLES) S.stop = TSPB_ERR_BUDGET;
-      S.first = NO_IDX;
-    }
-    __syncthreads();
-    if (S.stop) {
-      err = S.stop;
-      break;
-    }
-    ++passes;
-    if (MODE == TSPB_MODE_FIRST && tid == 0) my_pairs += S.total;
-    int bgain = 0;            // best: smallest gain of this thread (strictly below 0 to count)
-    unsigned bidx = NO_IDX;   // and its scan index (first in thread order wins ties)
-    int cnt = 0, evals = 0;
-    int ri[U], rr[U], ee[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      ee[u] = u * THREADS + tid;
-      ri[u] = ee[u] / k;
-      rr[u] = ee[u] - ri[u] * k;
-    }
-    for (int e0 = 0; e0 < E; e0 += STEP) {
-      int a[U], c[U], cd[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) a[u] = ee[u] < E ? tour[ri[u]] : -1;
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        c[u] = -1;
-        if (a[u] < 0) continue;
-        const unsigned ar = (unsigned)a[u] * (unsigned)k + (unsigned)rr[u];
-        if (PACKED) {
-          const uint32_t w = __ldg(packed + ar);
-          c[u] = (int)(w & 0xffffu);
-          cd[u] = (int)(w >> 16);
-        } else {
-          c[u] = __ldg(cand + ar);
-          cd[u] = cdist ? __ldg(cdist + ar) : -1;
-        }
-      }
-      bool ok[U];
-      int sa[U], sc[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        ok[u] = false;
-        if ((unsigned)c[u] >= (unsigned)n) continue;
-        const int i = ri[u];
-        // j in (i + 1, lim): one unsigned range test
-        ok[u] = (unsigned)(pos[c[u]] - (i + 2)) < (unsigned)(n - (i == 0) - (i + 2));
-        if (MODE == TSPB_MODE_BEST) cnt += ok[u];
-        if (ok[u]) {
-          sa[u] = succ[a[u]];
-          sc[u] = succ[c[u]];
-        }
-      }
-      int dbd[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u)
-        if (ok[u]) dbd[u] = dist ? __ldcg(dist + ((unsigned)sa[u] * stride + (unsigned)sc[u])) : ds(sa[u], sc[u]);
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        if (!ok[u]) continue;
-        ++evals;
-        const int dac = (PACKED || cd[u] >= 0) ? cd[u] : ds(a[u], c[u]);
-        const int gain = (dac - eout[a[u]]) + (dbd[u] - eout[c[u]]);
-        if (MODE == TSPB_MODE_BEST) {
-          if (gain < bgain) {
-            bgain = gain;
-            bidx = (unsigned)ee[u];
-          }
-        } else if (gain < 0) {
-          atomicMin(&S.first, (unsigned)ee[u]);
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        ee[u] += STEP;
-        rr[u] += sr;
-        ri[u] += sq;
-        if (rr[u] >= k) {
-          rr[u] -= k;
-          ++ri[u];
-        }
-      }
-      if (MODE == TSPB_MODE_FIRST) {
-        __syncthreads();
-        if (S.first != NO_IDX) break;
-      }
-    }
-    my_pairs += cnt;
-    my_eval += evals;
-    unsigned idx;
-    if (MODE == TSPB_MODE_BEST) {
-      const unsigned long long key = bidx == NO_IDX ? NO_KEY : gain_key(bgain, bidx);
-      const unsigned long long best = block_min(key, S.red64);
-      if (best == NO_KEY) break;
-      idx = (unsigned)best;
-    } else {
-      __syncthreads();
-      idx = S.first;
-      if (idx == NO_IDX) break;
-    }
-    const int bi = (int)(idx / (unsigned)k);
-    const int br = (int)(idx - (unsigned)bi * (unsigned)k);
-    const unsigned bar = (unsigned)tour[bi] * (unsigned)k + (unsigned)br;
-    const int ca = PACKED ? (int)(__ldg(packed + bar) & 0xffffu) : __ldg(cand + bar);
-    const int bj = pos[ca];
-    if (bi < 0 || bj <= bi + 1 || bj >= n) {
-      err = TSPB_ERR_RANGE;
-      break;
-    }
-    __syncthreads();
-    {
-      const int lo = bi + 1, hi = bj, half = (hi - lo + 1) >> 1;
-      for (int q = tid; q < half; q += THREADS) {
-        const int x = tour[lo + q], y = tour[hi - q];
-        tour[lo + q] = y;
-        tour[hi - q] = x;
-        pos[y] = lo + q;
-        pos[x] = hi - q;
-      }
-    }
-    __syncthreads();
-    for (int p = bi + tid; p <= bj; p += THREADS) {
-      const int x = tour[p], y = tour[p + 1 == n ? 0 : p + 1];
-      succ[x] = y;
-      eout[x] = ds(x, y);
-    }
-    __syncthreads();
-    ++moves;
-    if (MODE == TSPB_MODE_FIRST) {
-      // Only rows [bi, bj] (and row 0 when bj == n-1) can change their valid count.
-      const int r_hi = bj < rows - 1 ? bj : rows - 1;
-      const bool row0 = bj == n - 1 && bi > 0;
-      const int nr = r_hi - bi + 1 + (row0 ? 1 : 0);
-      long long d = 0;
-      for (int q = tid; q < nr; q += THREADS) {
-        const int i = q < r_hi - bi + 1 ? bi + q : 0;
-        const int v = row_count(i);
-        d += v - rcnt[i];
-        rcnt[i] = v;
-      }
-      d = warp_sum(d);
-      if ((tid & 31) == 0 && d != 0) atomicAdd(reinterpret_cast<unsigned long long*>(&S.total), (unsigned long long)d);
-    }
-  }
-
-  __syncthreads();
-  for (int p = tid; p < n; p += THREADS) g_tour[p] = tour[p];
-  const long long tp = block_sum(my_pairs, S.redll);
-  const long long te = block_sum(my_eval, S.redll);
-  if (tid == 0) {
-    if (A.status) A.status[t] = err;
-    if (A.stats) {
-      long long* st = A.stats + (long long)t * 4;
-      st[0] = passes;
-      st[1] = tp;
-      st[2] = moves;
-      st[3] = te;
-    }
-  }
+  ScanTour T;
+  T.g_tour = A.tours + (long long)t * A.n;
+  T.arrays = SMEM ? dsm : A.ws + (size_t)t * A.ws_tour_bytes;
+  T.n = A.n;
+  T.k = A.k;
+  T.ds = A.ds;
+  T.packed = A.cand_packed;
+  T.cand = A.cand;
+  T.cand_dist = A.cand_dist;
+  T.max_iter = A.max_iter;
+  T.status = A.status ? A.status + t : nullptr;
+  T.stats = A.stats ? A.stats + (long long)t * 4 : nullptr;
+  T.accumulate = 0;
+  T.moved = nullptr;
+  T.converged = nullptr;
+  scan_tour<MODE, THREADS, U, PACKED>(T, S);
 }
 
-size_t two_opt_scan_tour_bytes(int n) { return (size_t)20 * n; }
+size_t two_opt_scan_tour_bytes(int n, int mode) { return scan_tour_state_bytes(n, mode); }
 
-// Shared-memory carveout (percent of the unified L1/shared array) that holds exactly the
-// CTAs this launch keeps resident per SM; the rest stays L1 for the k-NN tables. The
-// default lets the driver take the largest split, which leaves too little L1.
-static int carveout_percent(int num_tours, size_t smem_per_cta, int max_ctas_per_sm) {
-  static int sms = 0, smem_sm = 0;
-  if (sms == 0) {
+// Shared-memory carveout (percent of the unified L1/shared array) that holds exactly
+// `ctas_per_sm` CTAs of `smem_per_cta` dynamic bytes; the rest stays L1 for the k-NN
+// tables. The default lets the driver take the largest split, which leaves too little L1.
+int carveout_for(int ctas_per_sm, size_t smem_per_cta) {
+  static int smem_sm = 0;
+  if (smem_sm == 0) {
     int dev = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
   }
-  if (sms <= 0 || smem_sm <= 0) return -1;
-  int per_sm = (num_tours + sms - 1) / sms;
-  if (per_sm > max_ctas_per_sm) per_sm = max_ctas_per_sm;
-  const long long need = (long long)per_sm * (long long)(smem_per_cta + sizeof(ScanSmem) + 1024);
+  if (smem_sm <= 0 || ctas_per_sm <= 0) return -1;
+  const long long need = (long long)ctas_per_sm * (long long)(smem_per_cta + sizeof(ScanSmem) + 1024);
   int pct = (int)((need * 100 + smem_sm - 1) / smem_sm);
   return pct < 1 ? 1 : (pct > 100 ? 100 : pct);
 }
 
+static int carveout_percent(int num_tours, size_t smem_per_cta, int max_ctas_per_sm) {
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  if (sms <= 0) return -1;
+  int per_sm = (num_tours + sms - 1) / sms;
+  if (per_sm > max_ctas_per_sm) per_sm = max_ctas_per_sm;
+  return carveout_for(per_sm, smem_per_cta);
+}
+
 template <int MODE, int THREADS, int U>
 static int launch_scan(const TwoOptArgs& a, size_t smem, cudaStream_t st) {
-  auto kern = a.cand_packed ? two_opt_scan_kernel<MODE, THREADS, U, true> : two_opt_scan_kernel<MODE, THREADS, U, false>;
+  auto kern = a.arrays_in_smem ? (a.cand_packed ? two_opt_scan_kernel<MODE, THREADS, U, true, true>
+                                                : two_opt_scan_kernel<MODE, THREADS, U, false, true>)
+                               : (a.cand_packed ? two_opt_scan_kernel<MODE, THREADS, U, true, false>
+                                                : two_opt_scan_kernel<MODE, THREADS, U, false, false>);
   if (smem > 48 * 1024) TSPB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int pct = carveout_percent(a.num_tours, smem, ScanMinBlocks<THREADS>::value);
   if (pct > 0) TSPB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
@@ -328,7 +90,7 @@ static int launch_scan_mode(const TwoOptArgs& a, int threads, size_t smem, cudaS
 }
 
 int launch_two_opt_scan(const TwoOptArgs& a, int mode, int threads, cudaStream_t st) {
-  const size_t smem = a.arrays_in_smem ? two_opt_scan_tour_bytes(a.n) : 0;
+  const size_t smem = a.arrays_in_smem ? two_opt_scan_tour_bytes(a.n, mode) : 0;
   if (mode == TSPB_MODE_BEST) return launch_scan_mode<TSPB_MODE_BEST>(a, threads, smem, st);
   return launch_scan_mode<TSPB_MODE_FIRST>(a, threads, smem, st);
 }

@@ -1,0 +1,322 @@
+// Per-tour body of the candidate-mode 2-opt rescan (best / first), shared by the
+// one-CTA-per-tour kernel and the persistent multi-instance batch kernel.
+//
+// Same semantics as the reference scan (src/algorithms/strategies/local_search/two_opt.py:
+// pair order :347-367, gains :237-245, best :386-440, first :442-489, passes :565-595),
+// arranged so that one pass keeps as many independent loads in flight as possible:
+//
+// - the tour is held position- and node-indexed: tour[p], pos[a], succ[a] and
+//   eout[a] = d(a, succ[a]); the gain of entry (i, r) with a = tour[i], c = N_k[a][r] is
+//   (d(a,c) - eout[a]) + (d(succ[a], succ[c]) - eout[c]);
+// - the k-NN table and d(a, c) come packed as one u32 per entry (c | d(a,c) << 16) when
+//   both fit 16 bits, so the whole per-instance table (80 KB at n=1000, k=20) stays in L1;
+// - each thread evaluates U entries per round with their loads issued back to back
+//   (k-NN word -> shared-memory lookups -> one L2 gather of d(succ[a], succ[c]), or an
+//   FP64 rebuild from coordinates when the instance has no matrix).
+//
+// best keeps a per-thread (gain, i*k + r) minimum and reduces once per pass. first
+// publishes the smallest improving index of a round with a shared atomicMin; once set,
+// later rounds only count the pairs the reference still evaluates (validity, no gains).
+#pragma once
+
+#include "two_opt.cuh"
+
+namespace tspb {
+
+struct ScanSmem {
+  unsigned long long red64[32];
+  long long redll[32];
+  long long total;  // first: valid entries of the current tour (kept exact across passes)
+  unsigned first;
+  int bad;
+  int stop;
+};
+
+template <int THREADS>
+struct ScanMinBlocks {
+  static constexpr int value = THREADS == 64 ? 16 : THREADS == 128 ? 8 : THREADS == 256 ? 4 : THREADS == 512 ? 2 : 1;
+};
+
+// Bytes of tour state per tour: tour, pos, succ, eout (+ per-row valid counts for first).
+__host__ __device__ inline size_t scan_tour_state_bytes(int n, int mode) {
+  return (size_t)(mode == TSPB_MODE_FIRST ? 20 : 16) * (size_t)n;
+}
+
+struct ScanTour {
+  int32_t* g_tour;        // the tour in global memory: read at entry, written back at exit
+  unsigned char* arrays;  // scan_tour_state_bytes(n, mode) bytes (shared memory or workspace)
+  int n, k;
+  DistSrc ds;
+  const uint32_t* packed;  // c | d(a, c) << 16 per entry, or nullptr
+  const int32_t* cand;
+  const int32_t* cand_dist;
+  long long max_iter;
+  int32_t* status;   // optional: TSPB status of this tour
+  long long* stats;  // optional: passes, pairs, moves, evaluated gains
+  int accumulate;    // 1: stats are added to the slot and only an error is stored in status
+                     // (sticky across launches); 0: both are overwritten
+  int32_t* moved;    // optional: 1 when at least one move was applied, else 0
+  uint8_t* converged;  // optional: 1 when the refinement ended on a pass without an improving
+                       // move (the tour is then a fixed point of any further refinement)
+};
+
+// Refines one tour with the whole CTA. Every thread of the CTA must call it.
+template <int MODE, int THREADS, int U, bool PACKED>
+__device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
+  const int n = T.n, k = T.k, rows = n - 2;
+  const int tid = threadIdx.x;
+  int32_t* g_tour = T.g_tour;
+  int* tour = reinterpret_cast<int*>(T.arrays);
+  int* pos = tour + n;
+  int* succ = pos + n;
+  int* eout = succ + n;
+  int* rcnt = eout + n;  // first: valid entries per row (position), n ints
+  const DistSrc ds = T.ds;
+  const uint32_t* __restrict__ packed = T.packed;
+  const int32_t* __restrict__ cand = T.cand;
+  const int32_t* __restrict__ cdist = T.cand_dist;
+  const int32_t* __restrict__ dist = T.ds.dist;
+  const unsigned stride = (unsigned)T.ds.stride;
+
+  if (tid == 0) {
+    S.bad = 0;
+    S.stop = 0;
+    S.total = 0;
+  }
+  for (int p = tid; p < n; p += THREADS) {
+    tour[p] = g_tour[p];
+    pos[p] = -1;
+  }
+  __syncthreads();
+  for (int p = tid; p < n; p += THREADS) {
+    const int v = tour[p];
+    if ((unsigned)v >= (unsigned)n || atomicExch(&pos[v], p) != -1) S.bad = 1;
+  }
+  __syncthreads();
+  if (S.bad) {
+    if (tid == 0) {
+      if (T.moved) *T.moved = 0;
+      if (T.converged) *T.converged = 0;
+      if (T.status) *T.status = TSPB_ERR_NOT_PERMUTATION;
+      if (T.stats && !T.accumulate)
+        for (int q = 0; q < 4; ++q) T.stats[q] = 0;
+    }
+    __syncthreads();  // every thread has read S.bad before the caller reuses S
+    return;
+  }
+  for (int p = tid; p < n; p += THREADS) {
+    const int x = tour[p], y = tour[p + 1 == n ? 0 : p + 1];
+    succ[x] = y;
+    eout[x] = ds(x, y);
+  }
+  __syncthreads();
+
+  // Valid entries of row i (the pairs the reference scan evaluates for that row).
+  auto row_count = [&](int i) -> int {
+    const int a = tour[i];
+    const int lo = i + 2, span = n - (i == 0) - lo;
+    int c = 0;
+    for (int r0 = 0; r0 < k; r0 += 4) {
+      int cc[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const unsigned ar = (unsigned)a * (unsigned)k + (unsigned)(r0 + u);
+        cc[u] = r0 + u < k ? (PACKED ? (int)(__ldg(packed + ar) & 0xffffu) : __ldg(cand + ar)) : -1;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if ((unsigned)cc[u] < (unsigned)n) c += (unsigned)(pos[cc[u]] - lo) < (unsigned)span;
+    }
+    return c;
+  };
+  if (MODE == TSPB_MODE_FIRST) {
+    long long sum = 0;
+    for (int i = tid; i < n; i += THREADS) {
+      const int v = i < rows ? row_count(i) : 0;
+      rcnt[i] = v;
+      sum += v;
+    }
+    sum = warp_sum(sum);
+    if ((tid & 31) == 0) atomicAdd(reinterpret_cast<unsigned long long*>(&S.total), (unsigned long long)sum);
+    __syncthreads();
+  }
+
+  const int E = rows * k;
+  constexpr int STEP = THREADS * U;
+  const int sq = STEP / k, sr = STEP - (STEP / k) * k;
+  long long passes = 0, moves = 0, my_pairs = 0, my_eval = 0;
+  int err = TSPB_OK;
+  bool converged = false;  // the last pass found no improving move: a local optimum
+  const long long t_start = clock64();
+
+  while (passes < T.max_iter) {
+    if (tid == 0) {
+      if (clock64() - t_start > BUDGET_CYCLES) S.stop = TSPB_ERR_BUDGET;
+      S.first = NO_IDX;
+    }
+    __syncthreads();
+    if (S.stop) {
+      err = S.stop;
+      break;
+    }
+    ++passes;
+    if (MODE == TSPB_MODE_FIRST && tid == 0) my_pairs += S.total;
+    int bgain = 0;            // best: smallest gain of this thread (strictly below 0 to count)
+    unsigned bidx = NO_IDX;   // and its scan index (first in thread order wins ties)
+    int cnt = 0, evals = 0;
+    int ri[U], rr[U], ee[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      ee[u] = u * THREADS + tid;
+      ri[u] = ee[u] / k;
+      rr[u] = ee[u] - ri[u] * k;
+    }
+    for (int e0 = 0; e0 < E; e0 += STEP) {
+      int a[U], c[U], cd[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) a[u] = ee[u] < E ? tour[ri[u]] : -1;
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        c[u] = -1;
+        if (a[u] < 0) continue;
+        const unsigned ar = (unsigned)a[u] * (unsigned)k + (unsigned)rr[u];
+        if (PACKED) {
+          const uint32_t w = __ldg(packed + ar);
+          c[u] = (int)(w & 0xffffu);
+          cd[u] = (int)(w >> 16);
+        } else {
+          c[u] = __ldg(cand + ar);
+          cd[u] = cdist ? __ldg(cdist + ar) : -1;
+        }
+      }
+      bool ok[U];
+      int sa[U], sc[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        ok[u] = false;
+        if ((unsigned)c[u] >= (unsigned)n) continue;
+        const int i = ri[u];
+        // j in (i + 1, lim): one unsigned range test
+        ok[u] = (unsigned)(pos[c[u]] - (i + 2)) < (unsigned)(n - (i == 0) - (i + 2));
+        if (MODE == TSPB_MODE_BEST) cnt += ok[u];
+        if (ok[u]) {
+          sa[u] = succ[a[u]];
+          sc[u] = succ[c[u]];
+        }
+      }
+      int dbd[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (ok[u]) dbd[u] = dist ? __ldcg(dist + ((unsigned)sa[u] * stride + (unsigned)sc[u])) : ds(sa[u], sc[u]);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (!ok[u]) continue;
+        ++evals;
+        const int dac = (PACKED || cd[u] >= 0) ? cd[u] : ds(a[u], c[u]);
+        const int gain = (dac - eout[a[u]]) + (dbd[u] - eout[c[u]]);
+        if (MODE == TSPB_MODE_BEST) {
+          if (gain < bgain) {
+            bgain = gain;
+            bidx = (unsigned)ee[u];
+          }
+        } else if (gain < 0) {
+          atomicMin(&S.first, (unsigned)ee[u]);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        ee[u] += STEP;
+        rr[u] += sr;
+        ri[u] += sq;
+        if (rr[u] >= k) {
+          rr[u] -= k;
+          ++ri[u];
+        }
+      }
+      if (MODE == TSPB_MODE_FIRST) {
+        __syncthreads();
+        if (S.first != NO_IDX) break;
+      }
+    }
+    my_pairs += cnt;
+    my_eval += evals;
+    unsigned idx;
+    if (MODE == TSPB_MODE_BEST) {
+      const unsigned long long key = bidx == NO_IDX ? NO_KEY : gain_key(bgain, bidx);
+      const unsigned long long best = block_min(key, S.red64);
+      if (best == NO_KEY) {
+        converged = true;
+        break;
+      }
+      idx = (unsigned)best;
+    } else {
+      __syncthreads();
+      idx = S.first;
+      if (idx == NO_IDX) {
+        converged = true;
+        break;
+      }
+    }
+    const int bi = (int)(idx / (unsigned)k);
+    const int br = (int)(idx - (unsigned)bi * (unsigned)k);
+    const unsigned bar = (unsigned)tour[bi] * (unsigned)k + (unsigned)br;
+    const int ca = PACKED ? (int)(__ldg(packed + bar) & 0xffffu) : __ldg(cand + bar);
+    const int bj = pos[ca];
+    if (bi < 0 || bj <= bi + 1 || bj >= n) {
+      err = TSPB_ERR_RANGE;
+      break;
+    }
+    __syncthreads();
+    {
+      const int lo = bi + 1, hi = bj, half = (hi - lo + 1) >> 1;
+      for (int q = tid; q < half; q += THREADS) {
+        const int x = tour[lo + q], y = tour[hi - q];
+        tour[lo + q] = y;
+        tour[hi - q] = x;
+        pos[y] = lo + q;
+        pos[x] = hi - q;
+      }
+    }
+    __syncthreads();
+    for (int p = bi + tid; p <= bj; p += THREADS) {
+      const int x = tour[p], y = tour[p + 1 == n ? 0 : p + 1];
+      succ[x] = y;
+      eout[x] = ds(x, y);
+    }
+    __syncthreads();
+    ++moves;
+    if (MODE == TSPB_MODE_FIRST) {
+      // Only rows [bi, bj] (and row 0 when bj == n-1) can change their valid count.
+      const int r_hi = bj < rows - 1 ? bj : rows - 1;
+      const bool row0 = bj == n - 1 && bi > 0;
+      const int nr = r_hi - bi + 1 + (row0 ? 1 : 0);
+      long long d = 0;
+      for (int q = tid; q < nr; q += THREADS) {
+        const int i = q < r_hi - bi + 1 ? bi + q : 0;
+        const int v = row_count(i);
+        d += v - rcnt[i];
+        rcnt[i] = v;
+      }
+      d = warp_sum(d);
+      if ((tid & 31) == 0 && d != 0) atomicAdd(reinterpret_cast<unsigned long long*>(&S.total), (unsigned long long)d);
+    }
+  }
+
+  __syncthreads();
+  for (int p = tid; p < n; p += THREADS) g_tour[p] = tour[p];
+  const long long tp = block_sum(my_pairs, S.redll);
+  const long long te = block_sum(my_eval, S.redll);
+  if (tid == 0) {
+    if (T.moved) *T.moved = moves > 0 ? 1 : 0;
+    if (T.converged) *T.converged = converged && err == TSPB_OK ? 1 : 0;
+    if (T.status && (!T.accumulate || err != TSPB_OK)) *T.status = err;
+    if (T.stats) {
+      long long* st = T.stats;
+      const long long v[4] = {passes, tp, moves, te};
+      for (int q = 0; q < 4; ++q) st[q] = T.accumulate ? st[q] + v[q] : v[q];
+    }
+  }
+  __syncthreads();  // S.redll is read by every thread before the caller reuses S
+}
+
+}  // namespace tspb
