@@ -337,13 +337,24 @@ def run_ga_bench(args) -> dict:
   n, P, G, elite, post_init, seed, desc = GA_WORKLOADS[args.workload]
   coords = instances.uniform_instance(n, seed)
 
+  from tsp_gpu_clean_b200.autotune import BatchAutotuner
+  from tsp_gpu_clean_b200.batch import FusedBatchSolver
+
+  tuner = BatchAutotuner()
+
   def run_once():
     ctx = ProblemContext(Problem.from_coordinates(coords), seed=42)
-    solver = FusedMemeticSolver(population_size=P, mutation_rate=0.05, tournament_k=5, nn_k=5,
-                                local_search=LocalSearchConfig("best", 10, 20), elite_count=elite, post_init=post_init,
-                                chunk=args.chunk)
+    ls = LocalSearchConfig("best", 10, 20)
     t0 = time.perf_counter()
-    best, stats = solver.evolve(ctx, list(range(n)), G, patience=10**9)
+    if args.engine == "batch":
+      solver = FusedBatchSolver(population_size=P, mutation_rate=0.05, tournament_k=5, nn_k=5, local_search=ls,
+                                elite_count=elite, post_init=post_init, max_matrix_dimension=None, tuner=tuner,
+                                chunk=args.chunk)
+      (best, stats), = solver.evolve([ctx], G, patience=10**9)
+    else:
+      solver = FusedMemeticSolver(population_size=P, mutation_rate=0.05, tournament_k=5, nn_k=5, local_search=ls,
+                                  elite_count=elite, post_init=post_init, chunk=args.chunk)
+      best, stats = solver.evolve(ctx, list(range(n)), G, patience=10**9)
     wall = time.perf_counter() - t0
     return solver, stats, wall
 
@@ -363,6 +374,174 @@ def run_ga_bench(args) -> dict:
           "e2e": {"value": gens / sum(walls), "unit": "generations/s", "h2d_bytes_per_step": int(coords.nbytes),
                   "d2h_bytes_per_step": int(n * 4 + (G + 1) * 8 + P * n * 4)},
           "gpu_launches": launches, "desc": desc, "best": stats["best_fitness"]}
+
+
+# ------------------------------------------------------------------------ uneven batch
+UNEVEN_SEED = 4242
+UNEVEN_DESC = ("uneven batch: {count} instances, n log-uniform in [50, 5000] (half uniform, half 10-50-cluster "
+               "mixtures), population 64, {G} generations, NN init k=5, tournament 5, PMX, inversion 0.05, 2-opt best "
+               "k=20 x10 post-init and on 8 elites; n > 4096 rebuilds distances from FP64 coordinates; one CUDA "
+               "graph replay per generation")
+
+
+def _knn_tables(c):
+  from tsp_gpu_clean_b200.problem import compute_candidate_list
+
+  return {5: compute_candidate_list(5, coords=c), 20: compute_candidate_list(20, coords=c)}
+
+
+def _uneven_inputs(count: int, pool=None):
+  """Coordinates of the batch and their host k-NN tables (k = 5 for the NN init, 20 for
+  2-opt), computed once like a ProblemContext's candidate cache (on the host cores)."""
+  coords = instances.uneven_batch(count, UNEVEN_SEED)
+  order = sorted(range(count), key=lambda i: -len(coords[i]))  # largest first for the pool
+  if pool is not None:
+    tabs = pool.map(_knn_tables, [coords[i] for i in order], chunksize=1)
+  else:
+    tabs = [_knn_tables(coords[i]) for i in order]
+  caches = [None] * count
+  for i, t in zip(order, tabs):
+    caches[i] = t
+  return coords, caches
+
+
+def _uneven_cpu_worker(args):
+  """Oracle GA generations/s on one instance of the batch (init excluded)."""
+  coords, cache, seed, gens = args
+  from oracle import distances as odist
+  from oracle import ga as oga
+
+  D = odist.euc2d_matrix(coords)
+  cfg = oga.GAConfig(population_size=64, mutation_rate=0.05, nn_k=5, tournament_k=5,
+                     local_search=oga.LocalSearchSpec("best", 10, 20), post_init=True, elite_count=8)
+  t0 = time.perf_counter()
+  oga.OracleGA(D, cache.__getitem__, cfg, np.random.default_rng(seed)).evolve(0, patience=10**9)
+  t1 = time.perf_counter()
+  oga.OracleGA(D, cache.__getitem__, cfg, np.random.default_rng(seed)).evolve(gens, patience=10**9)
+  t2 = time.perf_counter()
+  return gens, max((t2 - t1) - (t1 - t0), 1e-9), len(coords)
+
+
+def uneven_cpu_sample(pool, workers: int, coords, caches, gens: int) -> dict:
+  """Aggregate oracle generations/s over a size-stratified sample of the batch, one
+  instance per process (evenly spaced instances in size order)."""
+  order = sorted(range(len(coords)), key=lambda i: len(coords[i]))
+  step = max(1, len(order) // workers)
+  pick = [order[min(j * step + step // 2, len(order) - 1)] for j in range(min(workers, len(order)))]
+  t0 = time.perf_counter()
+  res = pool.map(_uneven_cpu_worker, [(coords[i], caches[i], 1000 + i, gens) for i in pick], chunksize=1)
+  wall = time.perf_counter() - t0
+  # each process runs one GA at a time; the aggregate is the sum of the per-process rates
+  value = sum(g / t for g, t, _ in res)
+  return {"value": value, "instances": len(pick), "sizes": [n for _, _, n in res], "wall_s": wall, "gens": gens}
+
+
+def run_uneven_bench(args) -> dict:
+  import torch
+
+  from tsp_gpu_clean_b200.autotune import BatchAutotuner
+  from tsp_gpu_clean_b200.batch import FusedBatchSolver
+  from tsp_gpu_clean_b200.build import build_library
+  from tsp_gpu_clean_b200.fused import LocalSearchConfig
+  from tsp_gpu_clean_b200.problem import Problem, ProblemContext
+
+  build_library()
+  coords, caches = args.uneven_inputs
+  G = args.generations
+  tuner = BatchAutotuner()
+
+  def run_once():
+    ctxs = [ProblemContext(Problem.from_coordinates(c), seed=1000 + i, candidate_cache=dict(caches[i]))
+            for i, c in enumerate(coords)]
+    solver = FusedBatchSolver(population_size=64, mutation_rate=0.05, tournament_k=5, nn_k=5,
+                              local_search=LocalSearchConfig("best", 10, 20), elite_count=8, post_init=True,
+                              max_matrix_dimension=4096, tuner=tuner, chunk=args.chunk)
+    t0 = time.perf_counter()
+    res = solver.evolve(ctxs, G, patience=10**9)
+    wall = time.perf_counter() - t0
+    return solver, res, wall
+
+  for _ in range(args.warmup):
+    run_once()
+  torch.cuda.synchronize()
+  loop_ms, walls, launches, gens, pairs, tune_s, pauses, ties = [], [], 0, 0, 0, 0.0, 0, 0
+  with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+    for _ in range(args.steps):
+      solver, res, wall = run_once()
+      loop_ms.append(solver.last_timing["loop_ms_device"])
+      walls.append(wall)
+      launches += solver.kernel_launches
+      gens += sum(st["generations_completed"] for _, st in res)
+      pairs += solver.two_opt_totals["pairs"]
+      tune_s += solver.last_timing["tune_s"]
+      pauses += sum(st["host_elite_generations"] for _, st in res)
+      ties += sum(st["elite_edge_ties"] for _, st in res)
+  loop_s = sum(loop_ms) / 1e3
+  total_n = sum(len(c) for c in coords)
+  h2d = sum(c.nbytes for c in coords) + sum(len(c) * (5 + 20) * 4 for c in coords)
+  h2d += len(coords) * G * 64 * (5 * 4 + 4 + 8 + 2 * 4)  # the tape
+  d2h = total_n * 4 + len(coords) * (G + 1) * 8
+  return {"value": gens / loop_s, "ms_per_step": sum(loop_ms) / args.steps, "clocks": clocks.summary(),
+          "e2e": {"value": gens / sum(walls), "unit": "generations/s", "h2d_bytes_per_step": int(h2d),
+                  "d2h_bytes_per_step": int(d2h)},
+          "gpu_launches": launches,
+          "detail": {"deltas_per_s": pairs / loop_s, "tours_evaluated_per_s": gens * (64 + 8) / loop_s,
+                     "replays_per_step": solver.replays, "host_checks_per_step": solver.last_timing["rounds"],
+                     "generations_per_step": gens // args.steps,
+                     "elite_edge_ties_per_step": ties // args.steps, "host_pauses_per_step": pauses // args.steps,
+                     "buckets": [{"n": [b.lo, b.hi], "coords": b.coords, "instances": len(b.items),
+                                  "two_opt_threads": b.two_opt_threads, "offspring_threads": b.offspring_threads}
+                                 for b in solver.buckets],
+                     "setup_s": solver.last_timing["setup_s"], "tune_s_total": tune_s}}
+
+
+def main_uneven(args) -> int:
+  world, rank, _ = _dist_env()
+  count, G = args.instances, args.generations
+  config = {"workload": UNEVEN_DESC.format(count=count, G=G), "instances": count, "population": 64, "generations": G,
+            "elite": 8, "seed": UNEVEN_SEED,
+            "l2": "not flushed: the matrices of the batch (about 1.9 GB) exceed L2 and are re-read every generation"}
+  workers = args.cpu_workers or min(os.cpu_count() or 1, 64)
+  sample_gens = args.cpu_gens or 2
+  if args.impl == "reference":
+    if rank != 0:
+      return 0
+    with mp.get_context("spawn").Pool(workers) as pool:
+      coords, caches = _uneven_inputs(count, pool)
+      vals = [uneven_cpu_sample(pool, workers, coords, caches, sample_gens) for _ in range(max(1, args.steps))]
+    value = statistics.mean(v["value"] for v in vals)
+    line = {"metric": "generations/s (aggregate over instances)", "value": value, "unit": "generations/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * count * G / value, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int32", "data": "synthetic (seeded)", "impl": "reference", "config": config,
+            "cpu_baseline": {"value": value, "unit": "generations/s", "cores": workers, "kind": "port",
+                             "sample": f"{vals[0]['instances']} size-stratified instances (n = {vals[0]['sizes']}), "
+                                       f"{sample_gens} generations each, one process per instance"},
+            "e2e": {"value": value, "unit": "generations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+  pool = mp.get_context("spawn").Pool(workers)  # before the first CUDA call
+  args.uneven_inputs = _uneven_inputs(count, pool)
+  if rank != 0 or world != 1 or args.no_cpu_baseline:
+    pool.close()
+    pool.join()
+    pool = None
+  res = run_uneven_bench(args)
+  line = {"metric": "generations/s (aggregate over instances)", "value": res["value"], "unit": "generations/s",
+          "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
+          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+          "data": "synthetic (seeded)", "config": config, "clocks": res["clocks"], "e2e": res["e2e"],
+          "gpu_launches": res["gpu_launches"], "detail": res["detail"]}
+  if pool is not None:
+    coords, caches = args.uneven_inputs
+    cpu = uneven_cpu_sample(pool, workers, coords, caches, sample_gens)
+    pool.close()
+    pool.join()
+    line["cpu_baseline"] = {"value": cpu["value"], "unit": "generations/s", "cores": workers, "kind": "port",
+                            "sample": f"{cpu['instances']} size-stratified instances (n = {cpu['sizes']}), "
+                                      f"{sample_gens} generations each, one process per instance, {cpu['wall_s']:.1f} s"}
+  print(json.dumps(line))
+  return 0
 
 
 def run_learned_bench(args) -> dict:
@@ -460,12 +639,16 @@ def main(argv=None) -> int:
   ap.add_argument("--kernel", default="scan", choices=["scan", "scan_unpacked", "cached"])
   ap.add_argument("--cpu-workers", type=int, default=0, help="0: all host cores, capped at 64")
   ap.add_argument("--no-cpu-baseline", action="store_true")
-  ap.add_argument("--workload", default="two_opt", choices=["two_opt", "learned", *GA_WORKLOADS])
+  ap.add_argument("--workload", default="two_opt", choices=["two_opt", "learned", "uneven", *GA_WORKLOADS])
+  ap.add_argument("--instances", type=int, default=256, help="uneven: instances in the batch")
+  ap.add_argument("--generations", type=int, default=100, help="uneven: generations")
   ap.add_argument("--train-instances", type=int, default=2000)
   ap.add_argument("--eval-instances", type=int, default=4)
   ap.add_argument("--eval-starts", type=int, default=8)
   ap.add_argument("--ga-label-generations", type=int, default=0)
   ap.add_argument("--chunk", type=int, default=16, help="GA: generations replayed between host checks")
+  ap.add_argument("--engine", default="single", choices=["single", "batch"],
+                  help="GA: one-run fused solver or the multi-instance batch engine with one instance")
   ap.add_argument("--cpu-gens", type=int, default=0, help="GA: generations in the CPU sample (0: workload default)")
   args = ap.parse_args(argv)
   if args.workload == "learned":
@@ -479,6 +662,8 @@ def main(argv=None) -> int:
                                  "train_instances": args.train_instances, "eval_instances_per_n": args.eval_instances,
                                  "starts": args.eval_starts}}))
     return 0
+  if args.workload == "uneven":
+    return main_uneven(args)
   if args.workload != "two_opt":
     return main_ga(args)
   world, rank, _ = _dist_env()

@@ -245,6 +245,114 @@ int tspb_generation_track(const double* fit, const int32_t* pop, int32_t P, int3
                           int32_t* best_tour, double* history, int32_t* done_gens, void* stream);
 
 /*
+ * Uneven multi-instance batch: many independent GA runs (one per instance, instances of
+ * different sizes) advanced together, every generation of every run replayed from one
+ * captured CUDA graph. No reference counterpart as a batch: each run computes exactly what
+ * the tspb_generation_* steps compute for it alone (same tape layout, same survival, elite
+ * and tracking rules); the runs progress independently through a per-instance control
+ * block ctl[i] = {generation, state, stall, done}.
+ *
+ * States: RUN (the next launch sequence runs a whole generation), STOPPED (patience ran
+ * out), PAUSED (the elite set is for the host to decide: it writes the elite rows to
+ * host_elites[i] and sets RESUME), RESUME (the next launch sequence finishes the paused
+ * generation with those elites, then continues), DONE (G generations ran).
+ *
+ * Elite-edge ties: when the elite-th and (elite+1)-th survivors tie, NumPy's unstable
+ * argsort decides which tied rows are elites (EliteOnlyLocalSearchStep,
+ * pipeline_steps.py:163). With the optional `clean` bits (1 = the row is a converged 2-opt
+ * local optimum, whose refinement is skipped because it changes nothing), a tie whose rows
+ * are all converged gives the same population for every choice and the run continues;
+ * any other tie pauses the run.
+ *
+ * Phases of the 2-opt, cost and tracking steps: POSTINIT (every row of parity 0, no gate;
+ * the post-init refinement), RESUME (runs in state RESUME, rows host_elites[i]), RUN (runs
+ * in state RUN, rows [0, elite)).
+ */
+#define TSPB_BATCH_RUN 0
+#define TSPB_BATCH_STOPPED 1
+#define TSPB_BATCH_PAUSED 2
+#define TSPB_BATCH_RESUME 3
+#define TSPB_BATCH_DONE 4
+
+#define TSPB_BATCH_PHASE_POSTINIT 0
+#define TSPB_BATCH_PHASE_RESUME 1
+#define TSPB_BATCH_PHASE_RUN 2
+
+typedef struct tspb_batch_instance {
+  int32_t n;                    /* cities, >= 4 */
+  int32_t k;                    /* k-NN entries per row, 1 <= k <= n - 1 */
+  int64_t pop_offset;           /* element offset of the P x n rows in pop[], off */
+  int64_t node_offset;          /* element offset of the n-slot in best_tour */
+  const int32_t* dist;          /* n x dist_stride int32, or NULL: distances from coords */
+  int64_t dist_stride;
+  const double* coords;         /* n x 2 float64; required when dist is NULL */
+  const uint32_t* cand_packed;  /* n x k words c | d(a, c) << 16 (tspb_candidate_pack) */
+  int64_t patience;             /* generations without a strict improvement before STOPPED */
+} tspb_batch_instance;
+
+typedef struct tspb_batch {
+  int32_t num_instances;
+  int32_t P;                /* population per instance, >= 2 */
+  int32_t kt;               /* tournament size */
+  int32_t elite;            /* elite rows refined per generation, 0..P */
+  int32_t G;                /* generations on the tape */
+  int32_t rows_max;         /* row slots per instance in ls_status / ls_stats (>= P) */
+  double mutation_rate;
+  const tspb_batch_instance* inst; /* device array [num_instances] */
+  int32_t* pop[2];          /* populations; instance i at generation g reads pop[g & 1] */
+  double* fit[2];           /* [I][P] */
+  int32_t* off;             /* offspring rows (pop layout) */
+  double* off_fit;          /* [I][P] */
+  int32_t* order;           /* [I][P] survival scratch */
+  const int32_t* tape_tourn; /* [I][G][P][kt] */
+  const int32_t* tape_cut_a; /* [I][G][P/2] */
+  const int32_t* tape_cut_b; /* [I][G][P/2] */
+  const double* tape_u;      /* [I][G][P] */
+  const int32_t* tape_inv_a; /* [I][G][P] */
+  const int32_t* tape_inv_b; /* [I][G][P] */
+  int32_t* ctl;             /* [I][4] generation, state, stall, done */
+  double* best_cost;        /* [I] */
+  int32_t* best_tour;       /* node_offset-indexed */
+  double* history;          /* [I][G + 1] */
+  int32_t* ties;            /* [I][G] elite-edge tie seen at generation g */
+  const int32_t* host_elites; /* [I][elite] */
+  int32_t* ls_status;       /* [I][rows_max] sticky 2-opt error of each row slot (0: none) */
+  int64_t* ls_stats;        /* optional [I][rows_max][4] passes, pairs, moves, evaluated gains (accumulated) */
+  uint8_t* clean[2];        /* optional [I][P] per population: 1 = converged 2-opt local optimum */
+  uint8_t* off_clean;       /* [I][P] the same for the offspring (required with clean) */
+} tspb_batch;
+
+/* Fitness of every row of pop[parity]; with set_best also the initial best (first
+ * minimum), history[i][0] and ctl (generation 0, RUN, or DONE when G == 0). */
+int tspb_batch_init(const tspb_batch* b, int32_t parity, int32_t set_best, void* stream);
+/* Offspring of generation ctl[i][0] for every RUN instance i in items[0..num_items), CTA
+ * per child row, `threads` per CTA (32..256, multiple of 32); max_n bounds the items' n
+ * (shared memory). Replaces SelectionCPUTournament.select_batch, CrossoverCPUPermPartiallyMapped
+ * and MutationCPUPermInversion for every run (as tspb_generation_offspring). */
+int tspb_batch_offspring(const tspb_batch* b, const int32_t* items, int32_t num_items, int32_t max_n,
+                         int32_t threads, void* stream);
+/* Survival of every RUN instance and the elite-edge tie rule (RUN -> PAUSED); replaces
+ * _select_survivors_assessed (genetic_algorithm.py:618-706) for every run. */
+int tspb_batch_survival(const tspb_batch* b, void* stream);
+/* 2-opt over the (item, row) units of one phase: persistent CTAs (ctas <= 0: every CTA
+ * that fits) take units from the device counter `queue` (zeroed by this call) in item
+ * order; put the largest instances first. `coords` != 0: every item has dist == NULL
+ * (distances rebuilt from coordinates), else every item has a matrix; an item that
+ * disagrees gets TSPB_ERR_UNSUPPORTED in ls_status. mode BEST or FIRST, candidate mode
+ * only, threads 64/128/256/512/1024. Replaces the post-init and elite refinement calls of
+ * LocalSearchCPUTourTwoOpt (pipeline_steps.py:103-125, 153-195) for every run. */
+int tspb_batch_two_opt(const tspb_batch* b, const int32_t* items, int32_t num_items, int32_t max_n,
+                       int32_t coords, int32_t phase, int32_t mode, int64_t max_iterations, int32_t threads,
+                       int32_t ctas, uint32_t* queue, void* stream);
+/* Resident CTAs per SM of tspb_batch_two_opt for this shape (0: does not fit). */
+int tspb_batch_two_opt_occupancy(int32_t max_n, int32_t mode, int32_t threads);
+/* Fitness of the refined rows of a phase (RESUME or RUN). */
+int tspb_batch_elite_cost(const tspb_batch* b, int32_t phase, void* stream);
+/* Best tracking, history, patience and the generation counter of a phase's instances:
+ * RUN/RESUME -> RUN, STOPPED or DONE (genetic_algorithm.py:876-910). */
+int tspb_batch_track(const tspb_batch* b, int32_t phase, void* stream);
+
+/*
  * k-nearest-neighbour table on the device (CTA per node): out[u][0..k) ordered by
  * (distance, node id), self excluded, k <= 64. Counterpart of compute_candidate_list
  *   (src/distances/matrix.py:140-211) with a fixed tie rule (lower id wins at the k-th

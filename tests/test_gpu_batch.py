@@ -1,0 +1,179 @@
+"""The uneven multi-instance batch against the reference's recorded runs and the oracle GA."""
+
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+import pytest
+
+from oracle import distances as odist
+from oracle import ga as oga
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def batch_mod():
+  import torch
+
+  if not torch.cuda.is_available():
+    pytest.skip("no CUDA device")
+  from tsp_gpu_clean_b200.build import build_library
+
+  build_library()
+  from tsp_gpu_clean_b200 import batch
+
+  return batch
+
+
+def _digest(t):
+  return hashlib.sha256(np.ascontiguousarray(t.cpu().numpy(), dtype=np.int32).tobytes()).hexdigest()
+
+
+def _oracle_run(coords, seed, P, rate, elite, post_init, mode, iters, k, G, patience):
+  D = odist.euc2d_matrix(coords)
+  cfg = oga.GAConfig(population_size=P, mutation_rate=rate, nn_k=5, tournament_k=5,
+                     local_search=oga.LocalSearchSpec(mode, iters, k), post_init=post_init, elite_count=elite)
+  cache = {}
+
+  def provider(kk):
+    if kk not in cache:
+      cache[kk] = odist.candidate_list(kk, coords=coords)
+    return cache[kk]
+
+  rng = np.random.default_rng(seed)
+  best, pop, fit, stats, _ = oga.OracleGA(D, provider, cfg, rng).evolve(G, patience=patience)
+  return best, pop, fit, stats, rng
+
+
+def _check_run(solver, res, ctxs, idx, oracle):
+  obest, opop, ofit, ostats, orng = oracle
+  best, stats = res[idx]
+  assert stats["generations_completed"] == ostats["generations_completed"]
+  assert np.array_equal(best, obest)
+  assert np.array_equal(solver.final_population[idx].cpu().numpy(), opop)
+  assert np.array_equal(solver.final_fitness[idx].cpu().numpy(), ofit)
+  assert stats["convergence_history"] == ostats["convergence_history"]
+  assert ctxs[idx].rng.bit_generator.state == orng.bit_generator.state
+
+
+def _lattice(w, h, step=10.0):
+  return np.array([[x * step, y * step] for x in range(w) for y in range(h)], dtype=np.float64)
+
+
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_batch_matches_reference_runs_and_oracle(batch_mod, golden, use_graph):
+  """The 100-city reference runs (fixed and default patience) inside one batch with
+  smaller and larger instances; the largest rebuilds distances from coordinates."""
+  from tsp_gpu_clean_b200.fused import LocalSearchConfig
+  from tsp_gpu_clean_b200.instances import clustered_instance, uniform_instance
+  from tsp_gpu_clean_b200.problem import Problem, ProblemContext
+
+  g = golden("ga.npz")
+  c1 = g["c1_coords"]
+  extra = [(uniform_instance(23, 5), 11), (clustered_instance(150, 6, 30.0, 6), 12), (uniform_instance(61, 7), 13)]
+  specs = [(c1, 42, 10**9), (c1, 42, None)] + [(c, s, 10**9) for c, s in extra]
+  ctxs = [ProblemContext(Problem.from_coordinates(c), seed=s) for c, s, _ in specs]
+  solver = batch_mod.FusedBatchSolver(population_size=128, mutation_rate=0.05, tournament_k=5, nn_k=5,
+                                      local_search=LocalSearchConfig("best", 10, 20), elite_count=16, post_init=True,
+                                      max_matrix_dimension=120, use_graph=use_graph, bucket_bounds=(32, 100, 128))
+  res = solver.evolve(ctxs, 50, patience=[p for _, _, p in specs])
+  assert any(b.coords for b in solver.buckets) and any(not b.coords for b in solver.buckets)
+  for tag, idx in (("c1", 0), ("c1default", 1)):
+    best, stats = res[idx]
+    assert stats["generations_completed"] == int(g[f"{tag}_gens"])
+    assert np.array_equal(np.asarray(stats["convergence_history"]), g[f"{tag}_history"])
+    assert np.array_equal(best, g[f"{tag}_best"])
+    assert _digest(solver.final_population[idx]) == str(g[f"{tag}_digests"][-1])
+    assert np.array_equal(solver.final_fitness[idx].cpu().numpy(), g[f"{tag}_fitness"][-1])
+    assert ctxs[idx].rng.bit_generator.state["state"]["state"] % (1 << 63) == int(g[f"{tag}_rng"][0])
+  for j, (coords, seed) in enumerate(extra):
+    _check_run(solver, res, ctxs, 2 + j, _oracle_run(coords, seed, 128, 0.05, 16, True, "best", 10, 20, 50, 10**9))
+  assert solver.two_opt_totals["pairs"] > 0
+
+
+@pytest.mark.parametrize("iters", [2, 50])
+def test_batch_elite_boundary_ties_match_oracle(batch_mod, iters):
+  """Lattice instances of different sizes tie at the elite edge in most generations. With
+  few 2-opt passes the tied rows are often unconverged (the run pauses for the host's
+  argsort); with many passes they are converged duplicates (settled on the device)."""
+  from tsp_gpu_clean_b200.fused import LocalSearchConfig
+  from tsp_gpu_clean_b200.problem import Problem, ProblemContext
+
+  lattices = [(_lattice(6, 6), 3), (_lattice(5, 7), 4), (_lattice(8, 8), 5), (_lattice(4, 5), 6)]
+  ctxs = [ProblemContext(Problem.from_coordinates(c), seed=s) for c, s in lattices]
+  solver = batch_mod.FusedBatchSolver(population_size=40, mutation_rate=0.3, elite_count=6, post_init=False,
+                                      local_search=LocalSearchConfig("best", iters, 8), max_matrix_dimension=40,
+                                      bucket_bounds=(36,), chunk=4)
+  res = solver.evolve(ctxs, 40, patience=10**9)
+  ties = sum(st["elite_edge_ties"] for _, st in res)
+  host = sum(st["host_elite_generations"] for _, st in res)
+  if iters == 2:
+    assert host > 0
+  else:
+    assert ties > host
+  for idx, (coords, seed) in enumerate(lattices):
+    _check_run(solver, res, ctxs, idx, _oracle_run(coords, seed, 40, 0.3, 6, False, "best", iters, 8, 40, 10**9))
+
+
+def test_batch_first_mode_and_early_stop_match_oracle(batch_mod):
+  from tsp_gpu_clean_b200.fused import LocalSearchConfig
+  from tsp_gpu_clean_b200.instances import uniform_instance
+  from tsp_gpu_clean_b200.problem import Problem, ProblemContext
+
+  insts = [(uniform_instance(n, 100 + n), 200 + n) for n in (9, 40, 77, 130)]
+  ctxs = [ProblemContext(Problem.from_coordinates(c), seed=s) for c, s in insts]
+  solver = batch_mod.FusedBatchSolver(population_size=24, mutation_rate=0.2, elite_count=5, post_init=True,
+                                      local_search=LocalSearchConfig("first", 4, 10), max_matrix_dimension=100)
+  res = solver.evolve(ctxs, 30, patience=3)
+  assert any(st["stopped_early"] for _, st in res)
+  for idx, (coords, seed) in enumerate(insts):
+    _check_run(solver, res, ctxs, idx, _oracle_run(coords, seed, 24, 0.2, 5, True, "first", 4, 10, 30, 3))
+
+
+def test_converged_row_skipping_changes_nothing(batch_mod):
+  """Skipping the refinement of converged rows gives the same runs, with less 2-opt work."""
+  from tsp_gpu_clean_b200.fused import LocalSearchConfig
+  from tsp_gpu_clean_b200.instances import uneven_batch
+  from tsp_gpu_clean_b200.problem import Problem, ProblemContext
+
+  coords = uneven_batch(5, 21, n_min=30, n_max=400)
+  out = []
+  for skip in (True, False):
+    ctxs = [ProblemContext(Problem.from_coordinates(c), seed=50 + i) for i, c in enumerate(coords)]
+    solver = batch_mod.FusedBatchSolver(population_size=32, elite_count=6, skip_converged=skip,
+                                        local_search=LocalSearchConfig("best", 10, 20))
+    res = solver.evolve(ctxs, 25, patience=10**9)
+    out.append(([r[0] for r in res], [p.cpu().numpy() for p in solver.final_population],
+                solver.two_opt_totals["pairs"], [r[1]["convergence_history"] for r in res]))
+  for a, b in zip(out[0][0], out[1][0]):
+    assert np.array_equal(a, b)
+  for a, b in zip(out[0][1], out[1][1]):
+    assert np.array_equal(a, b)
+  assert out[0][3] == out[1][3]
+  assert out[0][2] < out[1][2]
+
+
+def test_autotuner_cache_is_reused(batch_mod, tmp_path):
+  from tsp_gpu_clean_b200.autotune import BatchAutotuner
+  from tsp_gpu_clean_b200.fused import LocalSearchConfig
+  from tsp_gpu_clean_b200.instances import uneven_batch
+  from tsp_gpu_clean_b200.problem import Problem, ProblemContext
+
+  coords = uneven_batch(6, 9, n_min=50, n_max=600)
+  path = str(tmp_path / "tune.json")
+  outs = []
+  for rep in range(2):
+    tuner = BatchAutotuner(cache_path=path)
+    ctxs = [ProblemContext(Problem.from_coordinates(c), seed=i) for i, c in enumerate(coords)]
+    solver = batch_mod.FusedBatchSolver(population_size=16, elite_count=4,
+                                        local_search=LocalSearchConfig("best", 10, 20), tuner=tuner)
+    res = solver.evolve(ctxs, 5, patience=10**9)
+    outs.append([r[0] for r in res])
+    if rep == 0:
+      assert tuner.measured > 0
+    else:
+      assert tuner.measured == 0
+  for a, b in zip(*outs):
+    assert np.array_equal(a, b)

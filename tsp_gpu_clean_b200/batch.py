@@ -1,0 +1,516 @@
+"""Uneven multi-instance batch: many memetic-GA runs advanced by one CUDA graph per generation.
+
+`FusedBatchSolver.evolve(contexts, G)` runs, for every context, exactly the GA that
+`FusedMemeticSolver.evolve(context, range(n), G)` runs on it alone - the reference's
+
+    GeneticAlgorithm(population_size=P, mutation_rate=rate,
+                     initialization=InitializationCPUTourNearestNeighbor(k=nn_k),
+                     selection=SelectionCPUTournament(k=tournament_k),
+                     crossover=CrossoverCPUPermPartiallyMapped(), mutation=MutationCPUPermInversion(),
+                     evaluation=EvaluationCPUCost(), local_search=LocalSearchCPUTourTwoOpt(...),
+                     local_search_stage="none",
+                     pipeline=[PostInitLocalSearchStep(...), EliteOnlyLocalSearchStep(..., elite_count=k)])
+    .evolve(context, customers, max_generations, patience=...)
+
+(`src/algorithms/metaheuristics/genetic_algorithm.py:789-965`,
+`src/algorithms/pipeline_steps.py:85-195`) - with every instance's result (final
+population, fitness, best tour, convergence history, generator state) identical to the
+single run's.
+
+Layout in HBM: the populations of all instances sit in two flat int32 buffers at
+per-instance offsets (P x n rows each), fitness in (I, P) float64 arrays, the tapes of all
+runs in (I, G, ...) arrays, one {generation, state, stall, done} control block per run and
+one "converged" byte per row (a converged 2-opt local optimum is not refined again: the
+refinement would change nothing). Instances with n above `max_matrix_dimension` keep no
+matrix: their distances are rebuilt from FP64 coordinates in every kernel.
+
+Scheduling: instances are grouped into size buckets; each bucket gets its own offspring
+launch and its own persistent elite 2-opt launch (CTA size picked by `BatchAutotuner`).
+One captured graph holds the whole generation for every run and is replayed in chunks
+between host checks.
+
+Elite-edge ties (the elite set then follows NumPy's unstable argsort): when every tied
+row is converged, each argsort choice refines only rows that do not change, so the run
+goes on on the device. Otherwise the run pauses; at the next check the host takes
+`np.argsort` of its fitness, and the run finishes that generation at the start of the
+next replay.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+import time
+from dataclasses import dataclass, field
+from typing import Any, Sequence
+
+import numpy as np
+
+from . import native
+from .autotune import BatchAutotuner
+from .device import operands_for, ptr, require_gpu, stream_handle, torch
+from .fused import LocalSearchConfig, draw_generation_tape
+from .problem import resolve_rng
+from .strategies.initialization import InitializationB200TourNearestNeighbor
+
+#: Upper n of the default size buckets (the last bucket takes every larger instance).
+DEFAULT_BUCKET_BOUNDS = (128, 256, 512, 1024, 2048, 4096)
+TWO_OPT_THREADS = (64, 128, 256, 512, 1024)
+OFFSPRING_THREADS = (64, 128, 256)
+
+
+@dataclass
+class Bucket:
+  """Instances of one size class and the launch shapes chosen for them."""
+
+  lo: int
+  hi: int
+  coords: bool
+  items: list[int] = field(default_factory=list)
+  max_n: int = 0
+  two_opt_threads: int = 128
+  offspring_threads: int = 128
+  d_items: Any = None
+  queue: Any = None
+
+
+def elite_rows(fitness: np.ndarray, elite: int) -> np.ndarray:
+  """Rows of `argsort(fitness)[:elite]` for every row of an (m, P) fitness array.
+
+  `EliteOnlyLocalSearchStep` takes `np.argsort(fitness)[:k]` (`pipeline_steps.py:163`);
+  NumPy sorts each row of a 2-D array along the last axis with the same routine it uses
+  for a 1-D array, so the rows agree with the per-run call, ties included.
+  """
+  return np.argsort(fitness, axis=1)[:, :elite].astype(np.int32)
+
+
+class FusedBatchSolver:
+  def __init__(self, population_size: int = 64, mutation_rate: float = 0.05, tournament_k: int = 5, nn_k: int = 5,
+               local_search: LocalSearchConfig | None = None, elite_count: int = 8, post_init: bool = True,
+               max_matrix_dimension: int | None = 4096, use_graph: bool = True,
+               tuner: BatchAutotuner | None = None, bucket_bounds: Sequence[int] = DEFAULT_BUCKET_BOUNDS,
+               chunk: int = 16, skip_converged: bool = True) -> None:
+    if population_size < 2:
+      raise ValueError("population_size must be >= 2")
+    self.P = int(population_size)
+    self.rate = float(mutation_rate)
+    self.kt = int(tournament_k)
+    self.nn_k = int(nn_k)
+    self.ls = local_search if local_search is not None else LocalSearchConfig()
+    if self.ls.mode not in ("best", "batch", "first"):
+      raise ValueError("the batch 2-opt supports best/batch and first modes")
+    if not self.ls.candidate_k:
+      raise ValueError("the batch 2-opt runs in candidate mode (candidate_k >= 1)")
+    self.elite = min(int(elite_count), self.P) if elite_count else 0
+    self.post_init = bool(post_init)
+    self.max_matrix_dimension = max_matrix_dimension
+    self.use_graph = bool(use_graph)
+    self.chunk = max(1, int(chunk))
+    self.skip_converged = bool(skip_converged)
+    self.tuner = tuner if tuner is not None else BatchAutotuner()
+    self.bucket_bounds = tuple(sorted(int(b) for b in bucket_bounds))
+    self.kernel_launches = 0
+    self.replays = 0
+    self.last_timing: dict[str, float] = {}
+    self.buckets: list[Bucket] = []
+
+  # ------------------------------------------------------------------------ setup
+  def _make_buckets(self, ns: list[int], coords_flags: list[bool]) -> list[Bucket]:
+    buckets: dict[tuple[int, bool], Bucket] = {}
+    bounds = self.bucket_bounds
+    for i, (n, c) in enumerate(zip(ns, coords_flags)):
+      hi_idx = next((j for j, b in enumerate(bounds) if n <= b), len(bounds))
+      lo = bounds[hi_idx - 1] + 1 if hi_idx > 0 else 4
+      hi = bounds[hi_idx] if hi_idx < len(bounds) else 1 << 16
+      b = buckets.setdefault((hi_idx, c), Bucket(lo=lo, hi=hi, coords=c))
+      b.items.append(i)
+    out = []
+    for key in sorted(buckets, key=lambda kc: (-kc[0], kc[1])):
+      b = buckets[key]
+      b.items.sort(key=lambda i: (-ns[i], i))  # largest first: the persistent queue is LPT
+      b.max_n = max(ns[i] for i in b.items)
+      out.append(b)
+    return out
+
+  def _state(self) -> native.BatchState:
+    s = native.BatchState()
+    s.num_instances = self.I
+    s.P = self.P
+    s.kt = self.kt
+    s.elite = self.elite
+    s.G = self.G
+    s.rows_max = self.P
+    s.mutation_rate = self.rate
+    s.inst = self.d_inst.data_ptr()
+    s.pop[0] = self.pop[0].data_ptr()
+    s.pop[1] = self.pop[1].data_ptr()
+    s.fit[0] = self.fit[0].data_ptr()
+    s.fit[1] = self.fit[1].data_ptr()
+    s.off = self.off.data_ptr()
+    s.off_fit = self.off_fit.data_ptr()
+    s.order = self.order.data_ptr()
+    t = self.tape
+    s.tape_tourn, s.tape_cut_a, s.tape_cut_b = t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr()
+    s.tape_u, s.tape_inv_a, s.tape_inv_b = t[3].data_ptr(), t[4].data_ptr(), t[5].data_ptr()
+    s.ctl = self.ctl.data_ptr()
+    s.best_cost = self.best_cost.data_ptr()
+    s.best_tour = self.best_tour.data_ptr()
+    s.history = self.history.data_ptr()
+    s.ties = self.ties.data_ptr()
+    s.host_elites = self.host_elites.data_ptr()
+    s.ls_status = self.ls_status.data_ptr()
+    s.ls_stats = self.ls_stats.data_ptr()
+    if self.skip_converged:
+      s.clean[0] = self.clean[0].data_ptr()
+      s.clean[1] = self.clean[1].data_ptr()
+      s.off_clean = self.off_clean.data_ptr()
+    return s
+
+  # ------------------------------------------------------------------------ launches
+  @property
+  def _mode(self) -> int:
+    return native.MODE_CODES[self.ls.mode]
+
+  def _two_opt(self, st_ref, bucket: Bucket, phase: int, threads: int | None = None) -> None:
+    rc = native.load_library().tspb_batch_two_opt(
+      st_ref, ptr(bucket.d_items), len(bucket.items), bucket.max_n, 1 if bucket.coords else 0, phase, self._mode,
+      int(self.ls.max_iterations), int(threads or bucket.two_opt_threads), 0, ptr(bucket.queue), stream_handle())
+    native.check("tspb_batch_two_opt", rc)
+    self.kernel_launches += 1
+
+  def _offspring(self, st_ref, bucket: Bucket, threads: int | None = None) -> None:
+    rc = native.load_library().tspb_batch_offspring(st_ref, ptr(bucket.d_items), len(bucket.items), bucket.max_n,
+                                                    int(threads or bucket.offspring_threads), stream_handle())
+    native.check("tspb_batch_offspring", rc)
+    self.kernel_launches += 1
+
+  def _generation(self) -> None:
+    """Enqueue one replay: finish RESUME runs, then one generation of every RUN run."""
+    lib = native.load_library()
+    st = ctypes.byref(self.state)
+    sh = stream_handle()
+    R, U = native.TSPB_BATCH_PHASE_RESUME, native.TSPB_BATCH_PHASE_RUN
+    if self.elite:
+      for b in self.buckets:
+        self._two_opt(st, b, R)
+      native.check("tspb_batch_elite_cost", lib.tspb_batch_elite_cost(st, R, sh))
+      native.check("tspb_batch_track", lib.tspb_batch_track(st, R, sh))
+      self.kernel_launches += 2
+    for b in self.buckets:
+      self._offspring(st, b)
+    native.check("tspb_batch_survival", lib.tspb_batch_survival(st, sh))
+    self.kernel_launches += 3
+    if self.elite:
+      for b in self.buckets:
+        self._two_opt(st, b, U)
+      native.check("tspb_batch_elite_cost", lib.tspb_batch_elite_cost(st, U, sh))
+      self.kernel_launches += 1
+    native.check("tspb_batch_track", lib.tspb_batch_track(st, U, sh))
+    self.kernel_launches += 1
+
+  def _launches_per_replay(self) -> int:
+    nb = len(self.buckets)
+    per = nb + 3 + 1  # offspring per bucket, survival (3 kernels), track
+    if self.elite:
+      per += 2 * nb + 3  # two 2-opt phases per bucket, resume cost + track, run cost
+    return per
+
+  # ------------------------------------------------------------------------ autotuning
+  def _tune(self) -> None:
+    """CTA sizes per bucket from the tuner (measured once per shape, then cached)."""
+    lib = native.load_library()
+    name = torch.cuda.get_device_name()
+    for b in self.buckets:
+      if self.elite:
+        units = len(b.items) * self.elite
+        key = self.tuner.key(name, "two_opt", mode=self.ls.mode, k=self.k, iters=int(self.ls.max_iterations),
+                             lo=b.lo, hi=b.hi, coords=b.coords, units=units)
+        cands = [t for t in TWO_OPT_THREADS if lib.tspb_batch_two_opt_occupancy(b.max_n, self._mode, t) > 0]
+        if not cands:
+          raise ValueError(f"instances of n={b.max_n} do not fit the batch 2-opt's shared memory")
+        b.two_opt_threads = self.tuner.choose(key, cands, lambda t, b=b: self._probe_two_opt(b, t))
+      if self.G:
+        key = self.tuner.key(name, "offspring", lo=b.lo, hi=b.hi, coords=b.coords, units=len(b.items) * self.P)
+        b.offspring_threads = self.tuner.choose(key, list(OFFSPRING_THREADS),
+                                                lambda t, b=b: self._probe_offspring(b, t))
+
+  @staticmethod
+  def _timed(fn, reps: int = 3) -> float:
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    fn()  # warm-up (also sets the kernel attributes)
+    torch.cuda.synchronize()
+    start.record()
+    for _ in range(reps):
+      fn()
+    end.record()
+    end.synchronize()
+    return start.elapsed_time(end) / reps
+
+  def _probe_two_opt(self, b: Bucket, threads: int) -> float:
+    """Elite-shaped 2-opt work of one bucket on scratch copies of the initial tours: the
+    first `elite` rows of every instance, refined for up to max_iterations passes."""
+    e = max(self.elite, 2)  # the probe batch needs P >= 2
+    ns = self.ns
+    offs = np.zeros(self.I, dtype=np.int64)
+    offs[1:] = np.cumsum([e * n for n in ns])[:-1]
+    scratch = torch.empty(max(int(e * sum(ns)), 1), dtype=torch.int32, device="cuda")
+    inst = (native.BatchInstance * self.I)()
+    ctypes.memmove(inst, self.h_inst, ctypes.sizeof(inst))
+    for i in range(self.I):
+      inst[i].pop_offset = int(offs[i])
+    d_inst = torch.frombuffer(bytearray(inst), dtype=torch.uint8).cuda()
+    status = torch.zeros((self.I, e), dtype=torch.int32, device="cuda")
+    st = self._state()
+    st.P = e
+    st.rows_max = e
+    st.inst = d_inst.data_ptr()
+    st.ls_status = status.data_ptr()
+    st.ls_stats = None
+    st.pop[0] = st.pop[1] = scratch.data_ptr()
+    st.clean[0] = st.clean[1] = None  # measure the full refinement work
+    st.off_clean = None
+    st_ref = ctypes.byref(st)
+    lib = native.load_library()
+    src = [self.pop[0][self.pop_offsets[i]: self.pop_offsets[i] + e * ns[i]] for i in b.items]
+    dst = [scratch[int(offs[i]): int(offs[i]) + e * ns[i]] for i in b.items]
+
+    def fill():
+      for d, s_ in zip(dst, src):
+        d.copy_(s_)
+
+    def run():
+      fill()
+      rc = lib.tspb_batch_two_opt(st_ref, ptr(b.d_items), len(b.items), b.max_n, 1 if b.coords else 0,
+                                  native.TSPB_BATCH_PHASE_POSTINIT, self._mode, int(self.ls.max_iterations), threads, 0,
+                                  ptr(b.queue), stream_handle())
+      native.check("tspb_batch_two_opt", rc)
+
+    fill_ms = self._timed(fill)
+    ms = self._timed(run)
+    if int(status.max().item()) != 0:
+      raise RuntimeError("2-opt probe reported a bad tour")
+    return max(ms - fill_ms, 0.0)
+
+  def _probe_offspring(self, b: Bucket, threads: int) -> float:
+    # offspring writes only the scratch rows `off`, `off_fit`, `off_clean`: safe on the live state
+    st_ref = ctypes.byref(self.state)
+    return self._timed(lambda: self._offspring(st_ref, b, threads))
+
+  # ------------------------------------------------------------------------ evolve
+  def evolve(self, contexts: Sequence[Any], max_generations: int, patience: Any = None):
+    """Run every context's GA; returns a list of (best_tour, stats) in context order.
+
+    `patience`: one value for every run, or one per context; None means the reference's
+    default int(2 * sqrt(n)) (`genetic_algorithm.py:815-816`)."""
+    require_gpu()
+    t_start = time.perf_counter()
+    P, G, k = self.P, int(max_generations), int(self.ls.candidate_k)
+    self.G, self.I, self.k = G, len(contexts), k
+    self.kernel_launches = 0
+    self.replays = 0
+    if self.I == 0:
+      return []
+    ns = [int(c.dimension) for c in contexts]
+    if min(ns) < 4:
+      raise ValueError("every instance needs dimension >= 4")
+    self.ns = ns
+    rngs = [resolve_rng(c, None) for c in contexts]
+    prefix = np.zeros(self.I + 1, dtype=np.int64)
+    prefix[1:] = np.cumsum(ns)
+    self.pop_offsets = [int(P * prefix[i]) for i in range(self.I)]
+    total = int(prefix[-1])
+
+    # device buffers
+    dev = "cuda"
+    self.pop = [torch.empty(P * total, dtype=torch.int32, device=dev) for _ in range(2)]
+    self.off = torch.empty(P * total, dtype=torch.int32, device=dev)
+    self.fit = [torch.zeros((self.I, P), dtype=torch.float64, device=dev) for _ in range(2)]
+    self.off_fit = torch.zeros((self.I, P), dtype=torch.float64, device=dev)
+    self.order = torch.zeros((self.I, P), dtype=torch.int32, device=dev)
+    self.ctl = torch.zeros((self.I, 4), dtype=torch.int32, device=dev)
+    self.best_cost = torch.zeros(self.I, dtype=torch.float64, device=dev)
+    self.best_tour = torch.zeros(total, dtype=torch.int32, device=dev)
+    self.history = torch.zeros((self.I, G + 1), dtype=torch.float64, device=dev)
+    self.ties = torch.zeros((self.I, max(G, 1)), dtype=torch.int32, device=dev)
+    self.host_elites = torch.zeros((self.I, max(self.elite, 1)), dtype=torch.int32, device=dev)
+    self.ls_status = torch.zeros((self.I, P), dtype=torch.int32, device=dev)
+    self.ls_stats = torch.zeros((self.I, P, 4), dtype=torch.int64, device=dev)
+    self.clean = [torch.zeros((self.I, P), dtype=torch.uint8, device=dev) for _ in range(2)]
+    self.off_clean = torch.zeros((self.I, P), dtype=torch.uint8, device=dev)
+
+    # per instance: NN init (row seeds first), operands, tape
+    init = InitializationB200TourNearestNeighbor(k=self.nn_k, return_gpu=True)
+    h_inst = (native.BatchInstance * self.I)()
+    tapes = [np.empty((self.I, G, P, self.kt), np.int32), np.empty((self.I, G, P // 2), np.int32),
+             np.empty((self.I, G, P // 2), np.int32), np.empty((self.I, G, P), np.float64),
+             np.empty((self.I, G, P), np.int32), np.empty((self.I, G, P), np.int32)]
+    self.states = []
+    self._keep = []
+    coords_flags = []
+    for i, (ctx, n, rng) in enumerate(zip(contexts, ns, rngs)):
+      pop0 = init.initialize(list(range(n)), P, ctx)
+      self.pop[0][self.pop_offsets[i]: self.pop_offsets[i] + P * n].copy_(pop0.reshape(-1))
+      ops = operands_for(ctx)
+      dist, stride, coords = ops.distance_args(n, self.max_matrix_dimension)
+      tabs = ops.candidates(k, ctx.get_cpu_candidate_list(k), n, self.max_matrix_dimension)
+      if tabs.packed is None:
+        raise ValueError(f"instance {i}: k-NN table does not pack into 16-bit ids and distances")
+      tape, states = draw_generation_tape(rng, G, P, self.kt, n)
+      for a, t in zip(tapes, tape):
+        a[i] = t
+      self.states.append(states)
+      self._keep.append((dist, coords, tabs))
+      inst = h_inst[i]
+      inst.n = n
+      inst.k = tabs.k
+      inst.pop_offset = self.pop_offsets[i]
+      inst.node_offset = int(prefix[i])
+      inst.dist = dist.data_ptr() if dist is not None else None
+      inst.dist_stride = int(stride)
+      inst.coords = coords.data_ptr() if coords is not None else None
+      inst.cand_packed = tabs.packed.data_ptr()
+      pat = patience[i] if isinstance(patience, (list, tuple, np.ndarray)) else patience
+      inst.patience = int(pat) if pat is not None else int(2 * math.sqrt(n))
+      coords_flags.append(dist is None)
+    self.h_inst = h_inst
+    self.d_inst = torch.frombuffer(bytearray(h_inst), dtype=torch.uint8).cuda()
+    self.tape = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in tapes]
+    self.state = self._state()
+    st = ctypes.byref(self.state)
+    lib = native.load_library()
+    sh = stream_handle()
+
+    self.buckets = self._make_buckets(ns, coords_flags)
+    for b in self.buckets:
+      b.d_items = torch.tensor(b.items, dtype=torch.int32, device=dev)
+      b.queue = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    # initial fitness and best (before the post-init refinement, like the reference)
+    native.check("tspb_batch_init", lib.tspb_batch_init(st, 0, 1, sh))
+    torch.cuda.synchronize()
+    t_setup = time.perf_counter()
+    self._tune()
+    torch.cuda.synchronize()
+    t_tuned = time.perf_counter()
+    self.kernel_launches = 1
+    initial_best = self.best_cost.cpu().numpy().copy()
+    if self.post_init and G > 0:
+      for b in self.buckets:
+        self._two_opt(st, b, native.TSPB_BATCH_PHASE_POSTINIT)
+      native.check("tspb_batch_init", lib.tspb_batch_init(st, 0, 0, sh))
+      self.kernel_launches += 1
+    stats_before = self.ls_stats.sum(dim=(0, 1)).cpu().numpy()
+
+    graph = self._capture() if (self.use_graph and G > 0) else None
+    per_replay = self._launches_per_replay()
+    torch.cuda.synchronize()
+    t_loop = time.perf_counter()
+    ev_start = torch.cuda.Event(enable_timing=True)
+    ev_end = torch.cuda.Event(enable_timing=True)
+    ev_start.record()
+    ctl_host = torch.empty((self.I, 4), dtype=torch.int32, pin_memory=True)
+    ready = torch.cuda.Event()
+    host_elite_gens = np.zeros(self.I, dtype=np.int64)
+    live = (native.TSPB_BATCH_RUN, native.TSPB_BATCH_PAUSED, native.TSPB_BATCH_RESUME)
+    # Every round (replays, then one host check) advances each live run by a generation
+    # or leaves it paused for the host, who resumes it before the next round.
+    rounds, max_rounds = 0, 2 * G + 2
+    chunk, remaining = min(self.chunk, max(G, 1)), G
+    c = None
+    while G > 0 and rounds < max_rounds:
+      for _ in range(max(1, min(chunk, remaining))):
+        if graph is not None:
+          graph.replay()
+          self.kernel_launches += per_replay
+        else:
+          self._generation()
+        self.replays += 1
+      rounds += 1
+      ctl_host.copy_(self.ctl, non_blocking=True)
+      ready.record()
+      ready.synchronize()
+      c = ctl_host.numpy()
+      paused = np.nonzero(c[:, 1] == native.TSPB_BATCH_PAUSED)[0]
+      if paused.size:
+        parity = (c[paused, 0] + 1) & 1
+        fits = torch.stack(self.fit)[torch.from_numpy(parity).long().cuda(), torch.from_numpy(paused).long().cuda()]
+        rows = elite_rows(fits.cpu().numpy(), self.elite)  # pipeline_steps.py:163
+        he = self.host_elites.cpu().numpy()
+        he[paused] = rows
+        self.host_elites.copy_(torch.from_numpy(he))
+        c = c.copy()
+        c[paused, 1] = native.TSPB_BATCH_RESUME
+        self.ctl.copy_(torch.from_numpy(c))
+        host_elite_gens[paused] += 1
+        chunk = max(1, chunk // 2)
+      else:
+        chunk = min(2 * chunk, self.chunk)
+      alive = np.isin(c[:, 1], live)
+      if not alive.any():
+        break
+      remaining = G - int(c[alive, 0].min())
+    ev_end.record()
+    torch.cuda.synchronize()
+    t_end = time.perf_counter()
+    loop_ms = ev_start.elapsed_time(ev_end)
+    if G > 0 and c is not None and np.isin(c[:, 1], live).any():
+      raise RuntimeError("batch GA did not finish within its round bound")
+    if int(self.ls_status.max().item()) != 0:
+      raise RuntimeError(f"2-opt kernel reported status {int(self.ls_status.max().item())} inside the batch GA")
+
+    # results
+    ctl = self.ctl.cpu().numpy()
+    best_cost = self.best_cost.cpu().numpy()
+    best_tour = self.best_tour.cpu().numpy()
+    history = self.history.cpu().numpy()
+    ties = self.ties.cpu().numpy()
+    stats_all = self.ls_stats.sum(dim=(0, 1)).cpu().numpy() - stats_before
+    results = []
+    self.final_population, self.final_fitness = [], []
+    for i, rng in enumerate(rngs):
+      done = int(ctl[i, 3]) if G > 0 else 0
+      if 0 < done < G:
+        rng.bit_generator.state = self.states[i][done - 1]
+      parity = done % 2
+      n = ns[i]
+      self.final_population.append(self.pop[parity][self.pop_offsets[i]: self.pop_offsets[i] + P * n].view(P, n))
+      self.final_fitness.append(self.fit[parity][i])
+      results.append((best_tour[prefix[i]: prefix[i + 1]].astype(np.int32).copy(), {
+        "initial_fitness": float(initial_best[i]),
+        "best_fitness": float(best_cost[i]),
+        "best_is_feasible": True,
+        "generations_completed": done,
+        "stopped_early": done < G,
+        "stop_reason": "no_improvements" if done < G else "max_generations",
+        "convergence_history": history[i, : done + 1].tolist(),
+        "host_elite_generations": int(host_elite_gens[i]),
+        "elite_edge_ties": int(ties[i, :done].sum()) if G > 0 else 0,
+      }))
+    # 2-opt work inside the generation loop (the post-init refinement excluded)
+    self.two_opt_totals = {"passes": int(stats_all[0]), "pairs": int(stats_all[1]), "moves": int(stats_all[2]),
+                           "evaluated": int(stats_all[3])}
+    self.last_timing = {"setup_s": t_setup - t_start, "tune_s": t_tuned - t_setup, "loop_s": t_end - t_loop,
+                        "total_s": t_end - t_start, "loop_ms_device": loop_ms,
+                        "generations": int(ctl[:, 3].sum()) if G > 0 else 0, "replays": self.replays,
+                        "rounds": rounds}
+    return results
+
+  # ------------------------------------------------------------------------ graph
+  def _capture(self):
+    # Warm every launch path outside capture with every run parked (all kernels no-op).
+    launches = self.kernel_launches
+    saved = self.ctl.clone()
+    self.ctl[:, 1] = native.TSPB_BATCH_DONE
+    self._generation()
+    torch.cuda.synchronize()
+    self.ctl.copy_(saved)
+    stream = torch.cuda.Stream()
+    stream.wait_stream(torch.cuda.current_stream())
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream, capture_error_mode="relaxed"):
+      self._generation()
+    torch.cuda.current_stream().wait_stream(stream)
+    torch.cuda.synchronize()
+    self.kernel_launches = launches
+    return g

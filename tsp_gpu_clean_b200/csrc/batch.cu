@@ -1,0 +1,511 @@
+// Uneven multi-instance batch: many independent memetic-GA runs, one per instance, with
+// instances of different sizes, advanced by one captured launch sequence per generation.
+//
+// Every run computes what the single-run kernels (generation.cu) compute for it alone:
+// the same tape slices, survival order, elite rule, best tracking and patience
+// (genetic_algorithm.py:618-706, 789-965; pipeline_steps.py:153-195). What is new is the
+// data layout and the scheduling:
+//
+// - populations of all instances live in two flat buffers (pop[0], pop[1]) at
+//   per-instance offsets; a run at generation g reads pop[g & 1] and writes pop[(g+1) & 1],
+//   so the same launch sequence serves runs that are at different generations;
+// - a per-instance control block {generation, state, stall, done} gates every kernel;
+// - every row carries a "converged" bit: its last 2-opt refinement ended on a pass with no
+//   improving move, so refining it again changes nothing and is skipped. The bit follows
+//   the row through survival; a child identical to a converged parent inherits it;
+// - an elite-edge fitness tie lets NumPy's unstable argsort choose which tied rows are
+//   elites. When every tied row is converged, each choice refines only rows that do not
+//   change, so the run goes on. Otherwise the run pauses: the host takes the argsort and
+//   the run finishes that generation in the RESUME phase of a later launch sequence while
+//   the other runs continue;
+// - the elite 2-opt is one persistent launch per size bucket whose CTAs take
+//   (instance, row) units from an atomic counter, largest instances first, with the
+//   bucket's CTA size chosen by the host's autotuner.
+//
+// Instances with no distance matrix rebuild every distance from FP64 coordinates with the
+// reference's EUC_2D rounding (DistSrc).
+#include "generation.cuh"
+#include "two_opt_scan.cuh"
+
+namespace tspb {
+
+__device__ __forceinline__ DistSrc inst_ds(const tspb_batch_instance& I) {
+  DistSrc d;
+  d.dist = I.dist;
+  d.stride = I.dist_stride;
+  d.coords = reinterpret_cast<const double2*>(I.coords);
+  return d;
+}
+
+__device__ __forceinline__ int32_t* pop_buf(const tspb_batch& B, int parity) { return parity ? B.pop[1] : B.pop[0]; }
+__device__ __forceinline__ double* fit_buf(const tspb_batch& B, int parity) { return parity ? B.fit[1] : B.fit[0]; }
+__device__ __forceinline__ uint8_t* clean_buf(const tspb_batch& B, int parity) {
+  return parity ? B.clean[1] : B.clean[0];
+}
+
+// State that a phase's steps run in.
+__device__ __forceinline__ int phase_state(int phase) {
+  return phase == TSPB_BATCH_PHASE_RESUME ? TSPB_BATCH_RESUME : TSPB_BATCH_RUN;
+}
+
+// CTA per instance: fitness of every row of pop[parity]; optionally the initial best.
+__global__ void __launch_bounds__(256) batch_init_kernel(const tspb_batch B, int parity, int set_best) {
+  const int i = blockIdx.x;
+  const tspb_batch_instance I = B.inst[i];
+  const DistSrc ds = inst_ds(I);
+  const int P = B.P, n = I.n;
+  const int32_t* pop = pop_buf(B, parity) + I.pop_offset;
+  double* fit = fit_buf(B, parity) + (long long)i * P;
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int r = warp; r < P; r += nw) {
+    const double f = warp_tour_length(pop + (long long)r * n, n, ds);
+    if ((threadIdx.x & 31) == 0) fit[r] = f;
+  }
+  if (!set_best) return;
+  __syncthreads();
+  __shared__ int best_row;
+  if (threadIdx.x == 0) {
+    int b = 0;
+    for (int r = 1; r < P; ++r)
+      if (fit[r] < fit[b]) b = r;  // first minimum (np.argmin)
+    best_row = b;
+    B.best_cost[i] = fit[b];
+    B.history[(long long)i * (B.G + 1)] = fit[b];
+    int* c = B.ctl + 4 * i;
+    c[0] = 0;
+    c[1] = B.G > 0 ? TSPB_BATCH_RUN : TSPB_BATCH_DONE;
+    c[2] = 0;
+    c[3] = 0;
+  }
+  __syncthreads();
+  const int32_t* src = pop + (long long)best_row * n;
+  for (int t = threadIdx.x; t < n; t += blockDim.x) B.best_tour[I.node_offset + t] = src[t];
+}
+
+// CTA per (item, child row).
+__global__ void __launch_bounds__(256) batch_offspring_kernel(const tspb_batch B, const int32_t* __restrict__ items,
+                                                              int max_n) {
+  extern __shared__ int sm[];
+  const int P = B.P;
+  const int it = blockIdx.x / P, row = blockIdx.x - it * P;
+  const int i = items[it];
+  const int* c = B.ctl + 4 * i;
+  if (c[1] != TSPB_BATCH_RUN) return;
+  const long long g = c[0];
+  const tspb_batch_instance I = B.inst[i];
+  if (I.n > max_n) return;  // the host sizes shared memory for the bucket's largest n
+  const int n = I.n, kt = B.kt, pairs = P >> 1;
+  const long long slot = (long long)i * B.G + g;
+  GenTapeSlice sl;
+  sl.tourn = B.tape_tourn + slot * P * kt;
+  sl.cut_a = B.tape_cut_a + slot * pairs;
+  sl.cut_b = B.tape_cut_b + slot * pairs;
+  sl.u = B.tape_u + slot * P;
+  sl.inv_a = B.tape_inv_a + slot * P;
+  sl.inv_b = B.tape_inv_b + slot * P;
+  const int parity = (int)(g & 1);
+  const DistSrc ds = inst_ds(I);
+  const uint8_t* clean = B.clean[0] ? clean_buf(B, parity) + (long long)i * P : nullptr;
+  ChildOrigin origin;
+  offspring_row(pop_buf(B, parity) + I.pop_offset, fit_buf(B, parity) + (long long)i * P, P, n, kt, sl,
+                B.mutation_rate, ds, row, sm, B.off + I.pop_offset + (long long)row * n,
+                B.off_fit + (long long)i * P + row, clean ? &origin : nullptr);
+  if (clean && threadIdx.x == 0)  // a child identical to a converged parent is converged
+    B.off_clean[(long long)i * P + row] =
+        (origin.same[0] && clean[origin.parent[0]]) || (origin.same[1] && clean[origin.parent[1]]) ? 1 : 0;
+}
+
+// CTA per instance: stable rank of the 2P combined fitness (old population first), keep P.
+__global__ void batch_survival_rank_kernel(const tspb_batch B) {
+  extern __shared__ double f2[];
+  const int i = blockIdx.x, P = B.P;
+  const int* c = B.ctl + 4 * i;
+  if (c[1] != TSPB_BATCH_RUN) return;
+  const int parity = c[0] & 1;
+  const double* fa = fit_buf(B, parity) + (long long)i * P;
+  const double* fb = B.off_fit + (long long)i * P;
+  const int count = 2 * P;
+  for (int j = threadIdx.x; j < count; j += blockDim.x) f2[j] = j < P ? fa[j] : fb[j - P];
+  __syncthreads();
+  for (int j = threadIdx.x; j < count; j += blockDim.x) {
+    const double fj = f2[j];
+    int rank = 0;
+    for (int t = 0; t < count; ++t) {
+      const double ft = f2[t];
+      rank += (ft < fj) || (ft == fj && t < j);
+    }
+    if (rank < P) B.order[(long long)i * P + rank] = j;
+  }
+}
+
+// CTA per (instance, survivor): new_pop[r] = combined[order[r]] with its fitness and
+// converged bit; the elite-edge tie flag.
+__global__ void __launch_bounds__(128) batch_survival_gather_kernel(const tspb_batch B) {
+  const int P = B.P;
+  const int i = blockIdx.x / P, r = blockIdx.x - i * P;
+  const int* c = B.ctl + 4 * i;
+  if (c[1] != TSPB_BATCH_RUN) return;
+  const int g = c[0], parity = g & 1;
+  const tspb_batch_instance I = B.inst[i];
+  const int n = I.n;
+  const int32_t* order = B.order + (long long)i * P;
+  const double* fit = fit_buf(B, parity) + (long long)i * P;
+  const double* off_fit = B.off_fit + (long long)i * P;
+  const int o = order[r];
+  const int32_t* src = o < P ? pop_buf(B, parity) + I.pop_offset + (long long)o * n
+                             : B.off + I.pop_offset + (long long)(o - P) * n;
+  int32_t* dst = pop_buf(B, parity ^ 1) + I.pop_offset + (long long)r * n;
+  if ((n & 3) == 0 && ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0) {
+    const int4* s4 = reinterpret_cast<const int4*>(src);
+    int4* d4 = reinterpret_cast<int4*>(dst);
+    for (int t = threadIdx.x; t < (n >> 2); t += blockDim.x) d4[t] = s4[t];
+  } else {
+    for (int t = threadIdx.x; t < n; t += blockDim.x) dst[t] = src[t];
+  }
+  if (threadIdx.x == 0) {
+    const double f = o < P ? fit[o] : off_fit[o - P];
+    fit_buf(B, parity ^ 1)[(long long)i * P + r] = f;
+    if (B.clean[0]) {
+      const uint8_t* cs = clean_buf(B, parity) + (long long)i * P;
+      clean_buf(B, parity ^ 1)[(long long)i * P + r] = o < P ? cs[o] : B.off_clean[(long long)i * P + o - P];
+    }
+    const int e = B.elite;
+    if (e > 0 && e < P && r == e) {
+      const int oe = order[e - 1];
+      const double fe = oe < P ? fit[oe] : off_fit[oe - P];
+      B.ties[(long long)i * B.G + g] = fe == f ? 1 : 0;
+    }
+  }
+}
+
+// Thread per RUN instance, after the gather: an elite-edge tie pauses the run unless every
+// row of the tied group (contiguous: survivors are sorted by (fitness, index)) is converged.
+__global__ void batch_pause_kernel(const tspb_batch B) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= B.num_instances) return;
+  int* c = B.ctl + 4 * i;
+  if (c[1] != TSPB_BATCH_RUN || B.ties[(long long)i * B.G + c[0]] == 0) return;
+  bool settled = false;
+  if (B.clean[0]) {
+    const int P = B.P, e = B.elite, parity = (c[0] + 1) & 1;
+    const double* f = fit_buf(B, parity) + (long long)i * P;
+    const uint8_t* cl = clean_buf(B, parity) + (long long)i * P;
+    const double fe = f[e - 1];
+    int lo = e - 1, hi = e;
+    while (lo > 0 && f[lo - 1] == fe) --lo;
+    while (hi < P && f[hi] == fe) ++hi;
+    settled = true;
+    for (int r = lo; r < hi; ++r) settled = settled && cl[r] != 0;
+  }
+  if (!settled) c[1] = TSPB_BATCH_PAUSED;
+}
+
+// Persistent 2-opt over the (item, row) units of one phase. COORDS: the bucket's
+// instances rebuild distances from coordinates (no matrix); otherwise they all have one.
+template <int MODE, int THREADS, int U, bool COORDS>
+__global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value)
+    batch_two_opt_kernel(const tspb_batch B, const int32_t* __restrict__ items, int num_items, int rows, int phase,
+                         long long max_iter, int max_n, unsigned* __restrict__ queue) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  __shared__ ScanSmem S;
+  __shared__ unsigned s_unit;
+  const unsigned units = (unsigned)num_items * (unsigned)rows;
+  for (;;) {
+    if (threadIdx.x == 0) s_unit = atomicAdd(queue, 1u);
+    __syncthreads();
+    const unsigned u = s_unit;
+    __syncthreads();  // every thread has read s_unit before thread 0 takes the next unit
+    if (u >= units) return;
+    const int it = (int)(u / (unsigned)rows), e = (int)(u - (unsigned)it * (unsigned)rows);
+    const int i = items[it];
+    int parity = 0, row = e;
+    if (phase != TSPB_BATCH_PHASE_POSTINIT) {
+      const int* c = B.ctl + 4 * i;
+      if (c[1] != phase_state(phase)) continue;
+      parity = (c[0] + 1) & 1;
+      if (phase == TSPB_BATCH_PHASE_RESUME) {
+        row = B.host_elites[(long long)i * B.elite + e];
+        if ((unsigned)row >= (unsigned)B.P) {
+          if (threadIdx.x == 0) B.ls_status[(long long)i * B.rows_max + e] = TSPB_ERR_RANGE;
+          continue;
+        }
+      }
+    }
+    uint8_t* clean = B.clean[0] ? clean_buf(B, parity) + (long long)i * B.P + row : nullptr;
+    if (clean && *clean) continue;  // a converged local optimum: refining it changes nothing
+    const tspb_batch_instance I = B.inst[i];
+    if ((I.dist == nullptr) != COORDS || I.n > max_n || I.n < 4 || I.k < 1) {
+      if (threadIdx.x == 0) B.ls_status[(long long)i * B.rows_max + e] = TSPB_ERR_UNSUPPORTED;
+      continue;
+    }
+    ScanTour T;
+    T.g_tour = pop_buf(B, parity) + I.pop_offset + (long long)row * I.n;
+    T.arrays = dsm;
+    T.n = I.n;
+    T.k = I.k;
+    T.ds.dist = COORDS ? nullptr : I.dist;
+    T.ds.stride = COORDS ? 0 : I.dist_stride;
+    T.ds.coords = COORDS ? reinterpret_cast<const double2*>(I.coords) : nullptr;
+    T.packed = I.cand_packed;
+    T.cand = nullptr;
+    T.cand_dist = nullptr;
+    T.max_iter = max_iter;
+    T.status = B.ls_status + (long long)i * B.rows_max + e;
+    T.stats = B.ls_stats ? reinterpret_cast<long long*>(B.ls_stats) + ((long long)i * B.rows_max + e) * 4 : nullptr;
+    T.accumulate = 1;
+    T.moved = nullptr;
+    T.converged = clean;
+    scan_tour<MODE, THREADS, U, true>(T, S);
+  }
+}
+
+// Warp per (instance, refined row) of a phase: fitness after the 2-opt.
+__global__ void batch_elite_cost_kernel(const tspb_batch B, int phase) {
+  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int e_count = B.elite;
+  if (w >= (long long)B.num_instances * e_count) return;
+  const int i = (int)(w / e_count), e = (int)(w - (long long)i * e_count);
+  const int* c = B.ctl + 4 * i;
+  if (c[1] != phase_state(phase)) return;
+  const int parity = (c[0] + 1) & 1;
+  const int row = phase == TSPB_BATCH_PHASE_RESUME ? B.host_elites[(long long)i * e_count + e] : e;
+  if ((unsigned)row >= (unsigned)B.P) return;
+  const tspb_batch_instance I = B.inst[i];
+  const double f = warp_tour_length(pop_buf(B, parity) + I.pop_offset + (long long)row * I.n, I.n, inst_ds(I));
+  if ((threadIdx.x & 31) == 0) fit_buf(B, parity)[(long long)i * B.P + row] = f;
+}
+
+// CTA per instance of a phase: argmin of fitness (first minimum), strict improvement by
+// more than 1e-6 copies the tour, history[g + 1] = best so far, patience, generation + 1.
+__global__ void __launch_bounds__(128) batch_track_kernel(const tspb_batch B, int phase) {
+  const int i = blockIdx.x;
+  int* c = B.ctl + 4 * i;
+  if (c[1] != phase_state(phase)) return;
+  __shared__ double sv[32];
+  __shared__ int si[32];
+  __shared__ int improve;
+  const int P = B.P, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int g = c[0], parity = (g + 1) & 1;
+  const tspb_batch_instance I = B.inst[i];
+  const double* fit = fit_buf(B, parity) + (long long)i * P;
+  double bv = __longlong_as_double(0x7ff0000000000000LL);
+  int bi = P;
+  for (int r = tid; r < P; r += blockDim.x) {
+    const double f = fit[r];
+    if (f < bv || (f == bv && r < bi)) {
+      bv = f;
+      bi = r;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(FULL, bv, o);
+    const int oi = __shfl_xor_sync(FULL, bi, o);
+    if (ov < bv || (ov == bv && oi < bi)) {
+      bv = ov;
+      bi = oi;
+    }
+  }
+  if (lane == 0) {
+    sv[wid] = bv;
+    si[wid] = bi;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+      if (sv[w] < bv || (sv[w] == bv && si[w] < bi)) {
+        bv = sv[w];
+        bi = si[w];
+      }
+    si[0] = bi;
+    double best = B.best_cost[i];
+    improve = bv < best - 1e-6;
+    int stall = c[2];
+    if (improve) {
+      best = bv;
+      B.best_cost[i] = bv;
+      stall = 0;
+    } else {
+      stall += 1;
+    }
+    B.history[(long long)i * (B.G + 1) + g + 1] = best;
+    c[2] = stall;
+    c[3] = g + 1;
+    c[0] = g + 1;
+    c[1] = stall >= I.patience ? TSPB_BATCH_STOPPED : (g + 1 >= B.G ? TSPB_BATCH_DONE : TSPB_BATCH_RUN);
+  }
+  __syncthreads();
+  if (improve) {
+    const int32_t* src = pop_buf(B, parity) + I.pop_offset + (long long)si[0] * I.n;
+    for (int t = tid; t < I.n; t += blockDim.x) B.best_tour[I.node_offset + t] = src[t];
+  }
+}
+
+template <int MODE, int THREADS, int U>
+static int batch_two_opt_launch(const tspb_batch& b, const int32_t* items, int num_items, int rows, int phase,
+                                long long max_iter, int max_n, size_t smem, int ctas, int coords, unsigned* queue,
+                                cudaStream_t st) {
+  auto kern = coords ? batch_two_opt_kernel<MODE, THREADS, U, true> : batch_two_opt_kernel<MODE, THREADS, U, false>;
+  TSPB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  TSPB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem));
+  if (per_sm <= 0) return TSPB_ERR_UNSUPPORTED;
+  int dev = 0, sms = 0;
+  TSPB_CUDA_CHECK(cudaGetDevice(&dev));
+  TSPB_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const long long units = (long long)num_items * rows;
+  long long grid = (long long)per_sm * sms;
+  if (ctas > 0 && ctas < grid) grid = ctas;
+  if (grid > units) grid = units;
+  const int per_sm_used = (int)((grid + sms - 1) / sms);
+  const int pct = carveout_for(per_sm_used < per_sm ? per_sm_used : per_sm, smem);
+  if (pct > 0) TSPB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+  TSPB_CUDA_CHECK(cudaMemsetAsync(queue, 0, sizeof(unsigned), st));
+  kern<<<(int)grid, THREADS, smem, st>>>(b, items, num_items, rows, phase, max_iter, max_n, queue);
+  return tspb_launch_status();
+}
+
+template <int MODE, int THREADS, int U>
+static int batch_two_opt_occ(size_t smem) {
+  auto kern = batch_two_opt_kernel<MODE, THREADS, U, false>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem) != cudaSuccess) return 0;
+  return per_sm;
+}
+
+template <int MODE>
+static int batch_two_opt_mode(const tspb_batch& b, const int32_t* items, int num_items, int rows, int phase,
+                              long long max_iter, int max_n, int threads, size_t smem, int ctas, int coords,
+                              unsigned* queue, cudaStream_t st) {
+  switch (threads) {
+    case 64:
+      return batch_two_opt_launch<MODE, 64, 4>(b, items, num_items, rows, phase, max_iter, max_n, smem, ctas, coords,
+                                               queue, st);
+    case 128:
+      return batch_two_opt_launch<MODE, 128, 4>(b, items, num_items, rows, phase, max_iter, max_n, smem, ctas, coords,
+                                                queue, st);
+    case 256:
+      return batch_two_opt_launch<MODE, 256, 4>(b, items, num_items, rows, phase, max_iter, max_n, smem, ctas, coords,
+                                                queue, st);
+    case 512:
+      return batch_two_opt_launch<MODE, 512, 2>(b, items, num_items, rows, phase, max_iter, max_n, smem, ctas, coords,
+                                                queue, st);
+    case 1024:
+      return batch_two_opt_launch<MODE, 1024, 2>(b, items, num_items, rows, phase, max_iter, max_n, smem, ctas, coords,
+                                                 queue, st);
+    default: return TSPB_ERR_ARG;
+  }
+}
+
+template <int MODE>
+static int batch_two_opt_occ_mode(int threads, size_t smem) {
+  switch (threads) {
+    case 64: return batch_two_opt_occ<MODE, 64, 4>(smem);
+    case 128: return batch_two_opt_occ<MODE, 128, 4>(smem);
+    case 256: return batch_two_opt_occ<MODE, 256, 4>(smem);
+    case 512: return batch_two_opt_occ<MODE, 512, 2>(smem);
+    case 1024: return batch_two_opt_occ<MODE, 1024, 2>(smem);
+    default: return 0;
+  }
+}
+
+}  // namespace tspb
+
+using namespace tspb;
+
+static bool batch_ok(const tspb_batch* b) {
+  if (b == nullptr || b->num_instances < 0 || b->P < 2 || b->kt < 1 || b->elite < 0 || b->elite > b->P || b->G < 0)
+    return false;
+  if (b->rows_max < b->P) return false;
+  if ((b->clean[0] == nullptr) != (b->clean[1] == nullptr)) return false;
+  if (b->num_instances == 0) return true;
+  return b->inst && b->pop[0] && b->pop[1] && b->fit[0] && b->fit[1] && b->off && b->off_fit && b->order && b->ctl &&
+         b->best_cost && b->best_tour && b->history && b->ls_status;
+}
+
+static bool tape_ok(const tspb_batch* b) {
+  return b->tape_tourn && b->tape_u && b->tape_inv_a && b->tape_inv_b && b->tape_cut_a && b->tape_cut_b && b->ties &&
+         (b->clean[0] == nullptr || b->off_clean != nullptr);
+}
+
+extern "C" int tspb_batch_init(const tspb_batch* b, int32_t parity, int32_t set_best, void* stream) {
+  if (!batch_ok(b) || (parity != 0 && parity != 1)) return TSPB_ERR_ARG;
+  if (b->num_instances == 0) return TSPB_OK;
+  batch_init_kernel<<<b->num_instances, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(*b, parity, set_best);
+  return tspb_launch_status();
+}
+
+extern "C" int tspb_batch_offspring(const tspb_batch* b, const int32_t* items, int32_t num_items, int32_t max_n,
+                                    int32_t threads, void* stream) {
+  if (!batch_ok(b) || !tape_ok(b) || num_items < 0 || max_n < 1) return TSPB_ERR_ARG;
+  if (threads < 32 || threads > 256 || threads % 32 != 0) return TSPB_ERR_ARG;
+  if (num_items == 0 || b->G == 0) return TSPB_OK;
+  if (!items) return TSPB_ERR_ARG;
+  if ((long long)num_items * b->P > 0x7fffffffLL) return TSPB_ERR_UNSUPPORTED;
+  const size_t smem = offspring_smem_bytes(max_n);
+  if (smem > 200 * 1024) return TSPB_ERR_UNSUPPORTED;
+  if (smem > 48 * 1024)
+    TSPB_CUDA_CHECK(cudaFuncSetAttribute(batch_offspring_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  batch_offspring_kernel<<<num_items * b->P, threads, smem, reinterpret_cast<cudaStream_t>(stream)>>>(*b, items, max_n);
+  return tspb_launch_status();
+}
+
+extern "C" int tspb_batch_survival(const tspb_batch* b, void* stream) {
+  if (!batch_ok(b) || !tape_ok(b)) return TSPB_ERR_ARG;
+  if (b->num_instances == 0 || b->G == 0) return TSPB_OK;
+  if ((long long)b->num_instances * b->P > 0x7fffffffLL || b->P > 3072) return TSPB_ERR_UNSUPPORTED;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  int rank_threads = ((2 * b->P + 31) / 32) * 32;
+  if (rank_threads > 512) rank_threads = 512;
+  batch_survival_rank_kernel<<<b->num_instances, rank_threads, (size_t)16 * b->P, st>>>(*b);
+  batch_survival_gather_kernel<<<b->num_instances * b->P, 128, 0, st>>>(*b);
+  batch_pause_kernel<<<(b->num_instances + 127) / 128, 128, 0, st>>>(*b);
+  return tspb_launch_status();
+}
+
+extern "C" int tspb_batch_two_opt_occupancy(int32_t max_n, int32_t mode, int32_t threads) {
+  if (max_n < 4 || (mode != TSPB_MODE_BEST && mode != TSPB_MODE_FIRST)) return 0;
+  const size_t smem = scan_tour_state_bytes(max_n, mode);
+  if (smem > (size_t)smem_optin() - 2048) return 0;
+  return mode == TSPB_MODE_BEST ? batch_two_opt_occ_mode<TSPB_MODE_BEST>(threads, smem)
+                                : batch_two_opt_occ_mode<TSPB_MODE_FIRST>(threads, smem);
+}
+
+extern "C" int tspb_batch_two_opt(const tspb_batch* b, const int32_t* items, int32_t num_items, int32_t max_n,
+                                  int32_t coords, int32_t phase, int32_t mode, int64_t max_iterations, int32_t threads,
+                                  int32_t ctas, uint32_t* queue, void* stream) {
+  if (!batch_ok(b) || num_items < 0 || max_n < 4 || !queue) return TSPB_ERR_ARG;
+  if (phase < TSPB_BATCH_PHASE_POSTINIT || phase > TSPB_BATCH_PHASE_RUN) return TSPB_ERR_ARG;
+  if (mode != TSPB_MODE_BEST && mode != TSPB_MODE_FIRST) return TSPB_ERR_ARG;
+  const int rows = phase == TSPB_BATCH_PHASE_POSTINIT ? b->P : b->elite;
+  if (num_items == 0 || rows == 0 || max_iterations <= 0) return TSPB_OK;
+  if (!items) return TSPB_ERR_ARG;
+  if (phase == TSPB_BATCH_PHASE_RESUME && !b->host_elites) return TSPB_ERR_ARG;
+  if ((long long)num_items * rows > 0x7fffffffLL || max_n > 65535) return TSPB_ERR_UNSUPPORTED;
+  const size_t smem = scan_tour_state_bytes(max_n, mode);
+  if (smem > (size_t)smem_optin() - 2048) return TSPB_ERR_UNSUPPORTED;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (mode == TSPB_MODE_BEST)
+    return batch_two_opt_mode<TSPB_MODE_BEST>(*b, items, num_items, rows, phase, max_iterations, max_n, threads, smem,
+                                              ctas, coords != 0, queue, st);
+  return batch_two_opt_mode<TSPB_MODE_FIRST>(*b, items, num_items, rows, phase, max_iterations, max_n, threads, smem,
+                                             ctas, coords != 0, queue, st);
+}
+
+extern "C" int tspb_batch_elite_cost(const tspb_batch* b, int32_t phase, void* stream) {
+  if (!batch_ok(b) || (phase != TSPB_BATCH_PHASE_RESUME && phase != TSPB_BATCH_PHASE_RUN)) return TSPB_ERR_ARG;
+  if (b->num_instances == 0 || b->elite == 0 || b->G == 0) return TSPB_OK;
+  if (phase == TSPB_BATCH_PHASE_RESUME && !b->host_elites) return TSPB_ERR_ARG;
+  const long long threads = (long long)b->num_instances * b->elite * 32;
+  if ((threads + 255) / 256 > 0x7fffffffLL) return TSPB_ERR_UNSUPPORTED;
+  batch_elite_cost_kernel<<<(int)((threads + 255) / 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(*b, phase);
+  return tspb_launch_status();
+}
+
+extern "C" int tspb_batch_track(const tspb_batch* b, int32_t phase, void* stream) {
+  if (!batch_ok(b) || (phase != TSPB_BATCH_PHASE_RESUME && phase != TSPB_BATCH_PHASE_RUN)) return TSPB_ERR_ARG;
+  if (b->num_instances == 0 || b->G == 0) return TSPB_OK;
+  batch_track_kernel<<<b->num_instances, 128, 0, reinterpret_cast<cudaStream_t>(stream)>>>(*b, phase);
+  return tspb_launch_status();
+}

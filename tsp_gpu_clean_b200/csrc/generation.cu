@@ -16,7 +16,7 @@
 //   evaluate_tour_cpu                       (tour_cost.py:17-29)
 //   _select_survivors_assessed              (genetic_algorithm.py:618-706)
 //   best tracking / patience                (genetic_algorithm.py:876-910)
-#include "common.cuh"
+#include "generation.cuh"
 
 namespace tspb {
 
@@ -29,109 +29,24 @@ struct GenTape {
   const int32_t* inv_b;   // [G][P]
 };
 
-__device__ __forceinline__ int tournament_winner(const double* fit, const int32_t* c, int kt, int pop) {
-  int best = c[0];
-  if ((unsigned)best >= (unsigned)pop) best = 0;
-  double bf = fit[best];
-  for (int q = 1; q < kt; ++q) {
-    const int v = c[q];
-    if ((unsigned)v >= (unsigned)pop) continue;
-    const double f = fit[v];
-    if (f < bf) {
-      bf = f;
-      best = v;
-    }
-  }
-  return best;
-}
-
-// CTA per child row. Shared memory: inv_p2[n], child[n], in_seg bits.
+// CTA per child row of generation *gen.
 __global__ void __launch_bounds__(256) offspring_kernel(const int32_t* __restrict__ pop, const double* __restrict__ fit,
                                                         int P, int n, int kt, GenTape tape, const int* __restrict__ gen,
                                                         const int* __restrict__ stopped, double rate, DistSrc ds,
                                                         int32_t* __restrict__ off, double* __restrict__ off_fit) {
   if (*stopped) return;
   extern __shared__ int sm[];
-  int* inv_p2 = sm;
-  int* child = sm + n;
-  unsigned* in_seg = reinterpret_cast<unsigned*>(sm + 2 * n);
-  __shared__ int w[2];
-  __shared__ long long red[32];
-  const int g = *gen;
-  const int row = blockIdx.x, tid = threadIdx.x, T = blockDim.x;
+  const long long g = *gen;
   const int pairs = P >> 1;
-  const int q = row >> 1, h = row & 1;
-  const bool paired = row < 2 * pairs;
-  if (tid < 2) {
-    const int sel = paired ? 2 * q + (tid == 0 ? h : 1 - h) : row;
-    w[tid] = tournament_winner(fit, tape.tourn + ((long long)g * P + sel) * kt, kt, P);
-  }
-  __syncthreads();
-  const int32_t* p1 = pop + (long long)w[0] * n;
-  const int32_t* p2 = pop + (long long)w[1] * n;
-  if (!paired || n < 2) {
-    for (int p = tid; p < n; p += T) child[p] = __ldg(p1 + p);
-  } else {
-    int c1 = tape.cut_a[(long long)g * pairs + q], c2 = tape.cut_b[(long long)g * pairs + q];
-    if (c1 > c2) {
-      const int tmp = c1;
-      c1 = c2;
-      c2 = tmp;
-    }
-    const int words = (n + 31) >> 5;
-    for (int p = tid; p < n; p += T) child[p] = -1;
-    for (int wd = tid; wd < words; wd += T) in_seg[wd] = 0u;
-    __syncthreads();
-    for (int p = tid; p < n; p += T) {
-      inv_p2[__ldg(p2 + p)] = p;
-      if (p >= c1 && p <= c2) {
-        const int v1 = __ldg(p1 + p);
-        child[p] = v1;
-        atomicOr(&in_seg[v1 >> 5], 1u << (v1 & 31));
-      }
-    }
-    __syncthreads();
-    const int seg_len = c2 - c1 + 1;
-    for (int idx = c1 + tid; idx <= c2; idx += T) {
-      const int val = __ldg(p2 + idx);
-      if (in_seg[val >> 5] & (1u << (val & 31))) continue;
-      int pos = idx, steps = 0;
-      while (pos >= c1 && pos <= c2 && steps <= seg_len) {
-        pos = inv_p2[__ldg(p1 + pos)];
-        ++steps;
-      }
-      if (pos < c1 || pos > c2) child[pos] = val;
-    }
-    __syncthreads();
-    for (int p = tid; p < n; p += T)
-      if (child[p] == -1) child[p] = __ldg(p2 + p);
-  }
-  __syncthreads();
-  // inversion mutation of this child
-  const long long gi = (long long)g * P + row;
-  if (tape.u[gi] < rate) {
-    const int a = tape.inv_a[gi], b = tape.inv_b[gi];
-    const int lo = a < b ? a : b, hi = a < b ? b : a;
-    if (lo >= 0 && hi < n) {
-      const int half = (hi - lo + 1) >> 1;
-      for (int t = tid; t < half; t += T) {
-        const int x = child[lo + t], y = child[hi - t];
-        child[lo + t] = y;
-        child[hi - t] = x;
-      }
-    }
-  }
-  __syncthreads();
-  // write out and reduce the closed-tour length (exact int64, one float64 at the end)
-  int32_t* dst = off + (long long)row * n;
-  long long acc = 0;
-  for (int p = tid; p < n; p += T) {
-    const int v = child[p];
-    dst[p] = v;
-    acc += ds(v, child[p + 1 == n ? 0 : p + 1]);
-  }
-  acc = block_sum(acc, red);
-  if (tid == 0) off_fit[row] = n <= 1 ? 0.0 : (double)acc;
+  GenTapeSlice sl;
+  sl.tourn = tape.tourn + g * P * kt;
+  sl.cut_a = tape.cut_a ? tape.cut_a + g * pairs : nullptr;
+  sl.cut_b = tape.cut_b ? tape.cut_b + g * pairs : nullptr;
+  sl.u = tape.u + g * P;
+  sl.inv_a = tape.inv_a + g * P;
+  sl.inv_b = tape.inv_b + g * P;
+  const int row = blockIdx.x;
+  offspring_row(pop, fit, P, n, kt, sl, rate, ds, row, sm, off + (long long)row * n, off_fit + row);
 }
 
 // Stable rank of the 2P combined fitness (old population first), keep P.
@@ -262,13 +177,9 @@ __global__ void elite_cost_kernel(const int32_t* __restrict__ pop, int k, int n,
                                   const int* __restrict__ stopped, double* __restrict__ fit) {
   if (*stopped) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
   if (warp >= k) return;
-  const int32_t* t = pop + (long long)warp * n;
-  long long acc = 0;
-  for (int p = lane; p < n; p += 32) acc += ds(t[p], t[p + 1 == n ? 0 : p + 1]);
-  acc = warp_sum(acc);
-  if (lane == 0) fit[warp] = n <= 1 ? 0.0 : (double)acc;
+  const double f = warp_tour_length(pop + (long long)warp * n, n, ds);
+  if ((threadIdx.x & 31) == 0) fit[warp] = f;
 }
 
 }  // namespace tspb
@@ -294,7 +205,7 @@ extern "C" int tspb_generation_offspring(const int32_t* pop, const double* fit, 
     return TSPB_ERR_ARG;
   if (P >= 2 && (!tape_cut_a || !tape_cut_b)) return TSPB_ERR_ARG;
   if (!dist && !coords) return TSPB_ERR_ARG;
-  const size_t smem = (size_t)8 * n + (size_t)((n + 31) / 32) * 4;
+  const size_t smem = offspring_smem_bytes(n);
   if (smem > 200 * 1024) return TSPB_ERR_UNSUPPORTED;
   if (smem > 48 * 1024)
     TSPB_CUDA_CHECK(cudaFuncSetAttribute(offspring_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -169,6 +169,18 @@ class DeviceOperands:
     return self._coords
 
   def dist(self):
+    if self._dist is None and self._euc2d_on_device():
+      # The matrix of an EUC_2D coordinate problem is built in HBM from the coordinates with
+      # the reference's rounding (compute_distance_matrix, matrix.py:214-273): only the
+      # coordinates cross PCIe.
+      n = int(self.context.dimension)
+      check_free(n * n * 4, f"dense distance matrix (n={n})")
+      d = torch.empty((n, n), dtype=torch.int32, device="cuda")
+      if n:
+        from .native import call
+
+        call("tspb_euc2d_matrix", ptr(self.coords()), n, ptr(d), n, stream_handle())
+      self._dist = d
     if self._dist is None:
       D = self.context.get_cpu_distances()
       D = np.ascontiguousarray(D, dtype=np.int32)
@@ -178,6 +190,12 @@ class DeviceOperands:
       self._dist = device_tensor(D, torch.int32)
       self.h2d_bytes += D.nbytes
     return self._dist
+
+  def _euc2d_on_device(self) -> bool:
+    prob = self.context.problem
+    if getattr(prob, "distances", None) is not None or getattr(prob, "coordinates", None) is None:
+      return False
+    return getattr(prob, "edge_type", "EUC_2D") == "EUC_2D"
 
   def use_coords(self, n: int, max_matrix_dimension: int | None) -> bool:
     threshold = max_matrix_dimension

@@ -50,6 +50,33 @@ from .routes import sample_distinct_pairs
 from .strategies.initialization import InitializationB200TourNearestNeighbor
 
 
+def draw_generation_tape(rng: np.random.Generator, G: int, P: int, kt: int, n: int):
+  """Random draws of G generations from `rng` in the reference's order.
+
+  Per generation: tournament contestants (P, kt) (`tournament_selection.py:113`), PMX cut
+  pairs for P/2 pairs (`pmx_crossover.py:155`), inversion u (P) (`inversion_mutation.py:82`)
+  and inversion position pairs (P) (`route_helpers.py:214`). Returns the six tape arrays
+  (tourn, cut_a, cut_b, u, inv_a, inv_b), each with a leading G axis, and the generator
+  state after each generation (to rewind the generator after an early stop).
+  """
+  tourn = np.empty((G, P, kt), dtype=np.int32)
+  cut_a = np.empty((G, P // 2), dtype=np.int32)
+  cut_b = np.empty((G, P // 2), dtype=np.int32)
+  u = np.empty((G, P), dtype=np.float64)
+  inv_a = np.empty((G, P), dtype=np.int32)
+  inv_b = np.empty((G, P), dtype=np.int32)
+  states = []
+  for g in range(G):
+    tourn[g] = rng.integers(0, P, size=(P, kt), dtype=np.int32)
+    pairs = sample_distinct_pairs(rng, P // 2, 0, n)
+    cut_a[g], cut_b[g] = pairs[:, 0], pairs[:, 1]
+    u[g] = rng.random(P)
+    pos = sample_distinct_pairs(rng, P, 0, n)
+    inv_a[g], inv_b[g] = pos[:, 0], pos[:, 1]
+    states.append(rng.bit_generator.state)
+  return (tourn, cut_a, cut_b, u, inv_a, inv_b), states
+
+
 @dataclass
 class LocalSearchConfig:
   mode: str = "best"
@@ -80,23 +107,7 @@ class FusedMemeticSolver:
 
   # -------------------------------------------------------------------------- tape
   def _draw_tape(self, rng: np.random.Generator, G: int, n: int):
-    P = self.P
-    tourn = np.empty((G, P, self.kt), dtype=np.int32)
-    cut_a = np.empty((G, P // 2), dtype=np.int32)
-    cut_b = np.empty((G, P // 2), dtype=np.int32)
-    u = np.empty((G, P), dtype=np.float64)
-    inv_a = np.empty((G, P), dtype=np.int32)
-    inv_b = np.empty((G, P), dtype=np.int32)
-    states = []
-    for g in range(G):
-      tourn[g] = rng.integers(0, P, size=(P, self.kt), dtype=np.int32)   # tournament_selection.py:113
-      pairs = sample_distinct_pairs(rng, P // 2, 0, n)                    # pmx_crossover.py:155
-      cut_a[g], cut_b[g] = pairs[:, 0], pairs[:, 1]
-      u[g] = rng.random(P)                                                # inversion_mutation.py:82
-      pos = sample_distinct_pairs(rng, P, 0, n)                           # route_helpers.py:214
-      inv_a[g], inv_b[g] = pos[:, 0], pos[:, 1]
-      states.append(rng.bit_generator.state)
-    return (tourn, cut_a, cut_b, u, inv_a, inv_b), states
+    return draw_generation_tape(rng, G, self.P, self.kt, n)
 
   # -------------------------------------------------------------------------- launches
   def _two_opt(self, rows_ptr, num, skip=None):

@@ -68,7 +68,41 @@ SIGNATURES: dict[str, tuple] = {
                                    ctypes.c_float, _p]),
   "tspb_select_topk": (ctypes.c_int, [_p, _p, _i32, _i32, _i32, _p, _p]),
   "tspb_nn_init": (ctypes.c_int, [_p, _i32, _p, _i32, _i32, _p, _i32, _i32, _p, _sz, _p, _p]),
+  "tspb_batch_init": (ctypes.c_int, [_p, _i32, _i32, _p]),
+  "tspb_batch_offspring": (ctypes.c_int, [_p, _p, _i32, _i32, _i32, _p]),
+  "tspb_batch_survival": (ctypes.c_int, [_p, _p]),
+  "tspb_batch_two_opt": (ctypes.c_int, [_p, _p, _i32, _i32, _i32, _i32, _i32, _i64, _i32, _i32, _p, _p]),
+  "tspb_batch_two_opt_occupancy": (ctypes.c_int, [_i32, _i32, _i32]),
+  "tspb_batch_elite_cost": (ctypes.c_int, [_p, _i32, _p]),
+  "tspb_batch_track": (ctypes.c_int, [_p, _i32, _p]),
 }
+
+TSPB_BATCH_RUN = 0
+TSPB_BATCH_STOPPED = 1
+TSPB_BATCH_PAUSED = 2
+TSPB_BATCH_RESUME = 3
+TSPB_BATCH_DONE = 4
+TSPB_BATCH_PHASE_POSTINIT = 0
+TSPB_BATCH_PHASE_RESUME = 1
+TSPB_BATCH_PHASE_RUN = 2
+
+
+class BatchInstance(ctypes.Structure):
+  """`tspb_batch_instance` of include/tspb.h."""
+
+  _fields_ = [("n", _i32), ("k", _i32), ("pop_offset", _i64), ("node_offset", _i64), ("dist", _p),
+              ("dist_stride", _i64), ("coords", _p), ("cand_packed", _p), ("patience", _i64)]
+
+
+class BatchState(ctypes.Structure):
+  """`tspb_batch` of include/tspb.h (device pointers of one batch of GA runs)."""
+
+  _fields_ = [("num_instances", _i32), ("P", _i32), ("kt", _i32), ("elite", _i32), ("G", _i32), ("rows_max", _i32),
+              ("mutation_rate", _f64), ("inst", _p), ("pop", _p * 2), ("fit", _p * 2), ("off", _p), ("off_fit", _p),
+              ("order", _p), ("tape_tourn", _p), ("tape_cut_a", _p), ("tape_cut_b", _p), ("tape_u", _p),
+              ("tape_inv_a", _p), ("tape_inv_b", _p), ("ctl", _p), ("best_cost", _p), ("best_tour", _p),
+              ("history", _p), ("ties", _p), ("host_elites", _p), ("ls_status", _p), ("ls_stats", _p),
+              ("clean", _p * 2), ("off_clean", _p)]
 
 _lock = threading.Lock()
 _lib = None
