@@ -373,7 +373,8 @@ def run_ga_bench(args) -> dict:
   return {"value": value, "ms_per_step": sum(loop_ms) / args.steps, "clocks": clocks.summary(),
           "e2e": {"value": gens / sum(walls), "unit": "generations/s", "h2d_bytes_per_step": int(coords.nbytes),
                   "d2h_bytes_per_step": int(n * 4 + (G + 1) * 8 + P * n * 4)},
-          "gpu_launches": launches, "desc": desc, "best": stats["best_fitness"]}
+          "gpu_launches": launches, "desc": desc, "best": stats["best_fitness"],
+          "timing": {k: round(v, 4) for k, v in solver.last_timing.items() if isinstance(v, (int, float))}}
 
 
 # ------------------------------------------------------------------------ uneven batch
@@ -743,7 +744,8 @@ def main_ga(args) -> int:
   line = {"metric": "generations/s", "value": res["value"], "unit": "generations/s", "n_gpus": 1, "steps": args.steps,
           "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
           "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)", "config": config, "clocks": res["clocks"],
-          "e2e": res["e2e"], "gpu_launches": res["gpu_launches"], "detail": {"best_fitness": res["best"]}}
+          "e2e": res["e2e"], "gpu_launches": res["gpu_launches"],
+          "detail": {"best_fitness": res["best"], "engine": args.engine, "last_run": res["timing"]}}
   if not args.no_cpu_baseline:
     cpu = _ga_cpu_gens_per_s(args.workload, sample)
     line["cpu_baseline"] = {"value": cpu["value"], "unit": "generations/s", "cores": 1, "kind": "port",

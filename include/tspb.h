@@ -334,15 +334,17 @@ int tspb_batch_offspring(const tspb_batch* b, const int32_t* items, int32_t num_
 /* Survival of every RUN instance and the elite-edge tie rule (RUN -> PAUSED); replaces
  * _select_survivors_assessed (genetic_algorithm.py:618-706) for every run. */
 int tspb_batch_survival(const tspb_batch* b, void* stream);
+#define TSPB_BATCH_COORDS 1  /* every item has dist == NULL: distances rebuilt from coordinates */
+#define TSPB_BATCH_GROUPED 2 /* every item's k is a multiple of 4 and its packed table 16-byte aligned */
 /* 2-opt over the (item, row) units of one phase: persistent CTAs (ctas <= 0: every CTA
  * that fits) take units from the device counter `queue` (zeroed by this call) in item
- * order; put the largest instances first. `coords` != 0: every item has dist == NULL
- * (distances rebuilt from coordinates), else every item has a matrix; an item that
- * disagrees gets TSPB_ERR_UNSUPPORTED in ls_status. mode BEST or FIRST, candidate mode
- * only, threads 64/128/256/512/1024. Replaces the post-init and elite refinement calls of
- * LocalSearchCPUTourTwoOpt (pipeline_steps.py:103-125, 153-195) for every run. */
+ * order; put the largest instances first. `flags` (TSPB_BATCH_*) state what holds for
+ * every item; an item that disagrees gets TSPB_ERR_UNSUPPORTED in ls_status and is left
+ * unchanged. mode BEST or FIRST, candidate mode only, threads 64/128/256/512/1024.
+ * Replaces the post-init and elite refinement calls of LocalSearchCPUTourTwoOpt
+ * (pipeline_steps.py:103-125, 153-195) for every run. */
 int tspb_batch_two_opt(const tspb_batch* b, const int32_t* items, int32_t num_items, int32_t max_n,
-                       int32_t coords, int32_t phase, int32_t mode, int64_t max_iterations, int32_t threads,
+                       int32_t flags, int32_t phase, int32_t mode, int64_t max_iterations, int32_t threads,
                        int32_t ctas, uint32_t* queue, void* stream);
 /* Resident CTAs per SM of tspb_batch_two_opt for this shape (0: does not fit). */
 int tspb_batch_two_opt_occupancy(int32_t max_n, int32_t mode, int32_t threads);

@@ -200,3 +200,48 @@ def test_device_resident_roundtrip(b200):
   assert dev.is_cuda
   assert np.array_equal(dev.cpu().numpy(), host)
   assert np.array_equal(dev_in.cpu().numpy(), tours)
+
+
+_LAYOUT_ORACLE: dict = {}
+
+
+@pytest.mark.parametrize("mode", ["best", "first"])
+@pytest.mark.parametrize("k", [20, 12, 10, 7])
+@pytest.mark.parametrize("threads", [128, 512])
+def test_table_layouts_agree(b200, mode, k, threads):
+  """Plain candidates, packed words, and packed words read in row groups (k % 4 == 0) give
+  the same tours and the same pass/pair/move/gain counts, equal to the oracle's."""
+  import torch
+
+  from tsp_gpu_clean_b200 import native
+  from tsp_gpu_clean_b200.device import operands_for, ptr, stream_handle
+
+  n, T = 250, 16
+  coords = instances.clustered_instance(n, 12, 30.0, 31)
+  tours = instances.random_tours(n, T, 32)
+  ctx = _ctx(b200, coords=coords)
+  ops = operands_for(ctx)
+  dist, stride, _ = ops.distance_args(n, None)
+  tabs = ops.candidates(k, ctx.get_cpu_candidate_list(k), n, None)
+  assert tabs.packed is not None
+  lib = native.load_library()
+  outs = []
+  for packed in (None, tabs.packed):
+    work = torch.from_numpy(tours).cuda()
+    stats = torch.zeros((T, 4), dtype=torch.int64, device="cuda")
+    status = torch.zeros(T, dtype=torch.int32, device="cuda")
+    rc = lib.tspb_two_opt(ptr(work), T, n, ptr(dist), stride, None, ptr(tabs.cand), ptr(tabs.cand_dist), None, None,
+                          ptr(packed), tabs.k, native.MODE_CODES[mode], 10**9, threads, ptr(stats), ptr(status), None,
+                          0, stream_handle())
+    native.check("tspb_two_opt", rc)
+    assert int(status.max().item()) == 0
+    outs.append((work.cpu().numpy(), stats.cpu().numpy()))
+  assert np.array_equal(outs[0][0], outs[1][0])
+  assert np.array_equal(outs[0][1], outs[1][1])
+  key = (mode, k)
+  if key not in _LAYOUT_ORACLE:
+    _LAYOUT_ORACLE[key] = otwo.improve_batch(tours, odist.euc2d_matrix(coords), ctx.get_cpu_candidate_list(k), mode,
+                                             10**9)
+  want, st = _LAYOUT_ORACLE[key]
+  assert np.array_equal(outs[1][0], want)
+  assert np.array_equal(outs[1][1][:, :3], st)

@@ -68,6 +68,7 @@ class Bucket:
   coords: bool
   items: list[int] = field(default_factory=list)
   max_n: int = 0
+  grouped: bool = False  # every item's k % 4 == 0 and its packed table 16-byte aligned
   two_opt_threads: int = 128
   offspring_threads: int = 128
   d_items: Any = None
@@ -171,9 +172,13 @@ class FusedBatchSolver:
   def _mode(self) -> int:
     return native.MODE_CODES[self.ls.mode]
 
+  @staticmethod
+  def _flags(bucket: Bucket) -> int:
+    return (native.TSPB_BATCH_COORDS if bucket.coords else 0) | (native.TSPB_BATCH_GROUPED if bucket.grouped else 0)
+
   def _two_opt(self, st_ref, bucket: Bucket, phase: int, threads: int | None = None) -> None:
     rc = native.load_library().tspb_batch_two_opt(
-      st_ref, ptr(bucket.d_items), len(bucket.items), bucket.max_n, 1 if bucket.coords else 0, phase, self._mode,
+      st_ref, ptr(bucket.d_items), len(bucket.items), bucket.max_n, self._flags(bucket), phase, self._mode,
       int(self.ls.max_iterations), int(threads or bucket.two_opt_threads), 0, ptr(bucket.queue), stream_handle())
     native.check("tspb_batch_two_opt", rc)
     self.kernel_launches += 1
@@ -281,7 +286,7 @@ class FusedBatchSolver:
 
     def run():
       fill()
-      rc = lib.tspb_batch_two_opt(st_ref, ptr(b.d_items), len(b.items), b.max_n, 1 if b.coords else 0,
+      rc = lib.tspb_batch_two_opt(st_ref, ptr(b.d_items), len(b.items), b.max_n, self._flags(b),
                                   native.TSPB_BATCH_PHASE_POSTINIT, self._mode, int(self.ls.max_iterations), threads, 0,
                                   ptr(b.queue), stream_handle())
       native.check("tspb_batch_two_opt", rc)
@@ -383,6 +388,7 @@ class FusedBatchSolver:
 
     self.buckets = self._make_buckets(ns, coords_flags)
     for b in self.buckets:
+      b.grouped = all(h_inst[i].k % 4 == 0 and h_inst[i].cand_packed % 16 == 0 for i in b.items)
       b.d_items = torch.tensor(b.items, dtype=torch.int32, device=dev)
       b.queue = torch.zeros(1, dtype=torch.int32, device=dev)
 

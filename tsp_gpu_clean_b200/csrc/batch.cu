@@ -202,7 +202,9 @@ __global__ void batch_pause_kernel(const tspb_batch B) {
 
 // Persistent 2-opt over the (item, row) units of one phase. COORDS: the bucket's
 // instances rebuild distances from coordinates (no matrix); otherwise they all have one.
-template <int MODE, int THREADS, int U, bool COORDS>
+// LAYOUT: SCAN_GROUPED when every item's k is a multiple of U and its packed table is
+// U*4-byte aligned, else SCAN_PACKED.
+template <int MODE, int THREADS, int U, bool COORDS, int LAYOUT>
 __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value)
     batch_two_opt_kernel(const tspb_batch B, const int32_t* __restrict__ items, int num_items, int rows, int phase,
                          long long max_iter, int max_n, unsigned* __restrict__ queue) {
@@ -234,7 +236,9 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value)
     uint8_t* clean = B.clean[0] ? clean_buf(B, parity) + (long long)i * B.P + row : nullptr;
     if (clean && *clean) continue;  // a converged local optimum: refining it changes nothing
     const tspb_batch_instance I = B.inst[i];
-    if ((I.dist == nullptr) != COORDS || I.n > max_n || I.n < 4 || I.k < 1) {
+    const bool layout_ok = LAYOUT != SCAN_GROUPED ||
+                           (I.k % U == 0 && (reinterpret_cast<uintptr_t>(I.cand_packed) % (U * sizeof(uint32_t))) == 0);
+    if ((I.dist == nullptr) != COORDS || I.n > max_n || I.n < 4 || I.k < 1 || !layout_ok) {
       if (threadIdx.x == 0) B.ls_status[(long long)i * B.rows_max + e] = TSPB_ERR_UNSUPPORTED;
       continue;
     }
@@ -255,7 +259,7 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value)
     T.accumulate = 1;
     T.moved = nullptr;
     T.converged = clean;
-    scan_tour<MODE, THREADS, U, true>(T, S);
+    scan_tour<MODE, THREADS, U, LAYOUT>(T, S);
   }
 }
 
@@ -343,9 +347,13 @@ __global__ void __launch_bounds__(128) batch_track_kernel(const tspb_batch B, in
 
 template <int MODE, int THREADS, int U>
 static int batch_two_opt_launch(const tspb_batch& b, const int32_t* items, int num_items, int rows, int phase,
-                                long long max_iter, int max_n, size_t smem, int ctas, int coords, unsigned* queue,
+                                long long max_iter, int max_n, size_t smem, int ctas, int flags, unsigned* queue,
                                 cudaStream_t st) {
-  auto kern = coords ? batch_two_opt_kernel<MODE, THREADS, U, true> : batch_two_opt_kernel<MODE, THREADS, U, false>;
+  const bool coords = flags & TSPB_BATCH_COORDS, grouped = flags & TSPB_BATCH_GROUPED;
+  auto kern = coords ? (grouped ? batch_two_opt_kernel<MODE, THREADS, U, true, SCAN_GROUPED>
+                                : batch_two_opt_kernel<MODE, THREADS, U, true, SCAN_PACKED>)
+                     : (grouped ? batch_two_opt_kernel<MODE, THREADS, U, false, SCAN_GROUPED>
+                                : batch_two_opt_kernel<MODE, THREADS, U, false, SCAN_PACKED>);
   TSPB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   TSPB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem));
@@ -367,7 +375,7 @@ static int batch_two_opt_launch(const tspb_batch& b, const int32_t* items, int n
 
 template <int MODE, int THREADS, int U>
 static int batch_two_opt_occ(size_t smem) {
-  auto kern = batch_two_opt_kernel<MODE, THREADS, U, false>;
+  auto kern = batch_two_opt_kernel<MODE, THREADS, U, false, SCAN_GROUPED>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem) != cudaSuccess) return 0;
@@ -376,23 +384,23 @@ static int batch_two_opt_occ(size_t smem) {
 
 template <int MODE>
 static int batch_two_opt_mode(const tspb_batch& b, const int32_t* items, int num_items, int rows, int phase,
-                              long long max_iter, int max_n, int threads, size_t smem, int ctas, int coords,
+                              long long max_iter, int max_n, int threads, size_t smem, int ctas, int flags,
                               unsigned* queue, cudaStream_t st) {
   switch (threads) {
     case 64:
-      return batch_two_opt_launch<MODE, 64, 4>(b, items, num_items, rows, phase, max_iter, max_n, smem, ctas, coords,
+      return batch_two_opt_launch<MODE, 64, 4>(b, items, num_items, rows, phase, max_iter, max_n, smem, ctas, flags,
                                                queue, st);
     case 128:
-      return batch_two_opt_launch<MODE, 128, 4>(b, items, num_items, rows, phase, max_iter, max_n, smem, ctas, coords,
+      return batch_two_opt_launch<MODE, 128, 4>(b, items, num_items, rows, phase, max_iter, max_n, smem, ctas, flags,
                                                 queue, st);
     case 256:
-      return batch_two_opt_launch<MODE, 256, 4>(b, items, num_items, rows, phase, max_iter, max_n, smem, ctas, coords,
+      return batch_two_opt_launch<MODE, 256, 4>(b, items, num_items, rows, phase, max_iter, max_n, smem, ctas, flags,
                                                 queue, st);
     case 512:
-      return batch_two_opt_launch<MODE, 512, 2>(b, items, num_items, rows, phase, max_iter, max_n, smem, ctas, coords,
+      return batch_two_opt_launch<MODE, 512, 2>(b, items, num_items, rows, phase, max_iter, max_n, smem, ctas, flags,
                                                 queue, st);
     case 1024:
-      return batch_two_opt_launch<MODE, 1024, 2>(b, items, num_items, rows, phase, max_iter, max_n, smem, ctas, coords,
+      return batch_two_opt_launch<MODE, 1024, 2>(b, items, num_items, rows, phase, max_iter, max_n, smem, ctas, flags,
                                                  queue, st);
     default: return TSPB_ERR_ARG;
   }
@@ -473,9 +481,10 @@ extern "C" int tspb_batch_two_opt_occupancy(int32_t max_n, int32_t mode, int32_t
 }
 
 extern "C" int tspb_batch_two_opt(const tspb_batch* b, const int32_t* items, int32_t num_items, int32_t max_n,
-                                  int32_t coords, int32_t phase, int32_t mode, int64_t max_iterations, int32_t threads,
+                                  int32_t flags, int32_t phase, int32_t mode, int64_t max_iterations, int32_t threads,
                                   int32_t ctas, uint32_t* queue, void* stream) {
   if (!batch_ok(b) || num_items < 0 || max_n < 4 || !queue) return TSPB_ERR_ARG;
+  if (flags & ~(TSPB_BATCH_COORDS | TSPB_BATCH_GROUPED)) return TSPB_ERR_ARG;
   if (phase < TSPB_BATCH_PHASE_POSTINIT || phase > TSPB_BATCH_PHASE_RUN) return TSPB_ERR_ARG;
   if (mode != TSPB_MODE_BEST && mode != TSPB_MODE_FIRST) return TSPB_ERR_ARG;
   const int rows = phase == TSPB_BATCH_PHASE_POSTINIT ? b->P : b->elite;
@@ -488,9 +497,9 @@ extern "C" int tspb_batch_two_opt(const tspb_batch* b, const int32_t* items, int
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   if (mode == TSPB_MODE_BEST)
     return batch_two_opt_mode<TSPB_MODE_BEST>(*b, items, num_items, rows, phase, max_iterations, max_n, threads, smem,
-                                              ctas, coords != 0, queue, st);
+                                              ctas, flags, queue, st);
   return batch_two_opt_mode<TSPB_MODE_FIRST>(*b, items, num_items, rows, phase, max_iterations, max_n, threads, smem,
-                                             ctas, coords != 0, queue, st);
+                                             ctas, flags, queue, st);
 }
 
 extern "C" int tspb_batch_elite_cost(const tspb_batch* b, int32_t phase, void* stream) {

@@ -4,13 +4,15 @@
 // (src/algorithms/strategies/local_search/two_opt.py:347-367, 386-489, 565-595); this file
 // holds the one-CTA-per-tour launch, its shared-memory carveout policy and the k-NN
 // packing kernel.
+#include <type_traits>
+
 #include "two_opt_scan.cuh"
 
 namespace tspb {
 
 // SMEM: the tour state lives in shared memory (the compiler then addresses it with
 // shared-memory instructions); otherwise in the per-tour global workspace slice.
-template <int MODE, int THREADS, int U, bool PACKED, bool SMEM>
+template <int MODE, int THREADS, int U, int LAYOUT, bool SMEM>
 __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value) two_opt_scan_kernel(const TwoOptArgs A) {
   extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ ScanSmem S;
@@ -32,7 +34,7 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value) two_op
   T.accumulate = 0;
   T.moved = nullptr;
   T.converged = nullptr;
-  scan_tour<MODE, THREADS, U, PACKED>(T, S);
+  scan_tour<MODE, THREADS, U, LAYOUT>(T, S);
 }
 
 size_t two_opt_scan_tour_bytes(int n, int mode) { return scan_tour_state_bytes(n, mode); }
@@ -68,10 +70,16 @@ static int carveout_percent(int num_tours, size_t smem_per_cta, int max_ctas_per
 
 template <int MODE, int THREADS, int U>
 static int launch_scan(const TwoOptArgs& a, size_t smem, cudaStream_t st) {
-  auto kern = a.arrays_in_smem ? (a.cand_packed ? two_opt_scan_kernel<MODE, THREADS, U, true, true>
-                                                : two_opt_scan_kernel<MODE, THREADS, U, false, true>)
-                               : (a.cand_packed ? two_opt_scan_kernel<MODE, THREADS, U, true, false>
-                                                : two_opt_scan_kernel<MODE, THREADS, U, false, false>);
+  // the grouped layout loads U packed words at once: k % U == 0 and a U*4-byte aligned table
+  const bool aligned = (reinterpret_cast<uintptr_t>(a.cand_packed) % (U * sizeof(uint32_t))) == 0;
+  const int layout = a.cand_packed ? (a.k % U == 0 && aligned ? SCAN_GROUPED : SCAN_PACKED) : SCAN_PLAIN;
+  auto pick = [&](auto smem_tag) {
+    constexpr bool SM = decltype(smem_tag)::value;
+    return layout == SCAN_GROUPED  ? two_opt_scan_kernel<MODE, THREADS, U, SCAN_GROUPED, SM>
+           : layout == SCAN_PACKED ? two_opt_scan_kernel<MODE, THREADS, U, SCAN_PACKED, SM>
+                                   : two_opt_scan_kernel<MODE, THREADS, U, SCAN_PLAIN, SM>;
+  };
+  auto kern = a.arrays_in_smem ? pick(std::true_type{}) : pick(std::false_type{});
   if (smem > 48 * 1024) TSPB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int pct = carveout_percent(a.num_tours, smem, ScanMinBlocks<THREADS>::value);
   if (pct > 0) TSPB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct));

@@ -60,9 +60,35 @@ struct ScanTour {
                        // move (the tour is then a fixed point of any further refinement)
 };
 
+// k-NN table layouts of scan_tour: plain int32 candidates (+ optional distances), packed
+// words with round-robin entries, and packed words with each thread's U entries taken
+// contiguously from one row (needs k % U == 0): the row's a, succ[a], eout[a] are read
+// once per U entries and the U words arrive in one vector load.
+enum ScanLayout { SCAN_PLAIN = 0, SCAN_PACKED = 1, SCAN_GROUPED = 2 };
+
+template <int U>
+__device__ __forceinline__ void load_words(const uint32_t* p, uint32_t (&w)[U]) {
+  if constexpr (U == 4) {
+    const uint4 v = __ldg(reinterpret_cast<const uint4*>(p));
+    w[0] = v.x;
+    w[1] = v.y;
+    w[2] = v.z;
+    w[3] = v.w;
+  } else if constexpr (U == 2) {
+    const uint2 v = __ldg(reinterpret_cast<const uint2*>(p));
+    w[0] = v.x;
+    w[1] = v.y;
+  } else {
+#pragma unroll
+    for (int u = 0; u < U; ++u) w[u] = __ldg(p + u);
+  }
+}
+
 // Refines one tour with the whole CTA. Every thread of the CTA must call it.
-template <int MODE, int THREADS, int U, bool PACKED>
+template <int MODE, int THREADS, int U, int LAYOUT>
 __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
+  constexpr bool PACKED = LAYOUT != SCAN_PLAIN;
+  constexpr bool GROUPED = LAYOUT == SCAN_GROUPED;
   const int n = T.n, k = T.k, rows = n - 2;
   const int tid = threadIdx.x;
   int32_t* g_tour = T.g_tour;
@@ -144,6 +170,7 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
   const int E = rows * k;
   constexpr int STEP = THREADS * U;
   const int sq = STEP / k, sr = STEP - (STEP / k) * k;
+  const int g_row0 = (tid * U) / k, g_col0 = tid * U - g_row0 * k;  // grouped layout: first entry
   long long passes = 0, moves = 0, my_pairs = 0, my_eval = 0;
   int err = TSPB_OK;
   bool converged = false;  // the last pass found no improving move: a local optimum
@@ -164,6 +191,58 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
     int bgain = 0;            // best: smallest gain of this thread (strictly below 0 to count)
     unsigned bidx = NO_IDX;   // and its scan index (first in thread order wins ties)
     int cnt = 0, evals = 0;
+    if constexpr (GROUPED) {
+      // entries [e0 + tid*U, e0 + tid*U + U) of round e0 lie in row gi, columns gr..gr+U-1
+      int gi = g_row0, gr = g_col0;
+      for (int e0 = 0; e0 < E; e0 += STEP) {
+        const int eb = e0 + tid * U;
+        if (eb < E) {
+          const int a = tour[gi];
+          uint32_t w[U];
+          load_words<U>(packed + ((unsigned)a * (unsigned)k + (unsigned)gr), w);
+          const int sa = succ[a], ea = eout[a];
+          const int lo = gi + 2;
+          const unsigned span = (unsigned)(n - (gi == 0) - lo);
+          bool ok[U];
+          int c[U], sc[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            c[u] = (int)(w[u] & 0xffffu);
+            ok[u] = (unsigned)c[u] < (unsigned)n && (unsigned)(pos[c[u]] - lo) < span;
+            if (MODE == TSPB_MODE_BEST) cnt += ok[u];
+            if (ok[u]) sc[u] = succ[c[u]];
+          }
+          int dbd[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u)
+            if (ok[u]) dbd[u] = dist ? __ldcg(dist + ((unsigned)sa * stride + (unsigned)sc[u])) : ds(sa, sc[u]);
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            if (!ok[u]) continue;
+            ++evals;
+            const int gain = ((int)(w[u] >> 16) - ea) + (dbd[u] - eout[c[u]]);
+            if (MODE == TSPB_MODE_BEST) {
+              if (gain < bgain) {
+                bgain = gain;
+                bidx = (unsigned)(eb + u);
+              }
+            } else if (gain < 0) {
+              atomicMin(&S.first, (unsigned)(eb + u));
+            }
+          }
+        }
+        gr += sr;
+        gi += sq;
+        if (gr >= k) {
+          gr -= k;
+          ++gi;
+        }
+        if (MODE == TSPB_MODE_FIRST) {
+          __syncthreads();
+          if (S.first != NO_IDX) break;
+        }
+      }
+    } else {
     int ri[U], rr[U], ee[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
@@ -237,6 +316,7 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
         __syncthreads();
         if (S.first != NO_IDX) break;
       }
+    }
     }
     my_pairs += cnt;
     my_eval += evals;

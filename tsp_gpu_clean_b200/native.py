@@ -85,6 +85,8 @@ TSPB_BATCH_DONE = 4
 TSPB_BATCH_PHASE_POSTINIT = 0
 TSPB_BATCH_PHASE_RESUME = 1
 TSPB_BATCH_PHASE_RUN = 2
+TSPB_BATCH_COORDS = 1
+TSPB_BATCH_GROUPED = 2
 
 
 class BatchInstance(ctypes.Structure):
