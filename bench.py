@@ -47,6 +47,10 @@ K_CAND = 20
 #: position and successor reads = 12 B.
 BYTES_PER_DELTA = 24
 L2_FLUSH_BYTES = 256 << 20
+#: DRAM bytes (read + write) of one launch of the default workload's scan kernels, from one
+#: ncu capture of this command (profiles/two_opt_scan_c2.md); only the default 1024-tour,
+#: 128-thread scan configuration has a captured figure.
+NCU_DRAM_BYTES_PER_LAUNCH = {"best": 8_746_240, "first": 9_101_056}
 
 
 def _peaks() -> dict:
@@ -276,7 +280,9 @@ def run_gpu(args, pool) -> dict | None:
             "d2h_bytes_per_step": int(tours_np.nbytes * len(modes) + args.tours * 32 * len(modes))},
     "gpu_launches": launches,
     "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                 "frac": achieved_gbs / peaks["hbm_gbs"], "traffic": None,
+                 "frac": achieved_gbs / peaks["hbm_gbs"],
+                 "traffic": (NCU_DRAM_BYTES_PER_LAUNCH[dominant]
+                             if (args.tours, args.threads, args.kernel) == (instances.C2_TOURS, 128, "scan") else None),
                  "kernel": f"two_opt_{args.kernel}_kernel<{dominant}>",
                  "peak_source": peaks["source"],
                  "basis": f"{BYTES_PER_DELTA} B per gain the kernel computed"},

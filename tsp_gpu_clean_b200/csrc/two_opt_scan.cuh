@@ -144,10 +144,17 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
     int c = 0;
     for (int r0 = 0; r0 < k; r0 += 4) {
       int cc[4];
+      if constexpr (GROUPED && U % 4 == 0) {  // k % 4 == 0 and a 16-byte aligned table
+        uint32_t w[4];
+        load_words<4>(packed + ((unsigned)a * (unsigned)k + (unsigned)r0), w);
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const unsigned ar = (unsigned)a * (unsigned)k + (unsigned)(r0 + u);
-        cc[u] = r0 + u < k ? (PACKED ? (int)(__ldg(packed + ar) & 0xffffu) : __ldg(cand + ar)) : -1;
+        for (int u = 0; u < 4; ++u) cc[u] = (int)(w[u] & 0xffffu);
+      } else {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const unsigned ar = (unsigned)a * (unsigned)k + (unsigned)(r0 + u);
+          cc[u] = r0 + u < k ? (PACKED ? (int)(__ldg(packed + ar) & 0xffffu) : __ldg(cand + ar)) : -1;
+        }
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u)
