@@ -499,7 +499,9 @@ def run_uneven_bench(args) -> dict:
                      "buckets": [{"n": [b.lo, b.hi], "coords": b.coords, "instances": len(b.items),
                                   "two_opt_threads": b.two_opt_threads, "offspring_threads": b.offspring_threads}
                                  for b in solver.buckets],
-                     "setup_s": solver.last_timing["setup_s"], "tune_s_total": tune_s}}
+                     "setup_s": solver.last_timing["setup_s"], "tune_s_total": tune_s,
+                     "setup_parts_s": {k: round(solver.last_timing[k], 3)
+                                       for k in ("setup_operands_s", "setup_tape_s", "setup_nn_init_s")}}}
 
 
 def main_uneven(args) -> int:

@@ -208,6 +208,24 @@ int tspb_nn_init(const int32_t* customers, int32_t n, const int32_t* cand, int32
                  size_t workspace_bytes, int32_t* out, void* stream);
 
 /*
+ * Nearest-neighbour initial tours of many instances in one launch (customers 0..n-1 of
+ * each job), thread per (job, row), each row computed exactly as tspb_nn_init computes it.
+ * `jobs` is a device array; job j uses rows * (2 n + k) int32 of `workspace` from element
+ * ws_offsets[j] (device int64 array); max_rows bounds every job's rows.
+ */
+typedef struct tspb_nn_job {
+  int32_t n;              /* customers 0..n-1 */
+  int32_t k;              /* k-NN entries per row of cand (0: uniform choices only) */
+  const int32_t* cand;    /* n x k */
+  const uint64_t* seeds;  /* [rows] SplitMix64 row seeds (draw_row_seeds) */
+  int32_t* out;           /* rows x n */
+  int32_t rows;
+  int32_t pad;
+} tspb_nn_job;
+int tspb_nn_init_jobs(const tspb_nn_job* jobs, int32_t num_jobs, int32_t max_rows, int32_t* workspace,
+                      const int64_t* ws_offsets, void* stream);
+
+/*
  * One GA generation as graph-capturable steps. The random draws of all generations are
  * pre-drawn on the host in the reference's order and passed as a tape; `gen` (device
  * int) selects generation g's slice and is advanced by tspb_generation_track, `stopped`

@@ -68,7 +68,11 @@ def test_autotuner_picks_fastest_and_caches(tmp_path):
 def test_ctypes_structs_match_the_c_header(tmp_path):
   fields_i = [f[0] for f in native.BatchInstance._fields_]
   fields_b = [f[0] for f in native.BatchState._fields_]
+  fields_j = [f[0] for f in native.NNJob._fields_]
   src = ["#include <stdio.h>", "#include <stddef.h>", '#include "tspb.h"', "int main(void) {"]
+  src.append('printf("%zu\\n", sizeof(tspb_nn_job));')
+  for f in fields_j:
+    src.append(f'printf("%zu\\n", offsetof(tspb_nn_job, {f}));')
   src.append('printf("%zu\\n", sizeof(tspb_batch_instance));')
   for f in fields_i:
     src.append(f'printf("%zu\\n", offsetof(tspb_batch_instance, {f}));')
@@ -81,6 +85,7 @@ def test_ctypes_structs_match_the_c_header(tmp_path):
   exe = tmp_path / "layout"
   subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(c), "-o", str(exe)], check=True)
   out = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
-  want = [ctypes.sizeof(native.BatchInstance)] + [getattr(native.BatchInstance, f).offset for f in fields_i]
+  want = [ctypes.sizeof(native.NNJob)] + [getattr(native.NNJob, f).offset for f in fields_j]
+  want += [ctypes.sizeof(native.BatchInstance)] + [getattr(native.BatchInstance, f).offset for f in fields_i]
   want += [ctypes.sizeof(native.BatchState)] + [getattr(native.BatchState, f).offset for f in fields_b]
   assert out == want

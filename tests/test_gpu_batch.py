@@ -177,3 +177,28 @@ def test_autotuner_cache_is_reused(batch_mod, tmp_path):
       assert tuner.measured == 0
   for a, b in zip(*outs):
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("concurrent", [True, False])
+def test_rebuilt_distances_and_serial_buckets_match_oracle(batch_mod, concurrent):
+  """A tuner that always picks distances rebuilt from coordinates (buckets drop their
+  matrices), with buckets launched concurrently or one after another: same runs."""
+  from tsp_gpu_clean_b200.autotune import BatchAutotuner
+  from tsp_gpu_clean_b200.fused import LocalSearchConfig
+  from tsp_gpu_clean_b200.instances import uniform_instance
+  from tsp_gpu_clean_b200.problem import Problem, ProblemContext
+
+  class PickRebuild(BatchAutotuner):
+    def choose(self, key, candidates, probe):
+      odd = [c for c in candidates if c & 1]
+      return odd[-1] if ("two_opt" in key and odd) else list(candidates)[0]
+
+  insts = [(uniform_instance(n, 300 + n), 400 + n) for n in (33, 90, 180, 260)]
+  ctxs = [ProblemContext(Problem.from_coordinates(c), seed=s) for c, s in insts]
+  solver = batch_mod.FusedBatchSolver(population_size=24, mutation_rate=0.1, elite_count=4, post_init=True,
+                                      local_search=LocalSearchConfig("best", 10, 20), tuner=PickRebuild(),
+                                      bucket_bounds=(64, 128), concurrent_buckets=concurrent)
+  res = solver.evolve(ctxs, 15, patience=10**9)
+  assert all(b.coords for b in solver.buckets)
+  for idx, (coords, seed) in enumerate(insts):
+    _check_run(solver, res, ctxs, idx, _oracle_run(coords, seed, 24, 0.1, 4, True, "best", 10, 20, 15, 10**9))

@@ -51,7 +51,7 @@ from .autotune import BatchAutotuner
 from .device import operands_for, ptr, require_gpu, stream_handle, torch
 from .fused import LocalSearchConfig, draw_generation_tape
 from .problem import resolve_rng
-from .strategies.initialization import InitializationB200TourNearestNeighbor
+from .strategies.initialization import draw_row_seeds
 
 #: Upper n of the default size buckets (the last bucket takes every larger instance).
 DEFAULT_BUCKET_BOUNDS = (128, 256, 512, 1024, 2048, 4096)
@@ -69,6 +69,7 @@ class Bucket:
   items: list[int] = field(default_factory=list)
   max_n: int = 0
   grouped: bool = False  # every item's k % 4 == 0 and its packed table 16-byte aligned
+  can_rebuild: bool = False  # every item has coordinates: the tuner may pick them over the matrix
   two_opt_threads: int = 128
   offspring_threads: int = 128
   d_items: Any = None
@@ -90,7 +91,7 @@ class FusedBatchSolver:
                local_search: LocalSearchConfig | None = None, elite_count: int = 8, post_init: bool = True,
                max_matrix_dimension: int | None = 4096, use_graph: bool = True,
                tuner: BatchAutotuner | None = None, bucket_bounds: Sequence[int] = DEFAULT_BUCKET_BOUNDS,
-               chunk: int = 16, skip_converged: bool = True) -> None:
+               chunk: int = 16, skip_converged: bool = True, concurrent_buckets: bool = True) -> None:
     if population_size < 2:
       raise ValueError("population_size must be >= 2")
     self.P = int(population_size)
@@ -108,6 +109,8 @@ class FusedBatchSolver:
     self.use_graph = bool(use_graph)
     self.chunk = max(1, int(chunk))
     self.skip_converged = bool(skip_converged)
+    self.concurrent_buckets = bool(concurrent_buckets)
+    self._side: list = []
     self.tuner = tuner if tuner is not None else BatchAutotuner()
     self.bucket_bounds = tuple(sorted(int(b) for b in bucket_bounds))
     self.kernel_launches = 0
@@ -189,6 +192,23 @@ class FusedBatchSolver:
     native.check("tspb_batch_offspring", rc)
     self.kernel_launches += 1
 
+  def _per_bucket(self, fn) -> None:
+    """fn(bucket) for every bucket; with concurrent buckets each runs on its own side
+    stream forked from and joined back to the current stream (parallel graph branches)."""
+    if not self.concurrent_buckets or len(self.buckets) < 2:
+      for b in self.buckets:
+        fn(b)
+      return
+    main = torch.cuda.current_stream()
+    while len(self._side) < len(self.buckets):
+      self._side.append(torch.cuda.Stream())
+    for s, b in zip(self._side, self.buckets):
+      s.wait_stream(main)
+      with torch.cuda.stream(s):
+        fn(b)
+    for s in self._side[: len(self.buckets)]:
+      main.wait_stream(s)
+
   def _generation(self) -> None:
     """Enqueue one replay: finish RESUME runs, then one generation of every RUN run."""
     lib = native.load_library()
@@ -196,18 +216,15 @@ class FusedBatchSolver:
     sh = stream_handle()
     R, U = native.TSPB_BATCH_PHASE_RESUME, native.TSPB_BATCH_PHASE_RUN
     if self.elite:
-      for b in self.buckets:
-        self._two_opt(st, b, R)
+      self._per_bucket(lambda b: self._two_opt(st, b, R))
       native.check("tspb_batch_elite_cost", lib.tspb_batch_elite_cost(st, R, sh))
       native.check("tspb_batch_track", lib.tspb_batch_track(st, R, sh))
       self.kernel_launches += 2
-    for b in self.buckets:
-      self._offspring(st, b)
+    self._per_bucket(lambda b: self._offspring(st, b))
     native.check("tspb_batch_survival", lib.tspb_batch_survival(st, sh))
     self.kernel_launches += 3
     if self.elite:
-      for b in self.buckets:
-        self._two_opt(st, b, U)
+      self._per_bucket(lambda b: self._two_opt(st, b, U))
       native.check("tspb_batch_elite_cost", lib.tspb_batch_elite_cost(st, U, sh))
       self.kernel_launches += 1
     native.check("tspb_batch_track", lib.tspb_batch_track(st, U, sh))
@@ -229,11 +246,17 @@ class FusedBatchSolver:
       if self.elite:
         units = len(b.items) * self.elite
         key = self.tuner.key(name, "two_opt", mode=self.ls.mode, k=self.k, iters=int(self.ls.max_iterations),
-                             lo=b.lo, hi=b.hi, coords=b.coords, units=units)
-        cands = [t for t in TWO_OPT_THREADS if lib.tspb_batch_two_opt_occupancy(b.max_n, self._mode, t) > 0]
-        if not cands:
+                             lo=b.lo, hi=b.hi, coords=b.coords, rebuild=b.can_rebuild, units=units)
+        threads = [t for t in TWO_OPT_THREADS if lib.tspb_batch_two_opt_occupancy(b.max_n, self._mode, t) > 0]
+        if not threads:
           raise ValueError(f"instances of n={b.max_n} do not fit the batch 2-opt's shared memory")
-        b.two_opt_threads = self.tuner.choose(key, cands, lambda t, b=b: self._probe_two_opt(b, t))
+        # candidate = 2 * threads + source (1: distances rebuilt from coordinates)
+        sources = (0, 1) if (b.can_rebuild and not b.coords) else ((1,) if b.coords else (0,))
+        cands = [2 * t + src for t in threads for src in sources]
+        choice = self.tuner.choose(key, cands, lambda c, b=b: self._probe_two_opt(b, c // 2, bool(c & 1)))
+        b.two_opt_threads = choice // 2
+        if choice & 1 and not b.coords:
+          self._rebuild_from_coordinates(b)
       if self.G:
         key = self.tuner.key(name, "offspring", lo=b.lo, hi=b.hi, coords=b.coords, units=len(b.items) * self.P)
         b.offspring_threads = self.tuner.choose(key, list(OFFSPRING_THREADS),
@@ -252,9 +275,19 @@ class FusedBatchSolver:
     end.synchronize()
     return start.elapsed_time(end) / reps
 
-  def _probe_two_opt(self, b: Bucket, threads: int) -> float:
+  def _rebuild_from_coordinates(self, b: Bucket) -> None:
+    """The bucket's instances drop their matrix: every kernel rebuilds their distances from
+    the FP64 coordinates (the same values, bit for bit)."""
+    for i in b.items:
+      self.h_inst[i].dist = None
+      self.h_inst[i].dist_stride = 0
+    self.d_inst.copy_(torch.frombuffer(bytearray(self.h_inst), dtype=torch.uint8))
+    b.coords = True
+
+  def _probe_two_opt(self, b: Bucket, threads: int, rebuild: bool = False) -> float:
     """Elite-shaped 2-opt work of one bucket on scratch copies of the initial tours: the
-    first `elite` rows of every instance, refined for up to max_iterations passes."""
+    first `elite` rows of every instance, refined for up to max_iterations passes, with
+    the bucket's matrices or (rebuild) distances rebuilt from coordinates."""
     e = max(self.elite, 2)  # the probe batch needs P >= 2
     ns = self.ns
     offs = np.zeros(self.I, dtype=np.int64)
@@ -264,7 +297,11 @@ class FusedBatchSolver:
     ctypes.memmove(inst, self.h_inst, ctypes.sizeof(inst))
     for i in range(self.I):
       inst[i].pop_offset = int(offs[i])
+      if rebuild:
+        inst[i].dist = None
+        inst[i].dist_stride = 0
     d_inst = torch.frombuffer(bytearray(inst), dtype=torch.uint8).cuda()
+    flags = self._flags(b) | (native.TSPB_BATCH_COORDS if rebuild else 0)
     status = torch.zeros((self.I, e), dtype=torch.int32, device="cuda")
     st = self._state()
     st.P = e
@@ -286,7 +323,7 @@ class FusedBatchSolver:
 
     def run():
       fill()
-      rc = lib.tspb_batch_two_opt(st_ref, ptr(b.d_items), len(b.items), b.max_n, self._flags(b),
+      rc = lib.tspb_batch_two_opt(st_ref, ptr(b.d_items), len(b.items), b.max_n, flags,
                                   native.TSPB_BATCH_PHASE_POSTINIT, self._mode, int(self.ls.max_iterations), threads, 0,
                                   ptr(b.queue), stream_handle())
       native.check("tspb_batch_two_opt", rc)
@@ -301,6 +338,33 @@ class FusedBatchSolver:
     # offspring writes only the scratch rows `off`, `off_fit`, `off_clean`: safe on the live state
     st_ref = ctypes.byref(self.state)
     return self._timed(lambda: self._offspring(st_ref, b, threads))
+
+  def _nn_init(self, h_jobs, seeds_all: np.ndarray, tables: list, ns: list[int]) -> None:
+    """GRASP nearest-neighbour populations of every instance in one launch
+    (`tspb_nn_init_jobs`, each row as `InitializationCPUTourNearestNeighbor` builds it)."""
+    P = self.P
+    ks = [int(t.shape[1]) if t.ndim == 2 else 0 for t in tables]
+    cand_off = np.zeros(self.I + 1, dtype=np.int64)
+    cand_off[1:] = np.cumsum([n * k for n, k in zip(ns, ks)])
+    flat = np.zeros(max(int(cand_off[-1]), 1), dtype=np.int32)
+    for i, t in enumerate(tables):
+      flat[cand_off[i]: cand_off[i + 1]] = t.reshape(-1)
+    d_cand = torch.from_numpy(flat).cuda()
+    d_seeds = torch.from_numpy(seeds_all.view(np.int64)).cuda()
+    ws_off = np.zeros(self.I + 1, dtype=np.int64)
+    ws_off[1:] = np.cumsum([P * (2 * n + k) for n, k in zip(ns, ks)])
+    d_ws = torch.empty(max(int(ws_off[-1]), 1), dtype=torch.int32, device="cuda")
+    d_ws_off = torch.from_numpy(ws_off[:-1].copy()).cuda()
+    for i, (n, k) in enumerate(zip(ns, ks)):
+      job = h_jobs[i]
+      job.n, job.k, job.rows = n, k, P
+      job.cand = d_cand.data_ptr() + int(cand_off[i]) * 4
+      job.seeds = d_seeds.data_ptr() + i * P * 8
+      job.out = self.pop[0].data_ptr() + self.pop_offsets[i] * 4
+    d_jobs = torch.frombuffer(bytearray(h_jobs), dtype=torch.uint8).cuda()
+    native.call("tspb_nn_init_jobs", ptr(d_jobs), self.I, P, ptr(d_ws), ptr(d_ws_off), stream_handle())
+    torch.cuda.current_stream().synchronize()  # the host buffers above are released on return
+    self.kernel_launches += 1
 
   # ------------------------------------------------------------------------ evolve
   def evolve(self, contexts: Sequence[Any], max_generations: int, patience: Any = None):
@@ -344,24 +408,32 @@ class FusedBatchSolver:
     self.clean = [torch.zeros((self.I, P), dtype=torch.uint8, device=dev) for _ in range(2)]
     self.off_clean = torch.zeros((self.I, P), dtype=torch.uint8, device=dev)
 
-    # per instance: NN init (row seeds first), operands, tape
-    init = InitializationB200TourNearestNeighbor(k=self.nn_k, return_gpu=True)
+    # per instance: NN row seeds (drawn first, like the reference), operands, tape
     h_inst = (native.BatchInstance * self.I)()
+    h_jobs = (native.NNJob * self.I)()
+    seeds_all = np.empty((self.I, P), dtype=np.uint64)
+    nn_tables = []
     tapes = [np.empty((self.I, G, P, self.kt), np.int32), np.empty((self.I, G, P // 2), np.int32),
              np.empty((self.I, G, P // 2), np.int32), np.empty((self.I, G, P), np.float64),
              np.empty((self.I, G, P), np.int32), np.empty((self.I, G, P), np.int32)]
     self.states = []
     self._keep = []
     coords_flags = []
+    rebuildable = []
+    t_ops = t_tape = 0.0
     for i, (ctx, n, rng) in enumerate(zip(contexts, ns, rngs)):
-      pop0 = init.initialize(list(range(n)), P, ctx)
-      self.pop[0][self.pop_offsets[i]: self.pop_offsets[i] + P * n].copy_(pop0.reshape(-1))
+      seeds_all[i] = draw_row_seeds(rng, P)  # nearest_neighbor_init.py:118-121
+      nn_tables.append(np.ascontiguousarray(ctx.get_cpu_candidate_list(self.nn_k), dtype=np.int32))
+      t0 = time.perf_counter()
       ops = operands_for(ctx)
       dist, stride, coords = ops.distance_args(n, self.max_matrix_dimension)
       tabs = ops.candidates(k, ctx.get_cpu_candidate_list(k), n, self.max_matrix_dimension)
       if tabs.packed is None:
         raise ValueError(f"instance {i}: k-NN table does not pack into 16-bit ids and distances")
+      t1 = time.perf_counter()
       tape, states = draw_generation_tape(rng, G, P, self.kt, n)
+      t_ops += t1 - t0
+      t_tape += time.perf_counter() - t1
       for a, t in zip(tapes, tape):
         a[i] = t
       self.states.append(states)
@@ -373,11 +445,18 @@ class FusedBatchSolver:
       inst.node_offset = int(prefix[i])
       inst.dist = dist.data_ptr() if dist is not None else None
       inst.dist_stride = int(stride)
-      inst.coords = coords.data_ptr() if coords is not None else None
+      has_xy = ops._euc2d_on_device() or coords is not None
+      xy = coords if coords is not None else (ops.coords() if has_xy else None)
+      inst.coords = xy.data_ptr() if xy is not None else None
+      rebuildable.append(xy is not None)
+      self._keep.append(xy)
       inst.cand_packed = tabs.packed.data_ptr()
       pat = patience[i] if isinstance(patience, (list, tuple, np.ndarray)) else patience
       inst.patience = int(pat) if pat is not None else int(2 * math.sqrt(n))
       coords_flags.append(dist is None)
+    t0 = time.perf_counter()
+    self._nn_init(h_jobs, seeds_all, nn_tables, ns)
+    t_nn = time.perf_counter() - t0
     self.h_inst = h_inst
     self.d_inst = torch.frombuffer(bytearray(h_inst), dtype=torch.uint8).cuda()
     self.tape = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in tapes]
@@ -389,6 +468,7 @@ class FusedBatchSolver:
     self.buckets = self._make_buckets(ns, coords_flags)
     for b in self.buckets:
       b.grouped = all(h_inst[i].k % 4 == 0 and h_inst[i].cand_packed % 16 == 0 for i in b.items)
+      b.can_rebuild = all(rebuildable[i] for i in b.items)
       b.d_items = torch.tensor(b.items, dtype=torch.int32, device=dev)
       b.queue = torch.zeros(1, dtype=torch.int32, device=dev)
 
@@ -496,7 +576,8 @@ class FusedBatchSolver:
     # 2-opt work inside the generation loop (the post-init refinement excluded)
     self.two_opt_totals = {"passes": int(stats_all[0]), "pairs": int(stats_all[1]), "moves": int(stats_all[2]),
                            "evaluated": int(stats_all[3])}
-    self.last_timing = {"setup_s": t_setup - t_start, "tune_s": t_tuned - t_setup, "loop_s": t_end - t_loop,
+    self.last_timing = {"setup_s": t_setup - t_start, "setup_operands_s": t_ops, "setup_tape_s": t_tape,
+                        "setup_nn_init_s": t_nn, "tune_s": t_tuned - t_setup, "loop_s": t_end - t_loop,
                         "total_s": t_end - t_start, "loop_ms_device": loop_ms,
                         "generations": int(ctl[:, 3].sum()) if G > 0 else 0, "replays": self.replays,
                         "rounds": rounds}

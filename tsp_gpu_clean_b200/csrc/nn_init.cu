@@ -83,9 +83,88 @@ __global__ void nn_init_kernel(const int32_t* __restrict__ customers, int n, con
   }
 }
 
+// One thread per (job, row): the same procedure with customers 0..n-1 of each job, all
+// jobs in one launch (the rows of every instance of a batch start together).
+__global__ void nn_init_jobs_kernel(const tspb_nn_job* __restrict__ jobs, int num_jobs, int32_t* __restrict__ ws,
+                                    const long long* __restrict__ ws_offsets) {
+  const int j = blockIdx.y;
+  if (j >= num_jobs) return;
+  const tspb_nn_job J = jobs[j];
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= J.rows) return;
+  const int n = J.n, k = J.k;
+  if (n <= 0) return;
+  const long long per = 2LL * n + k;
+  int32_t* unv = ws + ws_offsets[j] + (long long)row * per;
+  int32_t* pmap = unv + n;
+  int32_t* order = pmap + n;
+  int32_t* dst = J.out + (long long)row * n;
+  for (int q = 0; q < n; ++q) {
+    unv[q] = q;
+    pmap[q] = q;
+  }
+  unsigned long long st = J.seeds[row];
+  int rem = n;
+  int s = (int)splitmix64_bounded(st, (unsigned)rem);
+  int cur = unv[s];
+  dst[0] = cur;
+  int last = rem - 1;
+  int ln = unv[last];
+  unv[s] = ln;
+  unv[last] = cur;
+  pmap[ln] = s;
+  pmap[cur] = last;
+  rem = last;
+  for (int step = 1; step < n; ++step) {
+    int chosen = -1;
+    if (k > 0) {
+      for (int i = 0; i < k; ++i) order[i] = i;
+      const int32_t* crow = J.cand + (long long)cur * k;
+      for (int i = 0; i < k; ++i) {
+        const int jj = i + (int)splitmix64_bounded(st, (unsigned)(k - i));
+        const int tmp = order[i];
+        order[i] = order[jj];
+        order[jj] = tmp;
+        const int nb = __ldg(crow + order[i]);
+        if (nb >= 0 && nb < n) {
+          const int p = pmap[nb];
+          if (p >= 0 && p < rem) {
+            chosen = nb;
+            break;
+          }
+        }
+      }
+    }
+    if (chosen < 0) chosen = unv[(int)splitmix64_bounded(st, (unsigned)rem)];
+    dst[step] = chosen;
+    const int p = pmap[chosen];
+    last = rem - 1;
+    ln = unv[last];
+    unv[p] = ln;
+    unv[last] = chosen;
+    pmap[ln] = p;
+    pmap[chosen] = last;
+    rem = last;
+    cur = chosen;
+  }
+}
+
 }  // namespace tspb
 
 using namespace tspb;
+
+extern "C" int tspb_nn_init_jobs(const tspb_nn_job* jobs, int32_t num_jobs, int32_t max_rows, int32_t* workspace,
+                                 const int64_t* ws_offsets, void* stream) {
+  if (num_jobs < 0 || max_rows < 0) return TSPB_ERR_ARG;
+  if (num_jobs == 0 || max_rows == 0) return TSPB_OK;
+  if (!jobs || !workspace || !ws_offsets) return TSPB_ERR_ARG;
+  if (num_jobs > 65535) return TSPB_ERR_UNSUPPORTED;
+  const int threads = 64;
+  const dim3 grid((max_rows + threads - 1) / threads, num_jobs);
+  nn_init_jobs_kernel<<<grid, threads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+      jobs, num_jobs, workspace, reinterpret_cast<const long long*>(ws_offsets));
+  return tspb_launch_status();
+}
 
 extern "C" int tspb_nn_init(const int32_t* customers, int32_t n, const int32_t* cand, int32_t cand_rows, int32_t k,
                             const uint64_t* seeds, int32_t pop, int32_t max_node, int32_t* workspace,

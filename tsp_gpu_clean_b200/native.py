@@ -68,6 +68,7 @@ SIGNATURES: dict[str, tuple] = {
                                    ctypes.c_float, _p]),
   "tspb_select_topk": (ctypes.c_int, [_p, _p, _i32, _i32, _i32, _p, _p]),
   "tspb_nn_init": (ctypes.c_int, [_p, _i32, _p, _i32, _i32, _p, _i32, _i32, _p, _sz, _p, _p]),
+  "tspb_nn_init_jobs": (ctypes.c_int, [_p, _i32, _i32, _p, _p, _p]),
   "tspb_batch_init": (ctypes.c_int, [_p, _i32, _i32, _p]),
   "tspb_batch_offspring": (ctypes.c_int, [_p, _p, _i32, _i32, _i32, _p]),
   "tspb_batch_survival": (ctypes.c_int, [_p, _p]),
@@ -87,6 +88,12 @@ TSPB_BATCH_PHASE_RESUME = 1
 TSPB_BATCH_PHASE_RUN = 2
 TSPB_BATCH_COORDS = 1
 TSPB_BATCH_GROUPED = 2
+
+
+class NNJob(ctypes.Structure):
+  """`tspb_nn_job` of include/tspb.h."""
+
+  _fields_ = [("n", _i32), ("k", _i32), ("cand", _p), ("seeds", _p), ("out", _p), ("rows", _i32), ("pad", _i32)]
 
 
 class BatchInstance(ctypes.Structure):
