@@ -226,6 +226,31 @@ int tspb_nn_init_jobs(const tspb_nn_job* jobs, int32_t num_jobs, int32_t max_row
                       const int64_t* ws_offsets, void* stream);
 
 /*
+ * The GA's random tape drawn exactly as NumPy's Generator(PCG64) draws it from
+ * `context.rng` (src/utils/rng.py:48-64), in the reference's per-generation order:
+ * tournament integers(0, P, (P, kt)) (tournament_selection.py:113), PMX cut pairs
+ * sample_distinct_pairs(P/2, 0, n) (pmx_crossover.py:155), inversion random(P)
+ * (inversion_mutation.py:82), inversion pairs sample_distinct_pairs(P, 0, n)
+ * (route_helpers.py:214). `tspb_pcg64` holds bit_generator.state: the 128-bit state and
+ * increment as (hi, lo) halves, has_uint32 and uinteger. The generator is advanced in
+ * place; `states` (optional, [G]) receives the state after each generation.
+ * tspb_tape_draw_host: one run on the host (plain C, no device).
+ * tspb_tape_draw: `num` runs on the device, one thread per run; gens, ns, the tape
+ *   arrays ([num][G][...]) and states ([num][G]) are device pointers.
+ */
+typedef struct tspb_pcg64 {
+  uint64_t state_hi, state_lo, inc_hi, inc_lo;
+  int32_t has_uint32;
+  uint32_t uinteger;
+} tspb_pcg64;
+int tspb_tape_draw_host(tspb_pcg64* gen, int32_t G, int32_t P, int32_t kt, int32_t n, int32_t* tourn,
+                        int32_t* cut_a, int32_t* cut_b, double* u, int32_t* inv_a, int32_t* inv_b,
+                        tspb_pcg64* states);
+int tspb_tape_draw(tspb_pcg64* gens, const int32_t* ns, int32_t num, int32_t G, int32_t P, int32_t kt,
+                   int32_t* tourn, int32_t* cut_a, int32_t* cut_b, double* u, int32_t* inv_a, int32_t* inv_b,
+                   tspb_pcg64* states, void* stream);
+
+/*
  * One GA generation as graph-capturable steps. The random draws of all generations are
  * pre-drawn on the host in the reference's order and passed as a tape; `gen` (device
  * int) selects generation g's slice and is advanced by tspb_generation_track, `stopped`

@@ -202,3 +202,43 @@ def test_rebuilt_distances_and_serial_buckets_match_oracle(batch_mod, concurrent
   assert all(b.coords for b in solver.buckets)
   for idx, (coords, seed) in enumerate(insts):
     _check_run(solver, res, ctxs, idx, _oracle_run(coords, seed, 24, 0.1, 4, True, "best", 10, 20, 15, 10**9))
+
+
+def test_device_tape_equals_numpy(batch_mod):
+  """`tspb_tape_draw` (one thread per run) gives every run NumPy's draws and end state."""
+  import ctypes
+
+  import torch
+
+  from tsp_gpu_clean_b200 import native
+  from tsp_gpu_clean_b200.device import ptr, stream_handle
+  from tsp_gpu_clean_b200.fused import draw_generation_tape_numpy
+
+  ns, G, P, kt = [5, 17, 300, 4899, 4], 12, 10, 5
+  rngs = [np.random.default_rng(70 + i) for i in range(len(ns))]
+  for i, r in enumerate(rngs):
+    r.integers(0, 9, size=i, dtype=np.int32)
+  refs = [np.random.Generator(np.random.PCG64()) for _ in ns]
+  for r, q in zip(refs, rngs):
+    r.bit_generator.state = q.bit_generator.state
+  I = len(ns)
+  h = (native.Pcg64 * I)(*[native.Pcg64.from_state(r.bit_generator.state) for r in rngs])
+  d_gens = torch.frombuffer(bytearray(h), dtype=torch.uint8).cuda()
+  d_ns = torch.tensor(ns, dtype=torch.int32, device="cuda")
+  tape = [torch.zeros((I, G, P, kt), dtype=torch.int32, device="cuda"),
+          torch.zeros((I, G, P // 2), dtype=torch.int32, device="cuda"),
+          torch.zeros((I, G, P // 2), dtype=torch.int32, device="cuda"),
+          torch.zeros((I, G, P), dtype=torch.float64, device="cuda"),
+          torch.zeros((I, G, P), dtype=torch.int32, device="cuda"),
+          torch.zeros((I, G, P), dtype=torch.int32, device="cuda")]
+  states = torch.zeros(I * G * ctypes.sizeof(native.Pcg64), dtype=torch.uint8, device="cuda")
+  native.call("tspb_tape_draw", ptr(d_gens), ptr(d_ns), I, G, P, kt, *[ptr(t) for t in tape], ptr(states),
+              stream_handle())
+  final = (native.Pcg64 * I).from_buffer_copy(d_gens.cpu().numpy().tobytes())
+  per_gen = (native.Pcg64 * (I * G)).from_buffer_copy(states.cpu().numpy().tobytes())
+  for i, (r, n) in enumerate(zip(refs, ns)):
+    want, wst = draw_generation_tape_numpy(r, G, P, kt, n)
+    for t, w in zip(tape, want):
+      assert np.array_equal(t[i].cpu().numpy(), w)
+    assert [per_gen[i * G + g].to_state() for g in range(G)] == list(wst)
+    assert final[i].to_state() == r.bit_generator.state

@@ -339,6 +339,49 @@ class FusedBatchSolver:
     st_ref = ctypes.byref(self.state)
     return self._timed(lambda: self._offspring(st_ref, b, threads))
 
+  def _draw_tapes(self, rngs: list, ns: list[int]) -> None:
+    """Every run's random tape, drawn on the device by `tspb_tape_draw` (one thread per run,
+    NumPy's PCG64 stream restated) when every generator is PCG64, else by NumPy on the host.
+    Each generator ends in the state it has after the reference draws G generations."""
+    I, G, P, kt = self.I, self.G, self.P, self.kt
+    dev = "cuda"
+    self.tape = [torch.empty((I, G, P, kt), dtype=torch.int32, device=dev),
+                 torch.empty((I, G, P // 2), dtype=torch.int32, device=dev),
+                 torch.empty((I, G, P // 2), dtype=torch.int32, device=dev),
+                 torch.empty((I, G, P), dtype=torch.float64, device=dev),
+                 torch.empty((I, G, P), dtype=torch.int32, device=dev),
+                 torch.empty((I, G, P), dtype=torch.int32, device=dev)]
+    gens = [native.Pcg64.from_state(r.bit_generator.state) for r in rngs]
+    self._dev_states = None
+    self.states = []
+    if G == 0:
+      return
+    if all(g is not None for g in gens):
+      h_gens = (native.Pcg64 * I)(*gens)
+      d_gens = torch.frombuffer(bytearray(h_gens), dtype=torch.uint8).cuda()
+      d_ns = torch.tensor(ns, dtype=torch.int32, device=dev)
+      self._dev_states = torch.empty(I * G * ctypes.sizeof(native.Pcg64), dtype=torch.uint8, device=dev)
+      native.call("tspb_tape_draw", ptr(d_gens), ptr(d_ns), I, G, P, kt, *[ptr(t) for t in self.tape],
+                  ptr(self._dev_states), stream_handle())
+      self.kernel_launches += 1
+      final = (native.Pcg64 * I).from_buffer_copy(d_gens.cpu().numpy().tobytes())
+      for r, g in zip(rngs, final):
+        r.bit_generator.state = g.to_state()
+      return
+    for i, (r, n) in enumerate(zip(rngs, ns)):
+      tape, states = draw_generation_tape(r, G, P, kt, n)
+      for t, a in zip(self.tape, tape):
+        t[i].copy_(torch.from_numpy(np.ascontiguousarray(a)))
+      self.states.append(states)
+
+  def _state_after(self, i: int, g: int) -> dict:
+    """Generator state of run i after generation g (0-based)."""
+    if self._dev_states is None:
+      return self.states[i][g]
+    sz = ctypes.sizeof(native.Pcg64)
+    off = (i * self.G + g) * sz
+    return native.Pcg64.from_buffer_copy(self._dev_states[off: off + sz].cpu().numpy().tobytes()).to_state()
+
   def _nn_init(self, h_jobs, seeds_all: np.ndarray, tables: list, ns: list[int]) -> None:
     """GRASP nearest-neighbour populations of every instance in one launch
     (`tspb_nn_init_jobs`, each row as `InitializationCPUTourNearestNeighbor` builds it)."""
@@ -413,10 +456,7 @@ class FusedBatchSolver:
     h_jobs = (native.NNJob * self.I)()
     seeds_all = np.empty((self.I, P), dtype=np.uint64)
     nn_tables = []
-    tapes = [np.empty((self.I, G, P, self.kt), np.int32), np.empty((self.I, G, P // 2), np.int32),
-             np.empty((self.I, G, P // 2), np.int32), np.empty((self.I, G, P), np.float64),
-             np.empty((self.I, G, P), np.int32), np.empty((self.I, G, P), np.int32)]
-    self.states = []
+
     self._keep = []
     coords_flags = []
     rebuildable = []
@@ -430,13 +470,7 @@ class FusedBatchSolver:
       tabs = ops.candidates(k, ctx.get_cpu_candidate_list(k), n, self.max_matrix_dimension)
       if tabs.packed is None:
         raise ValueError(f"instance {i}: k-NN table does not pack into 16-bit ids and distances")
-      t1 = time.perf_counter()
-      tape, states = draw_generation_tape(rng, G, P, self.kt, n)
-      t_ops += t1 - t0
-      t_tape += time.perf_counter() - t1
-      for a, t in zip(tapes, tape):
-        a[i] = t
-      self.states.append(states)
+      t_ops += time.perf_counter() - t0
       self._keep.append((dist, coords, tabs))
       inst = h_inst[i]
       inst.n = n
@@ -456,10 +490,11 @@ class FusedBatchSolver:
       coords_flags.append(dist is None)
     t0 = time.perf_counter()
     self._nn_init(h_jobs, seeds_all, nn_tables, ns)
-    t_nn = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    self._draw_tapes(rngs, ns)  # after the row seeds, like the reference
+    t_nn, t_tape = t1 - t0, time.perf_counter() - t1
     self.h_inst = h_inst
     self.d_inst = torch.frombuffer(bytearray(h_inst), dtype=torch.uint8).cuda()
-    self.tape = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in tapes]
     self.state = self._state()
     st = ctypes.byref(self.state)
     lib = native.load_library()
@@ -557,7 +592,7 @@ class FusedBatchSolver:
     for i, rng in enumerate(rngs):
       done = int(ctl[i, 3]) if G > 0 else 0
       if 0 < done < G:
-        rng.bit_generator.state = self.states[i][done - 1]
+        rng.bit_generator.state = self._state_after(i, done - 1)
       parity = done % 2
       n = ns[i]
       self.final_population.append(self.pop[parity][self.pop_offsets[i]: self.pop_offsets[i] + P * n].view(P, n))

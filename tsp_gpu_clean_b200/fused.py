@@ -36,6 +36,7 @@ to its state after the last generation that ran.
 
 from __future__ import annotations
 
+import ctypes
 import math
 import time
 from dataclasses import dataclass
@@ -50,7 +51,37 @@ from .routes import sample_distinct_pairs
 from .strategies.initialization import InitializationB200TourNearestNeighbor
 
 
+class GeneratorStates:
+  """Generator state after each generation of a natively drawn tape, as bit_generator.state
+  dicts on demand."""
+
+  def __init__(self, raw):
+    self.raw = raw
+
+  def __len__(self) -> int:
+    return len(self.raw)
+
+  def __getitem__(self, g: int) -> dict:
+    return self.raw[g].to_state()
+
+
 def draw_generation_tape(rng: np.random.Generator, G: int, P: int, kt: int, n: int):
+  """`draw_generation_tape_numpy`'s draws and end state, computed by libtspb's restatement
+  of NumPy's PCG64 stream (`tspb_tape_draw_host`) when `rng` is a PCG64 generator, else
+  by NumPy itself."""
+  g = native.Pcg64.from_state(rng.bit_generator.state)
+  if g is None or n < 2 or P < 2 or G <= 0:
+    return draw_generation_tape_numpy(rng, G, P, kt, n)
+  arrs = (np.empty((G, P, kt), np.int32), np.empty((G, P // 2), np.int32), np.empty((G, P // 2), np.int32),
+          np.empty((G, P), np.float64), np.empty((G, P), np.int32), np.empty((G, P), np.int32))
+  raw = (native.Pcg64 * G)()
+  native.call("tspb_tape_draw_host", ctypes.byref(g), G, P, kt, n,
+              *[a.ctypes.data_as(ctypes.c_void_p) for a in arrs], raw)
+  rng.bit_generator.state = g.to_state()
+  return arrs, GeneratorStates(raw)
+
+
+def draw_generation_tape_numpy(rng: np.random.Generator, G: int, P: int, kt: int, n: int):
   """Random draws of G generations from `rng` in the reference's order.
 
   Per generation: tournament contestants (P, kt) (`tournament_selection.py:113`), PMX cut

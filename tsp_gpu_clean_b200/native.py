@@ -69,6 +69,8 @@ SIGNATURES: dict[str, tuple] = {
   "tspb_select_topk": (ctypes.c_int, [_p, _p, _i32, _i32, _i32, _p, _p]),
   "tspb_nn_init": (ctypes.c_int, [_p, _i32, _p, _i32, _i32, _p, _i32, _i32, _p, _sz, _p, _p]),
   "tspb_nn_init_jobs": (ctypes.c_int, [_p, _i32, _i32, _p, _p, _p]),
+  "tspb_tape_draw_host": (ctypes.c_int, [_p, _i32, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _p]),
+  "tspb_tape_draw": (ctypes.c_int, [_p, _p, _i32, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _p, _p]),
   "tspb_batch_init": (ctypes.c_int, [_p, _i32, _i32, _p]),
   "tspb_batch_offspring": (ctypes.c_int, [_p, _p, _i32, _i32, _i32, _p]),
   "tspb_batch_survival": (ctypes.c_int, [_p, _p]),
@@ -88,6 +90,28 @@ TSPB_BATCH_PHASE_RESUME = 1
 TSPB_BATCH_PHASE_RUN = 2
 TSPB_BATCH_COORDS = 1
 TSPB_BATCH_GROUPED = 2
+
+
+class Pcg64(ctypes.Structure):
+  """`tspb_pcg64` of include/tspb.h: a NumPy PCG64 bit_generator.state."""
+
+  _fields_ = [("state_hi", ctypes.c_uint64), ("state_lo", ctypes.c_uint64), ("inc_hi", ctypes.c_uint64),
+              ("inc_lo", ctypes.c_uint64), ("has_uint32", _i32), ("uinteger", ctypes.c_uint32)]
+
+  _M = (1 << 64) - 1
+
+  @classmethod
+  def from_state(cls, state: dict) -> "Pcg64 | None":
+    if state.get("bit_generator") != "PCG64":
+      return None
+    s, inc = int(state["state"]["state"]), int(state["state"]["inc"])
+    return cls(s >> 64, s & cls._M, inc >> 64, inc & cls._M, int(state["has_uint32"]), int(state["uinteger"]))
+
+  def to_state(self) -> dict:
+    return {"bit_generator": "PCG64",
+            "state": {"state": (int(self.state_hi) << 64) | int(self.state_lo),
+                      "inc": (int(self.inc_hi) << 64) | int(self.inc_lo)},
+            "has_uint32": int(self.has_uint32), "uinteger": int(self.uinteger)}
 
 
 class NNJob(ctypes.Structure):
