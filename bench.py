@@ -359,7 +359,7 @@ def run_ga_bench(args) -> dict:
       (best, stats), = solver.evolve([ctx], G, patience=10**9)
     else:
       solver = FusedMemeticSolver(population_size=P, mutation_rate=0.05, tournament_k=5, nn_k=5, local_search=ls,
-                                  elite_count=elite, post_init=post_init, chunk=args.chunk)
+                                  elite_count=elite, post_init=post_init, chunk=args.chunk, engine="single")
       best, stats = solver.evolve(ctx, list(range(n)), G, patience=10**9)
     wall = time.perf_counter() - t0
     return solver, stats, wall
@@ -656,8 +656,8 @@ def main(argv=None) -> int:
   ap.add_argument("--eval-starts", type=int, default=8)
   ap.add_argument("--ga-label-generations", type=int, default=0)
   ap.add_argument("--chunk", type=int, default=16, help="GA: generations replayed between host checks")
-  ap.add_argument("--engine", default="single", choices=["single", "batch"],
-                  help="GA: one-run fused solver or the multi-instance batch engine with one instance")
+  ap.add_argument("--engine", default="batch", choices=["single", "batch"],
+                  help="GA: the multi-instance batch engine with one instance, or the one-run graph engine")
   ap.add_argument("--cpu-gens", type=int, default=0, help="GA: generations in the CPU sample (0: workload default)")
   args = ap.parse_args(argv)
   if args.workload == "learned":

@@ -31,9 +31,10 @@ def _digest(t):
   return hashlib.sha256(np.ascontiguousarray(t.cpu().numpy(), dtype=np.int32).tobytes()).hexdigest()
 
 
+@pytest.mark.parametrize("engine", ["batch", "single"])
 @pytest.mark.parametrize("use_graph", [True, False])
 @pytest.mark.parametrize("tag", ["c1", "c1default", "c3"])
-def test_fused_matches_reference(fused_mod, golden, tag, use_graph):
+def test_fused_matches_reference(fused_mod, golden, tag, use_graph, engine):
   from tsp_gpu_clean_b200.problem import Problem, ProblemContext
 
   g = golden("ga.npz")
@@ -42,7 +43,8 @@ def test_fused_matches_reference(fused_mod, golden, tag, use_graph):
   ctx = ProblemContext(Problem.from_coordinates(coords), seed=seed)
   solver = fused_mod.FusedMemeticSolver(population_size=pop_size, mutation_rate=float(g[f"{tag}_rate"]), tournament_k=5,
                                         nn_k=5, local_search=fused_mod.LocalSearchConfig("best", ls_iters, 20),
-                                        elite_count=elite, post_init=bool(post_init), use_graph=use_graph, chunk=7)
+                                        elite_count=elite, post_init=bool(post_init), use_graph=use_graph, chunk=7,
+                                        engine=engine)
   patience = None if tag == "c1default" else 10**9
   best, stats = solver.evolve(ctx, list(range(len(coords))), gens, patience=patience)
   assert stats["generations_completed"] == int(g[f"{tag}_gens"])
@@ -53,7 +55,8 @@ def test_fused_matches_reference(fused_mod, golden, tag, use_graph):
   assert ctx.rng.bit_generator.state["state"]["state"] % (1 << 63) == int(g[f"{tag}_rng"][0])
 
 
-def test_fused_with_elite_boundary_ties_matches_oracle(fused_mod):
+@pytest.mark.parametrize("engine", ["batch", "single"])
+def test_fused_with_elite_boundary_ties_matches_oracle(fused_mod, engine):
   """Integer-lattice cities give many equal tour lengths: ties across the elite edge
   make membership depend on NumPy's unstable argsort, resolved on the host."""
   from tsp_gpu_clean_b200.problem import Problem, ProblemContext
@@ -64,7 +67,8 @@ def test_fused_with_elite_boundary_ties_matches_oracle(fused_mod):
   for seed in (3, 4):
     ctx = ProblemContext(Problem.from_coordinates(coords), seed=seed)
     solver = fused_mod.FusedMemeticSolver(population_size=40, mutation_rate=0.3, elite_count=6, post_init=False,
-                                          local_search=fused_mod.LocalSearchConfig("best", 2, 8), chunk=5)
+                                          local_search=fused_mod.LocalSearchConfig("best", 2, 8), chunk=5,
+                                          engine=engine)
     best, stats = solver.evolve(ctx, list(range(n)), 40, patience=10**9)
     D = odist.euc2d_matrix(coords)
     cfg = oga.GAConfig(population_size=40, mutation_rate=0.3, nn_k=5, tournament_k=5,

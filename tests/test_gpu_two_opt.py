@@ -210,7 +210,7 @@ _LAYOUT_ORACLE: dict = {}
 @pytest.mark.parametrize("threads", [128, 512])
 def test_table_layouts_agree(b200, mode, k, threads):
   """Plain candidates, packed words, and packed words read in row groups (k % 4 == 0) give
-  the same tours and the same pass/pair/move/gain counts, equal to the oracle's."""
+  the same tours and the same pass/pair/move counts, equal to the oracle's."""
   import torch
 
   from tsp_gpu_clean_b200 import native
@@ -237,7 +237,9 @@ def test_table_layouts_agree(b200, mode, k, threads):
     assert int(status.max().item()) == 0
     outs.append((work.cpu().numpy(), stats.cpu().numpy()))
   assert np.array_equal(outs[0][0], outs[1][0])
-  assert np.array_equal(outs[0][1], outs[1][1])
+  # passes, oracle-equivalent pairs and moves agree; the count of gains actually computed
+  # (column 3) depends on the round width in first mode (a round finishes before stopping)
+  assert np.array_equal(outs[0][1][:, :3], outs[1][1][:, :3])
   key = (mode, k)
   if key not in _LAYOUT_ORACLE:
     _LAYOUT_ORACLE[key] = otwo.improve_batch(tours, odist.euc2d_matrix(coords), ctx.get_cpu_candidate_list(k), mode,

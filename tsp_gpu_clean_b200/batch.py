@@ -59,6 +59,17 @@ TWO_OPT_THREADS = (64, 128, 256, 512, 1024)
 OFFSPRING_THREADS = (64, 128, 256)
 
 
+_DEFAULT_TUNER: BatchAutotuner | None = None
+
+
+def default_tuner() -> BatchAutotuner:
+  """The process-wide tuner (its cache spans every solver of the process)."""
+  global _DEFAULT_TUNER
+  if _DEFAULT_TUNER is None:
+    _DEFAULT_TUNER = BatchAutotuner()
+  return _DEFAULT_TUNER
+
+
 @dataclass
 class Bucket:
   """Instances of one size class and the launch shapes chosen for them."""
@@ -111,7 +122,7 @@ class FusedBatchSolver:
     self.skip_converged = bool(skip_converged)
     self.concurrent_buckets = bool(concurrent_buckets)
     self._side: list = []
-    self.tuner = tuner if tuner is not None else BatchAutotuner()
+    self.tuner = tuner if tuner is not None else default_tuner()
     self.bucket_bounds = tuple(sorted(int(b) for b in bucket_bounds))
     self.kernel_launches = 0
     self.replays = 0

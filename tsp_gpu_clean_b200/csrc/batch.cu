@@ -396,12 +396,20 @@ static int batch_two_opt_mode(const tspb_batch& b, const int32_t* items, int num
     case 256:
       return batch_two_opt_launch<MODE, 256, 4>(b, items, num_items, rows, phase, max_iter, max_n, smem, ctas, flags,
                                                 queue, st);
+    // wide CTAs keep four entries per thread in flight only in the grouped layout (fewer
+    // registers per entry there); otherwise two
     case 512:
-      return batch_two_opt_launch<MODE, 512, 2>(b, items, num_items, rows, phase, max_iter, max_n, smem, ctas, flags,
-                                                queue, st);
+      return (flags & TSPB_BATCH_GROUPED)
+                 ? batch_two_opt_launch<MODE, 512, 4>(b, items, num_items, rows, phase, max_iter, max_n, smem, ctas,
+                                                      flags, queue, st)
+                 : batch_two_opt_launch<MODE, 512, 2>(b, items, num_items, rows, phase, max_iter, max_n, smem, ctas,
+                                                      flags, queue, st);
     case 1024:
-      return batch_two_opt_launch<MODE, 1024, 2>(b, items, num_items, rows, phase, max_iter, max_n, smem, ctas, flags,
-                                                 queue, st);
+      return (flags & TSPB_BATCH_GROUPED)
+                 ? batch_two_opt_launch<MODE, 1024, 4>(b, items, num_items, rows, phase, max_iter, max_n, smem, ctas,
+                                                       flags, queue, st)
+                 : batch_two_opt_launch<MODE, 1024, 2>(b, items, num_items, rows, phase, max_iter, max_n, smem, ctas,
+                                                       flags, queue, st);
     default: return TSPB_ERR_ARG;
   }
 }

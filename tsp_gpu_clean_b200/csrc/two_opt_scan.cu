@@ -92,7 +92,10 @@ static int launch_scan_mode(const TwoOptArgs& a, int threads, size_t smem, cudaS
   switch (threads) {
     case 64: return launch_scan<MODE, 64, 4>(a, smem, st);
     case 128: return launch_scan<MODE, 128, 4>(a, smem, st);
-    case 512: return launch_scan<MODE, 512, 2>(a, smem, st);
+    case 512: {  // four entries per thread in flight only where the grouped layout applies
+      const bool grouped = a.cand_packed && a.k % 4 == 0 && (reinterpret_cast<uintptr_t>(a.cand_packed) % 16) == 0;
+      return grouped ? launch_scan<MODE, 512, 4>(a, smem, st) : launch_scan<MODE, 512, 2>(a, smem, st);
+    }
     default: return launch_scan<MODE, 256, 4>(a, smem, st);
   }
 }

@@ -119,9 +119,13 @@ class LocalSearchConfig:
 class FusedMemeticSolver:
   def __init__(self, population_size: int = 128, mutation_rate: float = 0.05, tournament_k: int = 5, nn_k: int = 5,
                local_search: LocalSearchConfig | None = None, elite_count: int = 16, post_init: bool = True,
-               use_graph: bool = True, chunk: int = 16, max_matrix_dimension: int | None = None) -> None:
+               use_graph: bool = True, chunk: int = 16, max_matrix_dimension: int | None = None,
+               engine: str = "batch") -> None:
     if population_size < 2:
       raise ValueError("population_size must be >= 2")
+    if engine not in ("batch", "single"):
+      raise ValueError("engine must be 'batch' (the multi-instance engine with one run) or 'single'")
+    self.engine = engine
     self.P = population_size
     self.rate = mutation_rate
     self.kt = tournament_k
@@ -205,6 +209,8 @@ class FusedMemeticSolver:
     n = len(customers)
     if n < 4 or n != int(context.dimension) or list(customers) != list(range(n)):
       raise ValueError("FusedMemeticSolver needs the full tour customers = range(dimension) with dimension >= 4")
+    if self.engine == "batch":
+      return self._evolve_batch(context, max_generations, patience)
     if patience is None:
       patience = int(2 * math.sqrt(n))
     self.n, self.patience = n, patience
@@ -326,6 +332,25 @@ class FusedMemeticSolver:
       "host_elite_generations": self.host_elite_generations,
     }
     return best_tour, stats
+
+  def _evolve_batch(self, context: Any, max_generations: int, patience: int | None):
+    """The run as a one-instance batch (`batch.FusedBatchSolver`): the persistent 2-opt,
+    converged-row skipping and device-settled elite ties of the batch engine, same results."""
+    from .batch import FusedBatchSolver
+
+    solver = FusedBatchSolver(population_size=self.P, mutation_rate=self.rate, tournament_k=self.kt, nn_k=self.nn_k,
+                              local_search=self.ls, elite_count=self.elite, post_init=self.post_init,
+                              max_matrix_dimension=self.max_matrix_dimension, use_graph=self.use_graph,
+                              chunk=self.chunk)
+    (best, stats), = solver.evolve([context], max_generations, patience=patience)
+    self.final_population = solver.final_population[0]
+    self.final_fitness = solver.final_fitness[0]
+    self.last_timing = solver.last_timing
+    self.kernel_launches = solver.kernel_launches
+    self.host_elite_generations = stats["host_elite_generations"]
+    self.two_opt_totals = solver.two_opt_totals
+    stats = dict(stats, kernel_launches=solver.kernel_launches)
+    return best, stats
 
   # -------------------------------------------------------------------------- graph, snapshots
   def _capture(self):
