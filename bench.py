@@ -144,6 +144,35 @@ def _dist_env():
   return world, rank, local
 
 
+def _init_ranks():
+  """(world, rank) after binding this process to its GPU and, under torchrun, joining the
+  NCCL process group (short timeout: ranks that wait for one another end with an error)."""
+  import datetime
+
+  import torch
+  import torch.distributed as dist
+
+  world, rank, local = _dist_env()
+  torch.cuda.set_device(local)
+  if world > 1 and not dist.is_initialized():
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+  return world, rank
+
+
+def _barrier(world: int) -> None:
+  if world > 1:
+    import torch.distributed as dist
+
+    dist.barrier()
+
+
+def _finish_ranks(world: int) -> None:
+  if world > 1:
+    import torch.distributed as dist
+
+    dist.destroy_process_group()
+
+
 def aggregate(units: float, elapsed_s: float, world: int):
   """(sum of units over ranks, max elapsed over ranks); identity for one process."""
   if world <= 1:
@@ -339,6 +368,7 @@ def run_ga_bench(args) -> dict:
   from tsp_gpu_clean_b200.fused import FusedMemeticSolver, LocalSearchConfig
   from tsp_gpu_clean_b200.problem import Problem, ProblemContext
 
+  world, rank = _init_ranks()
   build_library()
   n, P, G, elite, post_init, seed, desc = GA_WORKLOADS[args.workload]
   coords = instances.uniform_instance(n, seed)
@@ -349,7 +379,8 @@ def run_ga_bench(args) -> dict:
   tuner = BatchAutotuner()
 
   def run_once():
-    ctx = ProblemContext(Problem.from_coordinates(coords), seed=42)
+    # one replica per rank: the same instance, the run's generator seeded per rank
+    ctx = ProblemContext(Problem.from_coordinates(coords), seed=42 + rank)
     ls = LocalSearchConfig("best", 10, 20)
     t0 = time.perf_counter()
     if args.engine == "batch":
@@ -367,6 +398,7 @@ def run_ga_bench(args) -> dict:
   for _ in range(args.warmup):
     run_once()
   torch.cuda.synchronize()
+  _barrier(world)
   loop_ms, walls, launches, gens = [], [], 0, 0
   with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
     for _ in range(args.steps):
@@ -375,11 +407,18 @@ def run_ga_bench(args) -> dict:
       walls.append(wall)
       launches += solver.kernel_launches
       gens += stats["generations_completed"]
-  value = gens / (sum(loop_ms) / 1e3)
-  return {"value": value, "ms_per_step": sum(loop_ms) / args.steps, "clocks": clocks.summary(),
-          "e2e": {"value": gens / sum(walls), "unit": "generations/s", "h2d_bytes_per_step": int(coords.nbytes),
+  torch.cuda.synchronize()
+  _barrier(world)
+  units, loop_s = aggregate(gens, sum(loop_ms) / 1e3, world)
+  e2e_units, wall_s = aggregate(gens, sum(walls), world)
+  _finish_ranks(world)
+  value = units / loop_s
+  return {"value": value, "ms_per_step": 1e3 * loop_s / args.steps, "clocks": clocks.summary(), "world": world,
+          "rank": rank,
+          "e2e": {"value": e2e_units / wall_s, "unit": "generations/s", "h2d_bytes_per_step": int(coords.nbytes),
                   "d2h_bytes_per_step": int(n * 4 + (G + 1) * 8 + P * n * 4)},
           "gpu_launches": launches, "desc": desc, "best": stats["best_fitness"],
+          "loop_ms_steps": [round(v, 3) for v in loop_ms],
           "timing": {k: round(v, 4) for k, v in solver.last_timing.items() if isinstance(v, (int, float))}}
 
 
@@ -397,10 +436,10 @@ def _knn_tables(c):
   return {5: compute_candidate_list(5, coords=c), 20: compute_candidate_list(20, coords=c)}
 
 
-def _uneven_inputs(count: int, pool=None):
+def _uneven_inputs(count: int, pool=None, seed: int = UNEVEN_SEED):
   """Coordinates of the batch and their host k-NN tables (k = 5 for the NN init, 20 for
   2-opt), computed once like a ProblemContext's candidate cache (on the host cores)."""
-  coords = instances.uneven_batch(count, UNEVEN_SEED)
+  coords = instances.uneven_batch(count, seed)
   order = sorted(range(count), key=lambda i: -len(coords[i]))  # largest first for the pool
   if pool is not None:
     tabs = pool.map(_knn_tables, [coords[i] for i in order], chunksize=1)
@@ -452,6 +491,7 @@ def run_uneven_bench(args) -> dict:
   from tsp_gpu_clean_b200.fused import LocalSearchConfig
   from tsp_gpu_clean_b200.problem import Problem, ProblemContext
 
+  world, rank = _init_ranks()
   build_library()
   coords, caches = args.uneven_inputs
   G = args.generations
@@ -471,6 +511,7 @@ def run_uneven_bench(args) -> dict:
   for _ in range(args.warmup):
     run_once()
   torch.cuda.synchronize()
+  _barrier(world)
   loop_ms, walls, launches, gens, pairs, tune_s, pauses, ties = [], [], 0, 0, 0, 0.0, 0, 0
   with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
     for _ in range(args.steps):
@@ -483,16 +524,22 @@ def run_uneven_bench(args) -> dict:
       tune_s += solver.last_timing["tune_s"]
       pauses += sum(st["host_elite_generations"] for _, st in res)
       ties += sum(st["elite_edge_ties"] for _, st in res)
-  loop_s = sum(loop_ms) / 1e3
+  torch.cuda.synchronize()
+  _barrier(world)
+  all_gens, loop_s = aggregate(gens, sum(loop_ms) / 1e3, world)
+  e2e_gens, wall_s = aggregate(gens, sum(walls), world)
+  all_pairs, _ = aggregate(pairs, 0.0, world)
+  _finish_ranks(world)
   total_n = sum(len(c) for c in coords)
   h2d = sum(c.nbytes for c in coords) + sum(len(c) * (5 + 20) * 4 for c in coords)
   h2d += len(coords) * G * 64 * (5 * 4 + 4 + 8 + 2 * 4)  # the tape
   d2h = total_n * 4 + len(coords) * (G + 1) * 8
-  return {"value": gens / loop_s, "ms_per_step": sum(loop_ms) / args.steps, "clocks": clocks.summary(),
-          "e2e": {"value": gens / sum(walls), "unit": "generations/s", "h2d_bytes_per_step": int(h2d),
-                  "d2h_bytes_per_step": int(d2h)},
+  return {"value": all_gens / loop_s, "ms_per_step": 1e3 * loop_s / args.steps, "clocks": clocks.summary(),
+          "world": world, "rank": rank,
+          "e2e": {"value": e2e_gens / wall_s, "unit": "generations/s", "h2d_bytes_per_step": int(h2d * world),
+                  "d2h_bytes_per_step": int(d2h * world)},
           "gpu_launches": launches,
-          "detail": {"deltas_per_s": pairs / loop_s, "tours_evaluated_per_s": gens * (64 + 8) / loop_s,
+          "detail": {"deltas_per_s": all_pairs / loop_s, "tours_evaluated_per_s": all_gens * (64 + 8) / loop_s,
                      "replays_per_step": solver.replays, "host_checks_per_step": solver.last_timing["rounds"],
                      "generations_per_step": gens // args.steps,
                      "elite_edge_ties_per_step": ties // args.steps, "host_pauses_per_step": pauses // args.steps,
@@ -529,15 +576,20 @@ def main_uneven(args) -> int:
             "e2e": {"value": value, "unit": "generations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
-  pool = mp.get_context("spawn").Pool(workers)  # before the first CUDA call
-  args.uneven_inputs = _uneven_inputs(count, pool)
+  # weak scaling: every rank gets its own batch of `count` instances (rank-specific seed)
+  pool = mp.get_context("spawn").Pool(max(1, workers // max(world, 1)))  # before the first CUDA call
+  args.uneven_inputs = _uneven_inputs(count, pool, seed=UNEVEN_SEED + 7919 * rank)
   if rank != 0 or world != 1 or args.no_cpu_baseline:
     pool.close()
     pool.join()
     pool = None
   res = run_uneven_bench(args)
+  if res["rank"] != 0:
+    return 0
+  if res["world"] > 1:
+    config["parallelism"] = f"{res['world']} ranks, each its own {count}-instance batch (weak scaling, no collective)"
   line = {"metric": "generations/s (aggregate over instances)", "value": res["value"], "unit": "generations/s",
-          "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
+          "n_gpus": res["world"], "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
           "data": "synthetic (seeded)", "config": config, "clocks": res["clocks"], "e2e": res["e2e"],
           "gpu_launches": res["gpu_launches"], "detail": res["detail"]}
@@ -749,12 +801,18 @@ def main_ga(args) -> int:
     print(json.dumps(line))
     return 0
   res = run_ga_bench(args)
-  line = {"metric": "generations/s", "value": res["value"], "unit": "generations/s", "n_gpus": 1, "steps": args.steps,
+  if res["rank"] != 0:
+    return 0
+  line = {"metric": "generations/s", "value": res["value"], "unit": "generations/s", "n_gpus": res["world"],
+          "steps": args.steps,
           "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
           "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)", "config": config, "clocks": res["clocks"],
           "e2e": res["e2e"], "gpu_launches": res["gpu_launches"],
-          "detail": {"best_fitness": res["best"], "engine": args.engine, "last_run": res["timing"]}}
-  if not args.no_cpu_baseline:
+          "detail": {"best_fitness": res["best"], "engine": args.engine, "last_run": res["timing"],
+                     "loop_ms_steps": res["loop_ms_steps"]}}
+  if res["world"] > 1:
+    config["parallelism"] = f"{res['world']} independent replicas (one GA run per GPU, generator seeded per rank)"
+  if not args.no_cpu_baseline and res["world"] == 1:
     cpu = _ga_cpu_gens_per_s(args.workload, sample)
     line["cpu_baseline"] = {"value": cpu["value"], "unit": "generations/s", "cores": 1, "kind": "port",
                             "sample": f"{sample} generations of the NumPy GA (init excluded), {cpu['loop_s']:.1f} s"}

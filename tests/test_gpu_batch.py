@@ -242,3 +242,20 @@ def test_device_tape_equals_numpy(batch_mod):
       assert np.array_equal(t[i].cpu().numpy(), w)
     assert [per_gen[i * G + g].to_state() for g in range(G)] == list(wst)
     assert final[i].to_state() == r.bit_generator.state
+
+
+def test_many_small_runs_device_tape_match_oracle(batch_mod):
+  """34 runs (the tape is drawn on the device from 32 runs up), every one bit-exact."""
+  from tsp_gpu_clean_b200.fused import LocalSearchConfig
+  from tsp_gpu_clean_b200.instances import uniform_instance
+  from tsp_gpu_clean_b200.problem import Problem, ProblemContext
+
+  assert batch_mod.DEVICE_TAPE_MIN_RUNS <= 34
+  insts = [(uniform_instance(5 + (7 * i) % 26, 500 + i), 600 + i) for i in range(34)]
+  ctxs = [ProblemContext(Problem.from_coordinates(c), seed=s) for c, s in insts]
+  solver = batch_mod.FusedBatchSolver(population_size=10, mutation_rate=0.2, elite_count=3, post_init=True,
+                                      local_search=LocalSearchConfig("best", 5, 6))
+  res = solver.evolve(ctxs, 6, patience=10**9)
+  assert solver._dev_states is not None
+  for idx, (coords, seed) in enumerate(insts):
+    _check_run(solver, res, ctxs, idx, _oracle_run(coords, seed, 10, 0.2, 3, True, "best", 5, 6, 6, 10**9))

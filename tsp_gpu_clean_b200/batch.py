@@ -56,7 +56,28 @@ from .strategies.initialization import draw_row_seeds
 #: Upper n of the default size buckets (the last bucket takes every larger instance).
 DEFAULT_BUCKET_BOUNDS = (128, 256, 512, 1024, 2048, 4096)
 TWO_OPT_THREADS = (64, 128, 256, 512, 1024)
+#: Runs from which the tape is drawn on the device (one thread per run) instead of the host.
+DEVICE_TAPE_MIN_RUNS = 32
 OFFSPRING_THREADS = (64, 128, 256)
+
+
+def capture_graph(enqueue) -> "torch.cuda.CUDAGraph":
+  """A CUDA graph of the launches `enqueue()` makes, captured on a side stream with the
+  plain begin/end calls (the `torch.cuda.graph` context manager also runs a full Python
+  garbage collection and empties the allocator cache on entry, which costs up to a second
+  in a long-lived process)."""
+  stream = torch.cuda.Stream()
+  stream.wait_stream(torch.cuda.current_stream())
+  g = torch.cuda.CUDAGraph()
+  with torch.cuda.stream(stream):
+    g.capture_begin(capture_error_mode="relaxed")
+    try:
+      enqueue()
+    finally:
+      g.capture_end()
+  torch.cuda.current_stream().wait_stream(stream)
+  torch.cuda.synchronize()
+  return g
 
 
 _DEFAULT_TUNER: BatchAutotuner | None = None
@@ -367,7 +388,8 @@ class FusedBatchSolver:
     self.states = []
     if G == 0:
       return
-    if all(g is not None for g in gens):
+    # one device thread per run pays only with many runs; a few runs draw faster on the host
+    if all(g is not None for g in gens) and I >= DEVICE_TAPE_MIN_RUNS:
       h_gens = (native.Pcg64 * I)(*gens)
       d_gens = torch.frombuffer(bytearray(h_gens), dtype=torch.uint8).cuda()
       d_ns = torch.tensor(ns, dtype=torch.int32, device=dev)
@@ -379,11 +401,14 @@ class FusedBatchSolver:
       for r, g in zip(rngs, final):
         r.bit_generator.state = g.to_state()
       return
+    host = [np.empty(tuple(t.shape), dtype=np.float64 if t.dtype == torch.float64 else np.int32) for t in self.tape]
     for i, (r, n) in enumerate(zip(rngs, ns)):
       tape, states = draw_generation_tape(r, G, P, kt, n)
-      for t, a in zip(self.tape, tape):
-        t[i].copy_(torch.from_numpy(np.ascontiguousarray(a)))
+      for h, a in zip(host, tape):
+        h[i] = a
       self.states.append(states)
+    for t, h in zip(self.tape, host):
+      t.copy_(torch.from_numpy(h))
 
   def _state_after(self, i: int, g: int) -> dict:
     """Generator state of run i after generation g (0-based)."""
@@ -538,6 +563,7 @@ class FusedBatchSolver:
     per_replay = self._launches_per_replay()
     torch.cuda.synchronize()
     t_loop = time.perf_counter()
+    t_prep = t_loop - t_tuned  # post-init refinement, graph capture
     ev_start = torch.cuda.Event(enable_timing=True)
     ev_end = torch.cuda.Event(enable_timing=True)
     ev_start.record()
@@ -623,7 +649,8 @@ class FusedBatchSolver:
     self.two_opt_totals = {"passes": int(stats_all[0]), "pairs": int(stats_all[1]), "moves": int(stats_all[2]),
                            "evaluated": int(stats_all[3])}
     self.last_timing = {"setup_s": t_setup - t_start, "setup_operands_s": t_ops, "setup_tape_s": t_tape,
-                        "setup_nn_init_s": t_nn, "tune_s": t_tuned - t_setup, "loop_s": t_end - t_loop,
+                        "setup_nn_init_s": t_nn, "tune_s": t_tuned - t_setup, "postinit_capture_s": t_prep,
+                        "results_s": time.perf_counter() - t_end, "loop_s": t_end - t_loop,
                         "total_s": t_end - t_start, "loop_ms_device": loop_ms,
                         "generations": int(ctl[:, 3].sum()) if G > 0 else 0, "replays": self.replays,
                         "rounds": rounds}
@@ -638,12 +665,6 @@ class FusedBatchSolver:
     self._generation()
     torch.cuda.synchronize()
     self.ctl.copy_(saved)
-    stream = torch.cuda.Stream()
-    stream.wait_stream(torch.cuda.current_stream())
-    g = torch.cuda.CUDAGraph()
-    with torch.cuda.graph(g, stream=stream, capture_error_mode="relaxed"):
-      self._generation()
-    torch.cuda.current_stream().wait_stream(stream)
-    torch.cuda.synchronize()
+    g = capture_graph(self._generation)
     self.kernel_launches = launches
     return g

@@ -360,14 +360,6 @@ class FusedMemeticSolver:
     self._generation(1)
     torch.cuda.synchronize()
     self.stopped.fill_(0)
-    graphs = []
-    stream = torch.cuda.Stream()
-    stream.wait_stream(torch.cuda.current_stream())
-    for parity in (0, 1):
-      g = torch.cuda.CUDAGraph()
-      with torch.cuda.graph(g, stream=stream, capture_error_mode="relaxed"):
-        self._generation(parity)
-      graphs.append(g)
-    torch.cuda.current_stream().wait_stream(stream)
-    torch.cuda.synchronize()
-    return graphs
+    from .batch import capture_graph
+
+    return [capture_graph(lambda p=parity: self._generation(p)) for parity in (0, 1)]
