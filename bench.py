@@ -386,11 +386,12 @@ def run_ga_bench(args) -> dict:
     if args.engine == "batch":
       solver = FusedBatchSolver(population_size=P, mutation_rate=0.05, tournament_k=5, nn_k=5, local_search=ls,
                                 elite_count=elite, post_init=post_init, max_matrix_dimension=None, tuner=tuner,
-                                chunk=args.chunk)
+                                chunk=args.chunk, use_graph=not args.no_graph)
       (best, stats), = solver.evolve([ctx], G, patience=10**9)
     else:
       solver = FusedMemeticSolver(population_size=P, mutation_rate=0.05, tournament_k=5, nn_k=5, local_search=ls,
-                                  elite_count=elite, post_init=post_init, chunk=args.chunk, engine="single")
+                                  elite_count=elite, post_init=post_init, chunk=args.chunk, engine="single",
+                                  use_graph=not args.no_graph)
       best, stats = solver.evolve(ctx, list(range(n)), G, patience=10**9)
     wall = time.perf_counter() - t0
     return solver, stats, wall
@@ -502,7 +503,8 @@ def run_uneven_bench(args) -> dict:
             for i, c in enumerate(coords)]
     solver = FusedBatchSolver(population_size=64, mutation_rate=0.05, tournament_k=5, nn_k=5,
                               local_search=LocalSearchConfig("best", 10, 20), elite_count=8, post_init=True,
-                              max_matrix_dimension=4096, tuner=tuner, chunk=args.chunk)
+                              max_matrix_dimension=4096, tuner=tuner, chunk=args.chunk,
+                              use_graph=not args.no_graph)
     t0 = time.perf_counter()
     res = solver.evolve(ctxs, G, patience=10**9)
     wall = time.perf_counter() - t0
@@ -708,6 +710,9 @@ def main(argv=None) -> int:
   ap.add_argument("--eval-starts", type=int, default=8)
   ap.add_argument("--ga-label-generations", type=int, default=0)
   ap.add_argument("--chunk", type=int, default=16, help="GA: generations replayed between host checks")
+  ap.add_argument("--no-graph", action="store_true",
+                  help="GA/uneven: launch every generation directly instead of replaying a captured graph "
+                       "(for kernel profilers, which do not follow launches inside a stream capture)")
   ap.add_argument("--engine", default="batch", choices=["single", "batch"],
                   help="GA: the multi-instance batch engine with one instance, or the one-run graph engine")
   ap.add_argument("--cpu-gens", type=int, default=0, help="GA: generations in the CPU sample (0: workload default)")
