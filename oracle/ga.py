@@ -43,6 +43,8 @@ class GAConfig:
   post_init: bool = True
   elite_count: int | None = 16
   periodic: tuple[int, str] | None = None  # (interval, target)
+  crossover: str = "pmx"  # "pmx" (CrossoverCPUPermPartiallyMapped) or "ox" (CrossoverCPUPermOrder)
+  mutation: str = "inversion"  # "inversion" (MutationCPUPermInversion) or "swap" (MutationCPUPermSwap)
 
 
 def routes_digest(routes: np.ndarray) -> str:
@@ -125,9 +127,10 @@ class OracleGA:
         elif s == "select":
           off = ga_ops.tournament_select(rng, pop, fit, cfg.population_size, cfg.tournament_k)
         elif s == "crossover":
-          off = ga_ops.pmx_batch(rng, off)
+          off = ga_ops.ox_batch(rng, off) if cfg.crossover == "ox" else ga_ops.pmx_batch(rng, off)
         elif s == "mutate":
-          off = ga_ops.inversion_batch(rng, off, cfg.mutation_rate)
+          off = (ga_ops.swap_batch(rng, off, cfg.mutation_rate) if cfg.mutation == "swap"
+                 else ga_ops.inversion_batch(rng, off, cfg.mutation_rate))
         elif s == "ls_offspring":
           off = self._improve(off)
         elif s == "eval_offspring":

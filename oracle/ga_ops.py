@@ -117,6 +117,74 @@ def pmx_batch(rng, batch: np.ndarray) -> np.ndarray:
   return pmx_apply(batch, pmx_cuts(rng, len(batch), batch.shape[1]))
 
 
+def ox_child(p1: np.ndarray, p2: np.ndarray, c1: int, c2: int) -> np.ndarray:
+  """One Order Crossover child of open permutations (`order_crossover.py:52-83`,
+  `is_closed=False`): the child keeps p1[c1..c2]; the free positions c2+1, ..., n-1, 0,
+  ..., c1-1 take, in this order, the genes of p2 read from index c2+1 onward (wrapping)
+  that are not in the kept segment."""
+  n = len(p1)
+  if n <= 1:
+    return p1.copy()
+  if c1 > c2:
+    c1, c2 = c2, c1
+  child = np.full(n, -1, dtype=np.int32)
+  child[c1 : c2 + 1] = p1[c1 : c2 + 1]
+  kept = set(int(v) for v in p1[c1 : c2 + 1])
+  dst = (c2 + 1) % n
+  for t in range(n):
+    gene = int(p2[(c2 + 1 + t) % n])
+    if gene in kept:
+      continue
+    while child[dst] != -1:  # only the kept segment is pre-filled
+      dst = (dst + 1) % n
+    child[dst] = gene
+    dst = (dst + 1) % n
+  return child
+
+
+def ox_apply(batch: np.ndarray, pairs: np.ndarray) -> np.ndarray:
+  """OX children of pairs `(2k, 2k+1)` sharing cuts; odd tail copied (`order_crossover.py:150-168`)."""
+  batch = np.asarray(batch, dtype=np.int32)
+  out = np.empty_like(batch)
+  for kk in range(len(batch) // 2):
+    i = 2 * kk
+    c1 = int(min(pairs[kk, 0], pairs[kk, 1]))
+    c2 = int(max(pairs[kk, 0], pairs[kk, 1]))
+    out[i] = ox_child(batch[i], batch[i + 1], c1, c2)
+    out[i + 1] = ox_child(batch[i + 1], batch[i], c1, c2)
+  if len(batch) % 2 == 1:
+    out[-1] = batch[-1]
+  return out
+
+
+def ox_batch(rng, batch: np.ndarray) -> np.ndarray:
+  """`CrossoverCPUPermOrder.crossover_batch` (`order_crossover.py:127-168`): the cut pairs
+  are drawn exactly as PMX draws them."""
+  batch = np.asarray(batch, dtype=np.int32)
+  if batch.ndim == 1 or len(batch) < 2 or batch.shape[1] < 2:
+    return batch.copy()
+  return ox_apply(batch, pmx_cuts(rng, len(batch), batch.shape[1]))
+
+
+def swap_apply(batch: np.ndarray, rate: float, u, p1, p2) -> np.ndarray:
+  """Swap of positions p1[r], p2[r] in every row with u[r] < rate (`swap_mutation.py:94-99`)."""
+  out = np.asarray(batch, dtype=np.int32).copy()
+  for r in np.flatnonzero(np.asarray(u) < rate):
+    a, b = int(p1[r]), int(p2[r])
+    out[r, a], out[r, b] = out[r, b], out[r, a]
+  return out
+
+
+def swap_batch(rng, batch: np.ndarray, rate: float) -> np.ndarray:
+  """`MutationCPUPermSwap.mutate_batch` (`swap_mutation.py:65-99`, uniform positions): the
+  draws are those of inversion (u, then a distinct position pair per row)."""
+  batch = np.asarray(batch, dtype=np.int32)
+  if batch.shape[1] < 2:
+    return batch.copy()
+  u, p1, p2 = inversion_draw(rng, len(batch), batch.shape[1])
+  return swap_apply(batch, rate, u, p1, p2)
+
+
 def inversion_draw(rng, num_routes: int, n: int):
   """`u = random(N)` then the position pairs (`inversion_mutation.py:82-91`)."""
   u = rng.random(num_routes)

@@ -15,6 +15,8 @@ Outputs (NumPy `.npz`, committed next to this script):
                        plus integer-lattice tie cases and duplicate-candidate tables;
 - `two_opt_c2.npz`     four tours of the 1000-city, 20-cluster instance refined to a
                        local optimum in best and first mode, with pass and pair counts;
+- `ox_swap.npz`        Order Crossover and swap mutation batches, and two GA runs with them
+                       (`python make_golden.py <reference root> ox` regenerates only this file)
 - `ops.npz`            tournament selection, PMX, inversion, tour cost, candidate
                        lists and the EUC_2D matrix on seeded inputs;
 - `ga.npz`             full GA runs (the 100-city memetic run for 50 generations, a
@@ -299,5 +301,77 @@ def main(ref_root: str) -> None:
   np.savez_compressed(os.path.join(HERE, "ga.npz"), **ga_out)
 
 
+def main_ox_swap(ref_root: str) -> None:
+  """`ox_swap.npz`: Order Crossover and swap mutation batches of the reference's CPU
+  strategies, and two GA runs that use them (tournament + OX + swap + 2-opt elites)."""
+  _setup(ref_root)
+  from algorithms import GeneticAlgorithm
+  from algorithms.pipeline_steps import EliteOnlyLocalSearchStep, PostInitLocalSearchStep
+  from algorithms.strategies import (
+    CrossoverCPUPermOrder,
+    EvaluationCPUCost,
+    InitializationCPUTourNearestNeighbor,
+    LocalSearchCPUTourTwoOpt,
+    MutationCPUPermSwap,
+    SelectionCPUTournament,
+  )
+  from data_models.problem import Problem
+  from protocols.problem_context import ProblemContext
+
+  from tsp_gpu_clean_b200 import instances
+
+  def coord_problem(coords):
+    return Problem(name="synthetic", dimension=len(coords), problem_type="TSP", edge_type="EUC_2D",
+                   coordinates=np.asarray(coords, dtype=np.float64), distances=None)
+
+  out: dict[str, np.ndarray] = {}
+  for tag, n, pop_size, rate in (("a", 52, 129, 0.05), ("b", 100, 128, 0.5), ("c", 1000, 64, 1.0),
+                                 ("d", 7, 10, 0.0), ("e", 4, 6, 1.0), ("f", 2, 5, 1.0)):
+    coords = instances.uniform_instance(n, 5252 + n)
+    ctx = ProblemContext(coord_problem(coords), xp=np, seed=321 + n)
+    pop = instances.random_tours(n, pop_size, 29 + n)
+    ox = CrossoverCPUPermOrder(seed=1).crossover_batch(pop.copy(), ctx)
+    sw = MutationCPUPermSwap(seed=1).mutate_batch(np.asarray(ox).copy(), rate, ctx)
+    out[f"{tag}_meta"] = np.array([n, pop_size, 321 + n])
+    out[f"{tag}_rate"] = np.array(rate)
+    out[f"{tag}_pop"] = pop
+    out[f"{tag}_ox"] = np.asarray(ox, dtype=np.int32)
+    out[f"{tag}_swap"] = np.asarray(sw, dtype=np.int32)
+    out[f"{tag}_rng_state"] = np.array([ctx.rng.bit_generator.state["state"]["state"] % (1 << 63)], dtype=np.int64)
+
+  def run_ga(tag, coords, pop_size, gens, elite, mutation_rate, post_init, patience):
+    t = time.time()
+    ctx = ProblemContext(coord_problem(coords), xp=np, seed=7)
+    ls = LocalSearchCPUTourTwoOpt(mode="best", max_iterations=10, candidate_k=20)
+    ev = EvaluationCPUCost()
+    steps = []
+    if post_init:
+      steps.append(PostInitLocalSearchStep(local_search=ls, evaluation=ev))
+    steps.append(EliteOnlyLocalSearchStep(local_search=ls, evaluation=ev, elite_count=elite))
+    ga = GeneticAlgorithm(population_size=pop_size, mutation_rate=mutation_rate, seed=7,
+                          initialization=InitializationCPUTourNearestNeighbor(k=5, seed=7),
+                          selection=SelectionCPUTournament(k=5, seed=7), crossover=CrossoverCPUPermOrder(seed=7),
+                          mutation=MutationCPUPermSwap(seed=7), local_search=ls, evaluation=ev,
+                          local_search_stage="none", pipeline=steps)
+    best, stats = ga.evolve(context=ctx, customers=list(range(len(coords))), max_generations=gens, patience=patience)
+    out[f"ga_{tag}_coords"] = coords
+    out[f"ga_{tag}_meta"] = np.array([pop_size, gens, elite, int(post_init), -1 if patience is None else patience])
+    out[f"ga_{tag}_rate"] = np.array(mutation_rate)
+    out[f"ga_{tag}_best"] = np.asarray(best, dtype=np.int32)
+    out[f"ga_{tag}_history"] = np.asarray(stats["convergence_history"], dtype=np.float64)
+    out[f"ga_{tag}_gens"] = np.array(stats["generations_completed"])
+    out[f"ga_{tag}_rng"] = np.array([ctx.rng.bit_generator.state["state"]["state"] % (1 << 63)], dtype=np.int64)
+    print(f"ga {tag}: {time.time() - t:.1f}s best={stats['best_fitness']} gens={stats['generations_completed']}")
+
+  run_ga("ox1", instances.uniform_instance(100, 77), 128, 40, 16, 0.05, True, 10**9)
+  run_ga("ox2", instances.clustered_instance(300, 12, 30.0, 78), 64, 30, 8, 0.3, False, None)
+  np.savez_compressed(os.path.join(HERE, "ox_swap.npz"), **out)
+
+
 if __name__ == "__main__":
-  main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+  root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+  part = sys.argv[2] if len(sys.argv) > 2 else "all"
+  if part in ("all", "core"):
+    main(root)
+  if part in ("all", "ox"):
+    main_ox_swap(root)

@@ -127,3 +127,41 @@ def test_nn_init_matches_reference(golden):
   rng = np.random.default_rng(42)
   pop = ga_ops.nn_init(rng, np.arange(100), 128, distances.candidate_list(5, coords=coords))
   assert np.array_equal(pop, g["c1_init"])
+
+
+@pytest.mark.parametrize("tag", ["a", "b", "c", "d", "e", "f"])
+def test_ox_and_swap_match_reference(golden, tag):
+  g = golden("ox_swap.npz")
+  n, pop_size, seed = (int(v) for v in g[f"{tag}_meta"])
+  rng = np.random.default_rng(seed)
+  ox = ga_ops.ox_batch(rng, g[f"{tag}_pop"])
+  assert np.array_equal(ox, g[f"{tag}_ox"])
+  sw = ga_ops.swap_batch(rng, ox, float(g[f"{tag}_rate"]))
+  assert np.array_equal(sw, g[f"{tag}_swap"])
+  assert rng.bit_generator.state["state"]["state"] % (1 << 63) == int(g[f"{tag}_rng_state"][0])
+  for row in sw:
+    assert np.array_equal(np.sort(row), np.arange(n))
+
+
+@pytest.mark.parametrize("tag", ["ox1", "ox2"])
+def test_oracle_ga_with_ox_and_swap_matches_reference(golden, tag):
+  g = golden("ox_swap.npz")
+  coords = g[f"ga_{tag}_coords"]
+  pop_size, gens, elite, post_init, patience = (int(v) for v in g[f"ga_{tag}_meta"])
+  D = distances.euc2d_matrix(coords)
+  cache = {}
+
+  def provider(k):
+    if k not in cache:
+      cache[k] = distances.candidate_list(k, coords=coords)
+    return cache[k]
+
+  cfg = ga.GAConfig(population_size=pop_size, mutation_rate=float(g[f"ga_{tag}_rate"]), nn_k=5, tournament_k=5,
+                    local_search=ga.LocalSearchSpec("best", 10, 20), post_init=bool(post_init), elite_count=elite,
+                    crossover="ox", mutation="swap")
+  rng = np.random.default_rng(7)
+  best, _, _, stats, _ = ga.OracleGA(D, provider, cfg, rng).evolve(gens, patience=None if patience < 0 else patience)
+  assert stats["generations_completed"] == int(g[f"ga_{tag}_gens"])
+  assert np.array_equal(np.asarray(stats["convergence_history"]), g[f"ga_{tag}_history"])
+  assert np.array_equal(best, g[f"ga_{tag}_best"])
+  assert rng.bit_generator.state["state"]["state"] % (1 << 63) == int(g[f"ga_{tag}_rng"][0])
