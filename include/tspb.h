@@ -179,6 +179,35 @@ int tspb_pmx(const int32_t* parents, int32_t num_routes, int32_t n,
              int32_t* children, int32_t* status, void* stream);
 
 /*
+ * Order Crossover (OX) of pairs (2q, 2q+1) sharing cuts (first[q], second[q]); the odd
+ * tail row is copied. Open permutations. The child keeps p1[c1..c2]; the free positions
+ * c2+1, ..., n-1, 0, ..., c1-1 take p2's remaining genes in the order met reading p2 from
+ * c2+1 (wrapping). Replaces CrossoverCPUPermOrder._apply_ox / crossover_batch
+ *   (src/algorithms/strategies/crossover/order_crossover.py:52-83, 127-168) and
+ *   order_crossover_kernel (.../crossover/kernels/order_crossover.cu).
+ * A parent that is not a permutation of 0..n-1 gives status[row] = TSPB_ERR_NOT_PERMUTATION
+ * and the child is a copy of p1.
+ */
+int tspb_ox(const int32_t* parents, int32_t num_routes, int32_t n,
+            const int32_t* cut_first, const int32_t* cut_second,
+            int32_t* children, int32_t* status, void* stream);
+
+/*
+ * Swap mutation in place: positions pos1[r], pos2[r] of row r exchanged when u[r] < rate.
+ * Replaces MutationCPUPermSwap.mutate_batch
+ *   (src/algorithms/strategies/mutation/swap_mutation.py:65-99) and swap_mutation_kernel
+ *   (.../mutation/kernels/swap_mutation.cu).
+ */
+int tspb_swap(int32_t* routes, int32_t num_routes, int32_t n, const double* u,
+              double rate, const int32_t* pos1, const int32_t* pos2, void* stream);
+
+/* Operators of the fused and batched generation. */
+#define TSPB_XOVER_PMX 0
+#define TSPB_XOVER_OX 1
+#define TSPB_MUT_INVERSION 0
+#define TSPB_MUT_SWAP 1
+
+/*
  * Inversion mutation in place: row r reversed over [min(p1,p2), max(p1,p2)] when
  * u[r] < rate. Replaces MutationCPUPermInversion.mutate_batch
  *   (src/algorithms/strategies/mutation/inversion_mutation.py:65-99) and
@@ -363,6 +392,8 @@ typedef struct tspb_batch {
   int64_t* ls_stats;        /* optional [I][rows_max][4] passes, pairs, moves, evaluated gains (accumulated) */
   uint8_t* clean[2];        /* optional [I][P] per population: 1 = converged 2-opt local optimum */
   uint8_t* off_clean;       /* [I][P] the same for the offspring (required with clean) */
+  int32_t crossover;        /* TSPB_XOVER_PMX or TSPB_XOVER_OX */
+  int32_t mutation;         /* TSPB_MUT_INVERSION or TSPB_MUT_SWAP */
 } tspb_batch;
 
 /* Fitness of every row of pop[parity]; with set_best also the initial best (first

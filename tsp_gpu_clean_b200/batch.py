@@ -108,6 +108,13 @@ class Bucket:
   queue: Any = None
 
 
+# Operators of the generation: PMX (pmx_crossover.py) or OX (order_crossover.py) with
+# inversion (inversion_mutation.py) or swap (swap_mutation.py) mutation. All four draw the
+# same random numbers, so one tape serves every combination.
+CROSSOVER_CODES = {"pmx": native.TSPB_XOVER_PMX, "ox": native.TSPB_XOVER_OX}
+MUTATION_CODES = {"inversion": native.TSPB_MUT_INVERSION, "swap": native.TSPB_MUT_SWAP}
+
+
 def elite_rows(fitness: np.ndarray, elite: int) -> np.ndarray:
   """Rows of `argsort(fitness)[:elite]` for every row of an (m, P) fitness array.
 
@@ -123,9 +130,15 @@ class FusedBatchSolver:
                local_search: LocalSearchConfig | None = None, elite_count: int = 8, post_init: bool = True,
                max_matrix_dimension: int | None = 4096, use_graph: bool = True,
                tuner: BatchAutotuner | None = None, bucket_bounds: Sequence[int] = DEFAULT_BUCKET_BOUNDS,
-               chunk: int = 16, skip_converged: bool = True, concurrent_buckets: bool = True) -> None:
+               chunk: int = 16, skip_converged: bool = True, concurrent_buckets: bool = True,
+               crossover: str = "pmx", mutation: str = "inversion") -> None:
     if population_size < 2:
       raise ValueError("population_size must be >= 2")
+    if crossover not in CROSSOVER_CODES:
+      raise ValueError(f"crossover must be one of {sorted(CROSSOVER_CODES)}")
+    if mutation not in MUTATION_CODES:
+      raise ValueError(f"mutation must be one of {sorted(MUTATION_CODES)}")
+    self.crossover, self.mutation = crossover, mutation
     self.P = int(population_size)
     self.rate = float(mutation_rate)
     self.kt = int(tournament_k)
@@ -200,6 +213,8 @@ class FusedBatchSolver:
       s.clean[0] = self.clean[0].data_ptr()
       s.clean[1] = self.clean[1].data_ptr()
       s.off_clean = self.off_clean.data_ptr()
+    s.crossover = CROSSOVER_CODES[self.crossover]
+    s.mutation = MUTATION_CODES[self.mutation]
     return s
 
   # ------------------------------------------------------------------------ launches

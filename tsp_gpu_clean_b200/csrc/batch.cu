@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(256) batch_offspring_kernel(const tspb_batch B
   ChildOrigin origin;
   offspring_row(pop_buf(B, parity) + I.pop_offset, fit_buf(B, parity) + (long long)i * P, P, n, kt, sl,
                 B.mutation_rate, ds, row, sm, B.off + I.pop_offset + (long long)row * n,
-                B.off_fit + (long long)i * P + row, clean ? &origin : nullptr);
+                B.off_fit + (long long)i * P + row, clean ? &origin : nullptr, B.crossover, B.mutation);
   if (clean && threadIdx.x == 0)  // a child identical to a converged parent is converged
     B.off_clean[(long long)i * P + row] =
         (origin.same[0] && clean[origin.parent[0]]) || (origin.same[1] && clean[origin.parent[1]]) ? 1 : 0;
@@ -435,6 +435,8 @@ static bool batch_ok(const tspb_batch* b) {
     return false;
   if (b->rows_max < b->P) return false;
   if ((b->clean[0] == nullptr) != (b->clean[1] == nullptr)) return false;
+  if (b->crossover != TSPB_XOVER_PMX && b->crossover != TSPB_XOVER_OX) return false;
+  if (b->mutation != TSPB_MUT_INVERSION && b->mutation != TSPB_MUT_SWAP) return false;
   if (b->num_instances == 0) return true;
   return b->inst && b->pop[0] && b->pop[1] && b->fit[0] && b->fit[1] && b->off && b->off_fit && b->order && b->ctl &&
          b->best_cost && b->best_tour && b->history && b->ls_status;

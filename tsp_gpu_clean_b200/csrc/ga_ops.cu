@@ -2,7 +2,7 @@
 // inversion mutation, stable survival ranking, permutation validation, the EUC_2D
 // matrix and the candidate-distance table. Each kernel states the reference code whose
 // result it reproduces bit for bit.
-#include "common.cuh"
+#include "generation.cuh"
 
 namespace tspb {
 
@@ -161,6 +161,81 @@ __global__ void pmx_kernel(const int32_t* __restrict__ parents, int num_routes, 
   if (tid == 0 && status) status[row] = 0;
 }
 
+// CTA per child, Order Crossover with validated parents (order_crossover.py:52-83).
+// Shared memory: child[n], in_seg, and the seen-bitmaps of p1 and p2.
+__global__ void ox_kernel(const int32_t* __restrict__ parents, int num_routes, int n,
+                          const int32_t* __restrict__ cut_first, const int32_t* __restrict__ cut_second,
+                          int32_t* __restrict__ children, int32_t* __restrict__ status) {
+  extern __shared__ int sm[];
+  const int words = (n + 31) >> 5;
+  int* child = sm;                                                // n
+  unsigned* in_seg = reinterpret_cast<unsigned*>(sm + n);         // words
+  unsigned* seen1 = in_seg + words;                               // words
+  unsigned* seen2 = seen1 + words;                                // words
+  __shared__ int bad;
+  __shared__ int red[32];
+  const int row = blockIdx.x;
+  const int tid = threadIdx.x, T = blockDim.x;
+  const int pairs = num_routes >> 1;
+  int32_t* out = children + (long long)row * n;
+  if (row >= 2 * pairs) {  // odd tail copied unchanged (order_crossover.py:167-168)
+    for (int p = tid; p < n; p += T) out[p] = __ldg(parents + (long long)row * n + p);
+    if (tid == 0 && status) status[row] = 0;
+    return;
+  }
+  const int q = row >> 1, h = row & 1;
+  const int32_t* p1 = parents + (long long)(2 * q + h) * n;
+  const int32_t* p2 = parents + (long long)(2 * q + 1 - h) * n;
+  int c1 = __ldg(cut_first + q), c2 = __ldg(cut_second + q);
+  if (c1 > c2) {
+    const int tmp = c1;
+    c1 = c2;
+    c2 = tmp;
+  }
+  if (tid == 0) bad = (c1 < 0 || c2 >= n) ? 1 : 0;
+  for (int w = tid; w < 3 * words; w += T) in_seg[w] = 0u;
+  __syncthreads();
+  for (int p = tid; p < n; p += T) {
+    const int v1 = __ldg(p1 + p), v2 = __ldg(p2 + p);
+    if ((unsigned)v1 >= (unsigned)n || (unsigned)v2 >= (unsigned)n) {
+      bad = 1;
+      continue;
+    }
+    if (atomicOr(&seen1[v1 >> 5], 1u << (v1 & 31)) & (1u << (v1 & 31))) bad = 1;
+    if (atomicOr(&seen2[v2 >> 5], 1u << (v2 & 31)) & (1u << (v2 & 31))) bad = 1;
+  }
+  __syncthreads();
+  if (bad) {
+    for (int p = tid; p < n; p += T) out[p] = __ldg(p1 + p);
+    if (tid == 0 && status) status[row] = TSPB_ERR_NOT_PERMUTATION;
+    return;
+  }
+  for (int p = c1 + tid; p <= c2; p += T) {
+    const int v1 = __ldg(p1 + p);
+    child[p] = v1;
+    atomicOr(&in_seg[v1 >> 5], 1u << (v1 & 31));
+  }
+  __syncthreads();
+  ox_fill(p2, n, c2, child, in_seg, red);
+  __syncthreads();
+  for (int p = tid; p < n; p += T) out[p] = child[p];
+  if (tid == 0 && status) status[row] = 0;
+}
+
+// Thread per route: exchange of positions p1, p2 when u < rate (swap_mutation.py:94-99).
+__global__ void swap_kernel(int32_t* __restrict__ routes, int num_routes, int n, const double* __restrict__ u,
+                            double rate, const int32_t* __restrict__ pos1, const int32_t* __restrict__ pos2) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= num_routes) return;
+  if (!(__ldg(u + r) < rate)) return;
+  const int a = __ldg(pos1 + r), b = __ldg(pos2 + r);
+  if ((unsigned)a >= (unsigned)n || (unsigned)b >= (unsigned)n) return;
+  int32_t* t = routes + (long long)r * n;
+  const int x = t[a];
+  t[a] = t[b];
+  t[b] = x;
+}
+
 // Warp per route, reversal of [min(p1,p2), max(p1,p2)] when u < rate
 // (inversion_mutation.py:93-97).
 __global__ void inversion_kernel(int32_t* __restrict__ routes, int num_routes, int n, const double* __restrict__ u,
@@ -306,6 +381,31 @@ extern "C" int tspb_pmx(const int32_t* parents, int32_t num_routes, int32_t n, c
   const int threads = n >= 1024 ? 512 : (n >= 256 ? 256 : 128);
   pmx_kernel<<<num_routes, threads, smem, reinterpret_cast<cudaStream_t>(stream)>>>(parents, num_routes, n, cut_first,
                                                                                     cut_second, children, status);
+  return tspb_launch_status();
+}
+
+extern "C" int tspb_ox(const int32_t* parents, int32_t num_routes, int32_t n, const int32_t* cut_first,
+                       const int32_t* cut_second, int32_t* children, int32_t* status, void* stream) {
+  if (num_routes < 0 || n < 0) return TSPB_ERR_ARG;
+  if (num_routes == 0 || n == 0) return TSPB_OK;
+  if (!parents || !children || (num_routes >= 2 && (!cut_first || !cut_second))) return TSPB_ERR_ARG;
+  const size_t smem = (size_t)4 * n + (size_t)3 * ((n + 31) / 32) * 4;
+  if (smem > 200 * 1024) return TSPB_ERR_UNSUPPORTED;
+  if (smem > 48 * 1024) TSPB_CUDA_CHECK(cudaFuncSetAttribute(ox_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int threads = n >= 1024 ? 512 : (n >= 256 ? 256 : 128);
+  ox_kernel<<<num_routes, threads, smem, reinterpret_cast<cudaStream_t>(stream)>>>(parents, num_routes, n, cut_first,
+                                                                                   cut_second, children, status);
+  return tspb_launch_status();
+}
+
+extern "C" int tspb_swap(int32_t* routes, int32_t num_routes, int32_t n, const double* u, double rate,
+                         const int32_t* pos1, const int32_t* pos2, void* stream) {
+  if (num_routes < 0 || n < 0) return TSPB_ERR_ARG;
+  if (num_routes == 0 || n == 0) return TSPB_OK;
+  if (!routes || !u || !pos1 || !pos2) return TSPB_ERR_ARG;
+  const int threads = 128;
+  swap_kernel<<<(num_routes + threads - 1) / threads, threads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+      routes, num_routes, n, u, rate, pos1, pos2);
   return tspb_launch_status();
 }
 

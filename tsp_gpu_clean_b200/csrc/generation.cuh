@@ -43,6 +43,62 @@ __host__ __device__ inline size_t offspring_smem_bytes(int n) {
   return (size_t)8 * n + (size_t)((n + 31) / 32) * 4;
 }
 
+// Exclusive prefix sum of v over the CTA (blockDim a multiple of 32); `red` holds 32 ints.
+__device__ __forceinline__ int block_exclusive_scan(int v, int* red) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (int)(blockDim.x >> 5);
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(FULL, x, o);
+    if (lane >= o) x += y;
+  }
+  __syncthreads();  // red may still be read by a previous scan
+  if (lane == 31) red[wid] = x;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int w = 0; w < nw; ++w) {
+      const int t = red[w];
+      red[w] = acc;
+      acc += t;
+    }
+  }
+  __syncthreads();
+  return red[wid] + x - v;
+}
+
+// Order Crossover fill (order_crossover.py:52-83, open permutations): child[c1..c2]
+// already holds p1's segment, whose genes are marked in `in_seg`. The free positions
+// c2+1, ..., n-1, 0, ..., c1-1 form one run in that rotated order; they take, in order,
+// the genes of p2 read from index c2+1 onward (wrapping) that are not in the segment.
+// Each thread scans a contiguous stretch of the rotated p2; a CTA prefix count of kept
+// genes gives every kept gene its free position. `red` holds 32 ints.
+__device__ __forceinline__ void ox_fill(const int32_t* __restrict__ p2, int n, int c2, int* child,
+                                        const unsigned* in_seg, int* red) {
+  const int T = blockDim.x, tid = threadIdx.x;
+  const int chunk = (n + T - 1) / T;
+  const int t0 = min(tid * chunk, n), t1 = min(t0 + chunk, n);
+  const int base = c2 + 1;  // <= n
+  int cnt = 0;
+  for (int t = t0; t < t1; ++t) {
+    int idx = base + t;
+    if (idx >= n) idx -= n;
+    const int g = __ldg(p2 + idx);
+    cnt += (in_seg[g >> 5] & (1u << (g & 31))) ? 0 : 1;
+  }
+  int m = block_exclusive_scan(cnt, red);
+  for (int t = t0; t < t1; ++t) {
+    int idx = base + t;
+    if (idx >= n) idx -= n;
+    const int g = __ldg(p2 + idx);
+    if (in_seg[g >> 5] & (1u << (g & 31))) continue;
+    int dst = base + m;
+    if (dst >= n) dst -= n;
+    child[dst] = g;
+    ++m;
+  }
+}
+
 // Parents of a child and whether the child equals each of them (filled when requested).
 struct ChildOrigin {
   int parent[2];
@@ -50,19 +106,23 @@ struct ChildOrigin {
 };
 
 // Child `row` of one generation with the whole CTA: tournament winners (row pairs 2q, 2q+1
-// share PMX cuts q; an odd last row copies its winner), PMX, inversion when u < rate, then
-// the row and its closed-tour length are written to off_row / off_fit_row. `sm` holds
-// offspring_smem_bytes(n) bytes. With `origin`, every thread also learns the parents and
-// whether the child is identical to each.
+// share the cuts q; an odd last row copies its winner), crossover (PMX or OX), mutation
+// when u < rate (inversion or swap), then the row and its closed-tour length are written to
+// off_row / off_fit_row. `sm` holds offspring_smem_bytes(n) bytes. With `origin`, every
+// thread also learns the parents and whether the child is identical to each. OX and swap
+// draw exactly the numbers PMX and inversion draw (order_crossover.py:148-150,
+// swap_mutation.py:86-93), so the tape is the same for every operator choice.
 __device__ __forceinline__ void offspring_row(const int32_t* __restrict__ pop, const double* __restrict__ fit, int P,
                                               int n, int kt, const GenTapeSlice& tape, double rate, const DistSrc& ds,
                                               int row, int* sm, int32_t* __restrict__ off_row,
-                                              double* __restrict__ off_fit_row, ChildOrigin* origin = nullptr) {
+                                              double* __restrict__ off_fit_row, ChildOrigin* origin = nullptr,
+                                              int crossover = TSPB_XOVER_PMX, int mutation = TSPB_MUT_INVERSION) {
   int* inv_p2 = sm;
   int* child = sm + n;
   unsigned* in_seg = reinterpret_cast<unsigned*>(sm + 2 * n);
   __shared__ int w[2];
   __shared__ long long red[32];
+  __shared__ int scan_red[32];
   const int tid = threadIdx.x, T = blockDim.x;
   const int pairs = P >> 1;
   const int q = row >> 1, h = row & 1;
@@ -76,6 +136,23 @@ __device__ __forceinline__ void offspring_row(const int32_t* __restrict__ pop, c
   const int32_t* p2 = pop + (long long)w[1] * n;
   if (!paired || n < 2) {
     for (int p = tid; p < n; p += T) child[p] = __ldg(p1 + p);
+  } else if (crossover == TSPB_XOVER_OX) {
+    int c1 = tape.cut_a[q], c2 = tape.cut_b[q];
+    if (c1 > c2) {
+      const int tmp = c1;
+      c1 = c2;
+      c2 = tmp;
+    }
+    const int words = (n + 31) >> 5;
+    for (int wd = tid; wd < words; wd += T) in_seg[wd] = 0u;
+    __syncthreads();
+    for (int p = c1 + tid; p <= c2; p += T) {
+      const int v1 = __ldg(p1 + p);
+      child[p] = v1;
+      atomicOr(&in_seg[v1 >> 5], 1u << (v1 & 31));
+    }
+    __syncthreads();
+    ox_fill(p2, n, c2, child, in_seg, scan_red);
   } else {
     int c1 = tape.cut_a[q], c2 = tape.cut_b[q];
     if (c1 > c2) {
@@ -112,11 +189,17 @@ __device__ __forceinline__ void offspring_row(const int32_t* __restrict__ pop, c
       if (child[p] == -1) child[p] = __ldg(p2 + p);
   }
   __syncthreads();
-  // inversion mutation of this child
+  // mutation of this child
   if (tape.u[row] < rate) {
     const int a = tape.inv_a[row], b = tape.inv_b[row];
     const int lo = a < b ? a : b, hi = a < b ? b : a;
-    if (lo >= 0 && hi < n) {
+    if (mutation == TSPB_MUT_SWAP) {
+      if (tid == 0 && lo >= 0 && hi < n) {
+        const int x = child[a];
+        child[a] = child[b];
+        child[b] = x;
+      }
+    } else if (lo >= 0 && hi < n) {
       const int half = (hi - lo + 1) >> 1;
       for (int t = tid; t < half; t += T) {
         const int x = child[lo + t], y = child[hi - t];

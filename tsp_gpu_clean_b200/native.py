@@ -51,6 +51,8 @@ SIGNATURES: dict[str, tuple] = {
   "tspb_pmx": (ctypes.c_int, [_p, _i32, _i32, _p, _p, _p, _p, _p]),
   "tspb_scatter_rows": (ctypes.c_int, [_p, _i32, _i32, _p, _p, _i32, _p]),
   "tspb_inversion": (ctypes.c_int, [_p, _i32, _i32, _p, _f64, _p, _p, _p]),
+  "tspb_ox": (ctypes.c_int, [_p, _i32, _i32, _p, _p, _p, _p, _p]),
+  "tspb_swap": (ctypes.c_int, [_p, _i32, _i32, _p, _f64, _p, _p, _p]),
   "tspb_stable_rank": (ctypes.c_int, [_p, _i32, _i32, _p, _p]),
   "tspb_validate_perm": (ctypes.c_int, [_p, _i32, _i32, _p, _p]),
   "tspb_euc2d_matrix": (ctypes.c_int, [_p, _i32, _p, _i64, _p]),
@@ -88,6 +90,10 @@ TSPB_BATCH_DONE = 4
 TSPB_BATCH_PHASE_POSTINIT = 0
 TSPB_BATCH_PHASE_RESUME = 1
 TSPB_BATCH_PHASE_RUN = 2
+TSPB_XOVER_PMX = 0
+TSPB_XOVER_OX = 1
+TSPB_MUT_INVERSION = 0
+TSPB_MUT_SWAP = 1
 TSPB_BATCH_COORDS = 1
 TSPB_BATCH_GROUPED = 2
 
@@ -135,7 +141,7 @@ class BatchState(ctypes.Structure):
               ("order", _p), ("tape_tourn", _p), ("tape_cut_a", _p), ("tape_cut_b", _p), ("tape_u", _p),
               ("tape_inv_a", _p), ("tape_inv_b", _p), ("ctl", _p), ("best_cost", _p), ("best_tour", _p),
               ("history", _p), ("ties", _p), ("host_elites", _p), ("ls_status", _p), ("ls_stats", _p),
-              ("clean", _p * 2), ("off_clean", _p)]
+              ("clean", _p * 2), ("off_clean", _p), ("crossover", _i32), ("mutation", _i32)]
 
 _lock = threading.Lock()
 _lib = None

@@ -5,18 +5,22 @@ from __future__ import annotations
 from .initialization import InitializationB200TourNearestNeighbor
 from .local_search import LocalSearchB200TourTwoOpt
 from .operators import (
+  CrossoverB200PermOrder,
   CrossoverB200PermPartiallyMapped,
   EvaluationB200Cost,
   MutationB200PermInversion,
+  MutationB200PermSwap,
   SelectionB200Tournament,
 )
 
 STRATEGY_REGISTRY: dict[str, type] = {
+  "CrossoverB200PermOrder": CrossoverB200PermOrder,
   "CrossoverB200PermPartiallyMapped": CrossoverB200PermPartiallyMapped,
   "EvaluationB200Cost": EvaluationB200Cost,
   "InitializationB200TourNearestNeighbor": InitializationB200TourNearestNeighbor,
   "LocalSearchB200TourTwoOpt": LocalSearchB200TourTwoOpt,
   "MutationB200PermInversion": MutationB200PermInversion,
+  "MutationB200PermSwap": MutationB200PermSwap,
   "SelectionB200Tournament": SelectionB200Tournament,
 }
 
@@ -46,11 +50,13 @@ def register_strategy(name: str, strategy_cls: type, *, overwrite: bool = False)
 
 __all__ = [
   "STRATEGY_REGISTRY",
+  "CrossoverB200PermOrder",
   "CrossoverB200PermPartiallyMapped",
   "EvaluationB200Cost",
   "InitializationB200TourNearestNeighbor",
   "LocalSearchB200TourTwoOpt",
   "MutationB200PermInversion",
+  "MutationB200PermSwap",
   "SelectionB200Tournament",
   "register_strategy",
 ]

@@ -8,6 +8,8 @@ produces bit-identical results for the same inputs and the same random draws:
 - `SelectionB200Tournament` <- `SelectionCPUTournament` (`tournament_selection.py:29-128`)
 - `CrossoverB200PermPartiallyMapped` <- `CrossoverCPUPermPartiallyMapped` (`pmx_crossover.py:36-171`)
 - `MutationB200PermInversion` <- `MutationCPUPermInversion` (`inversion_mutation.py:36-99`)
+- `CrossoverB200PermOrder`  <- `CrossoverCPUPermOrder` (`order_crossover.py:36-168`)
+- `MutationB200PermSwap`    <- `MutationCPUPermSwap` (`swap_mutation.py:36-99`)
 
 Random draws are taken on the host from `context.rng` (falling back to the strategy's
 own generator) with the same calls, shapes and order as the reference, then uploaded;
@@ -141,6 +143,8 @@ class SelectionB200Tournament(StrategyBase):
 class CrossoverB200PermPartiallyMapped(StrategyBase):
   """PMX on pairs (2q, 2q+1) sharing cut points; the odd tail row is copied."""
 
+  _entry = "tspb_pmx"
+
   def __init__(self, seed: Any = None) -> None:
     super().__init__(seed)
 
@@ -158,7 +162,7 @@ class CrossoverB200PermPartiallyMapped(StrategyBase):
     if high - low < 2:
       return p1.copy()
     if (low, high) != (0, n):
-      raise NotImplementedError("CrossoverB200PermPartiallyMapped covers open permutations only")
+      raise NotImplementedError(f"{type(self).__name__} covers open permutations only")
     cuts = sample_distinct_pairs(rng, 1, low, high)
     pair = np.stack([p1, p2])
     out = self._pmx_device(pair, cuts)
@@ -171,7 +175,7 @@ class CrossoverB200PermPartiallyMapped(StrategyBase):
     second = device_tensor(np.ascontiguousarray(pairs[:, 1]), torch.int32)
     out = torch.empty_like(d_in)
     status = torch.empty(num, dtype=torch.int32, device="cuda")
-    native.call("tspb_pmx", ptr(d_in), num, n, ptr(first), ptr(second), ptr(out), ptr(status), stream_handle())
+    native.call(self._entry, ptr(d_in), num, n, ptr(first), ptr(second), ptr(out), ptr(status), stream_handle())
     self.kernel_launches += 1
     if int(status.max().item()) != 0:
       raise NotPermutationError("crossover_batch: a parent is not a permutation of 0..n-1")
@@ -193,7 +197,7 @@ class CrossoverB200PermPartiallyMapped(StrategyBase):
     if n <= 1 or high - low < 2:
       return batch.clone() if is_device_array(batch) else np.array(batch, dtype=np.int32)
     if (low, high) != (0, n):
-      raise NotImplementedError("CrossoverB200PermPartiallyMapped covers open permutations only")
+      raise NotImplementedError(f"{type(self).__name__} covers open permutations only")
     rng = resolve_rng(context, self.rng)
     pairs = sample_distinct_pairs(rng, num // 2, low, high)
     if num // 2 == 0:
@@ -203,8 +207,24 @@ class CrossoverB200PermPartiallyMapped(StrategyBase):
     return self._pmx_device(batch, pairs)
 
 
+class CrossoverB200PermOrder(CrossoverB200PermPartiallyMapped):
+  """Order Crossover on pairs (2q, 2q+1) sharing cut points; the odd tail row is copied.
+
+  The child keeps `p1[c1..c2]`; positions `c2+1, ..., n-1, 0, ..., c1-1` take the genes of
+  `p2` not in that segment, in the order met reading `p2` from `c2+1` with wrap-around
+  (`CrossoverCPUPermOrder._apply_ox`, `order_crossover.py:52-83`). Draws are those of the
+  reference: one `sample_distinct_pairs(rng, N // 2, low, high)` per batch
+  (`order_crossover.py:148-150`), one pair per single `crossover` call. Depot-bounded
+  (closed) tours raise NotImplementedError.
+  """
+
+  _entry = "tspb_ox"
+
+
 class MutationB200PermInversion(StrategyBase):
   """Reverse `[min(p1,p2), max(p1,p2)]` of every row whose `u < mutation_rate`."""
+
+  _entry = "tspb_inversion"
 
   def __init__(self, seed: Any = None, candidate_k: int | None = None) -> None:
     super().__init__(seed)
@@ -237,7 +257,7 @@ class MutationB200PermInversion(StrategyBase):
     u = device_tensor(probs, torch.float64)
     d1 = device_tensor(pos1.astype(np.int32), torch.int32)
     d2 = device_tensor(pos2.astype(np.int32), torch.int32)
-    native.call("tspb_inversion", ptr(d_routes), num, n, ptr(u), float(mutation_rate), ptr(d1), ptr(d2), stream_handle())
+    native.call(self._entry, ptr(d_routes), num, n, ptr(u), float(mutation_rate), ptr(d1), ptr(d2), stream_handle())
     self.kernel_launches += 1
     if on_dev:
       return restore_shape(d_routes, was_1d)
@@ -258,6 +278,17 @@ class MutationB200PermInversion(StrategyBase):
       pos1[i] = first
       pos2[i] = _proximity_index(row, first, low, high, cand, rng)
     return pos1, pos2
+
+
+class MutationB200PermSwap(MutationB200PermInversion):
+  """Exchange positions `pos1`, `pos2` of every row whose `u < mutation_rate`.
+
+  Draws follow `MutationCPUPermSwap.mutate_batch` (`swap_mutation.py:65-99`): `rng.random(N)`,
+  then the positions of `sample_mutation_positions` (`route_helpers.py:183-231`), uniform
+  distinct pairs or, with `candidate_k`, a k-NN neighbour's position for the second one.
+  """
+
+  _entry = "tspb_swap"
 
 
 def _proximity_index(route, anchor, low, high, cand, rng) -> int:
