@@ -255,6 +255,21 @@ int tspb_nn_init_jobs(const tspb_nn_job* jobs, int32_t num_jobs, int32_t max_row
                       const int64_t* ws_offsets, void* stream);
 
 /*
+ * Uniform random-permutation initial population, CTA per row: row r is `customers`
+ * (n entries; NULL means 0..n-1) shuffled by Fisher-Yates from position n-1 down to 1,
+ * position i swapped with the SplitMix64 bounded draw in [0, i] of the stream seeded with
+ * seeds[r]. Replaces InitializationCPUPermRandom.initialize
+ *   (src/algorithms/strategies/initialization/random_init.py:30-55) and random_init_kernel
+ *   (.../initialization/kernels/random_init.cu).
+ */
+int tspb_random_init(const uint64_t* seeds, int32_t rows, int32_t n, const int32_t* customers, int32_t* out,
+                     void* stream);
+/* The same for many instances in one launch (customers 0..n-1 of each job; the jobs'
+ * `k` and `cand` are ignored); max_n and max_rows bound every job's n and rows. */
+int tspb_random_init_jobs(const tspb_nn_job* jobs, int32_t num_jobs, int32_t max_rows, int32_t max_n,
+                          void* stream);
+
+/*
  * The GA's random tape drawn exactly as NumPy's Generator(PCG64) draws it from
  * `context.rng` (src/utils/rng.py:48-64), in the reference's per-generation order:
  * tournament integers(0, P, (P, kt)) (tournament_selection.py:113), PMX cut pairs
@@ -338,7 +353,11 @@ int tspb_generation_track(const double* fit, const int32_t* pop, int32_t P, int3
  *
  * Phases of the 2-opt, cost and tracking steps: POSTINIT (every row of parity 0, no gate;
  * the post-init refinement), RESUME (runs in state RESUME, rows host_elites[i]), RUN (runs
- * in state RUN, rows [0, elite)).
+ * in state RUN, rows [0, elite)), OFFSPRING (runs in state RUN, every offspring row of
+ * `off`: the 2-opt of LocalSearchStep(target="offspring") that the reference's
+ * local_search_stage="post_mutation" places between mutation and evaluation,
+ * genetic_algorithm.py:254-277, 333-343; with `clean`, a converged child is skipped and
+ * off_clean records the refinement's convergence).
  */
 #define TSPB_BATCH_RUN 0
 #define TSPB_BATCH_STOPPED 1
@@ -349,6 +368,7 @@ int tspb_generation_track(const double* fit, const int32_t* pop, int32_t P, int3
 #define TSPB_BATCH_PHASE_POSTINIT 0
 #define TSPB_BATCH_PHASE_RESUME 1
 #define TSPB_BATCH_PHASE_RUN 2
+#define TSPB_BATCH_PHASE_OFFSPRING 3
 
 typedef struct tspb_batch_instance {
   int32_t n;                    /* cities, >= 4 */
@@ -422,7 +442,7 @@ int tspb_batch_two_opt(const tspb_batch* b, const int32_t* items, int32_t num_it
                        int32_t ctas, uint32_t* queue, void* stream);
 /* Resident CTAs per SM of tspb_batch_two_opt for this shape (0: does not fit). */
 int tspb_batch_two_opt_occupancy(int32_t max_n, int32_t mode, int32_t threads);
-/* Fitness of the refined rows of a phase (RESUME or RUN). */
+/* Fitness of the refined rows of a phase (RESUME, RUN, or OFFSPRING into off_fit). */
 int tspb_batch_elite_cost(const tspb_batch* b, int32_t phase, void* stream);
 /* Best tracking, history, patience and the generation counter of a phase's instances:
  * RUN/RESUME -> RUN, STOPPED or DONE (genetic_algorithm.py:876-910). */

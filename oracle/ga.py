@@ -45,6 +45,7 @@ class GAConfig:
   periodic: tuple[int, str] | None = None  # (interval, target)
   crossover: str = "pmx"  # "pmx" (CrossoverCPUPermPartiallyMapped) or "ox" (CrossoverCPUPermOrder)
   mutation: str = "inversion"  # "inversion" (MutationCPUPermInversion) or "swap" (MutationCPUPermSwap)
+  init: str = "nn"  # "nn" (InitializationCPUTourNearestNeighbor) or "random" (InitializationCPUPermRandom)
 
 
 def routes_digest(routes: np.ndarray) -> str:
@@ -105,7 +106,10 @@ class OracleGA:
     if patience is None:
       patience = int(2 * math.sqrt(n))
     customers = np.arange(n, dtype=np.int32)
-    pop = ga_ops.nn_init(rng, customers, cfg.population_size, self.cand_provider(cfg.nn_k))
+    if cfg.init == "random":
+      pop = ga_ops.random_init(rng, customers, cfg.population_size)
+    else:
+      pop = ga_ops.nn_init(rng, customers, cfg.population_size, self.cand_provider(cfg.nn_k))
     fit = self._cost(pop)
     best_idx = int(np.argmin(fit))
     best_cost = float(fit[best_idx])

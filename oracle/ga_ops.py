@@ -314,6 +314,33 @@ def nn_row(customers: np.ndarray, cand: np.ndarray, seed: int) -> np.ndarray:
   return out
 
 
+def random_init(rng, customers, population_size: int) -> np.ndarray:
+  """`InitializationCPUPermRandom.initialize` (`random_init.py:30-55`): row seeds as for the
+  nearest-neighbour init, then per row a Fisher-Yates shuffle of `customers` from the
+  last position down to 1, position i swapped with a SplitMix64 draw in [0, i]. The
+  SplitMix64 state advances by its constant increment each step, so step t of a row uses
+  state seed + t * increment; all rows advance together here."""
+  cust = np.asarray(customers, dtype=np.int32)
+  seeds = draw_row_seeds(rng, population_size)
+  n = cust.size
+  pop = np.tile(cust, (population_size, 1)).astype(np.int32)
+  if population_size == 0 or n == 0:
+    return pop.reshape(population_size, n)
+  rows = np.arange(population_size)
+  state = seeds.astype(np.uint64)
+  with np.errstate(over="ignore"):
+    for i in range(n - 1, 0, -1):
+      state = state + np.uint64(0x9E3779B97F4A7C15)
+      z = (state ^ (state >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+      z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+      z = z ^ (z >> np.uint64(31))
+      j = (((z >> np.uint64(32)) * np.uint64(i + 1)) >> np.uint64(32)).astype(np.intp)
+      a = pop[:, i].copy()
+      pop[:, i] = pop[rows, j]
+      pop[rows, j] = a
+  return pop
+
+
 def nn_init(rng, customers, population_size: int, cand: np.ndarray) -> np.ndarray:
   """`InitializationCPUTourNearestNeighbor.initialize` (`nearest_neighbor_init.py:109-132`)."""
   cust = np.asarray(customers, dtype=np.int32)

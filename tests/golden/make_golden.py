@@ -17,6 +17,9 @@ Outputs (NumPy `.npz`, committed next to this script):
                        local optimum in best and first mode, with pass and pair counts;
 - `ox_swap.npz`        Order Crossover and swap mutation batches, and two GA runs with them
                        (`python make_golden.py <reference root> ox` regenerates only this file)
+- `stage.npz`          random-permutation populations, and GA runs with 2-opt on every
+                       offspring (`post_mutation`), two in the Chapter-4 configuration
+                       (`... stage` regenerates only this file)
 - `ops.npz`            tournament selection, PMX, inversion, tour cost, candidate
                        lists and the EUC_2D matrix on seeded inputs;
 - `ga.npz`             full GA runs (the 100-city memetic run for 50 generations, a
@@ -368,6 +371,86 @@ def main_ox_swap(ref_root: str) -> None:
   np.savez_compressed(os.path.join(HERE, "ox_swap.npz"), **out)
 
 
+def main_stage(ref_root: str) -> None:
+  """`stage.npz`: the reference's random-permutation initialisation, and GA runs with
+  2-opt on every offspring (`local_search_stage="post_mutation"`), the configuration of
+  the reference's published Chapter-4 benchmarks (random init, tournament 5, OX, swap,
+  2-opt k=20 x10), plus one run mixing the stage with PMX, inversion, NN init and the
+  post-init and elite steps."""
+  _setup(ref_root)
+  from algorithms import GeneticAlgorithm
+  from algorithms.pipeline_steps import EliteOnlyLocalSearchStep, PostInitLocalSearchStep
+  from algorithms.strategies import (
+    CrossoverCPUPermOrder,
+    CrossoverCPUPermPartiallyMapped,
+    EvaluationCPUCost,
+    InitializationCPUPermRandom,
+    InitializationCPUTourNearestNeighbor,
+    LocalSearchCPUTourTwoOpt,
+    MutationCPUPermInversion,
+    MutationCPUPermSwap,
+    SelectionCPUTournament,
+  )
+  from data_models.problem import Problem
+  from protocols.problem_context import ProblemContext
+
+  from tsp_gpu_clean_b200 import instances
+
+  def coord_problem(coords):
+    return Problem(name="synthetic", dimension=len(coords), problem_type="TSP", edge_type="EUC_2D",
+                   coordinates=np.asarray(coords, dtype=np.float64), distances=None)
+
+  out: dict[str, np.ndarray] = {}
+  for tag, n, pop_size in (("r1", 1, 3), ("r2", 2, 4), ("r3", 7, 9), ("r4", 100, 64), ("r5", 1002, 256)):
+    coords = instances.uniform_instance(n, 900 + n)
+    ctx = ProblemContext(coord_problem(coords), xp=np, seed=41 + n)
+    customers = list(range(n)) if tag != "r3" else [3 * c + 5 for c in range(n)]
+    pop = InitializationCPUPermRandom(seed=1).initialize(customers, pop_size, ctx)
+    out[f"{tag}_meta"] = np.array([n, pop_size, 41 + n])
+    out[f"{tag}_customers"] = np.asarray(customers, dtype=np.int32)
+    pop = np.ascontiguousarray(pop, dtype=np.int32)
+    if pop.size > 50_000:  # large populations are pinned by their digest
+      out[f"{tag}_digest"] = np.frombuffer(hashlib.sha256(pop.tobytes()).digest(), dtype=np.uint8)
+    else:
+      out[f"{tag}_pop"] = pop
+    out[f"{tag}_rng_state"] = np.array([ctx.rng.bit_generator.state["state"]["state"] % (1 << 63)], dtype=np.int64)
+
+  def run_ga(tag, coords, pop_size, gens, mutation_rate, patience, chapter4=True, elite=0, post_init=False):
+    t = time.time()
+    ctx = ProblemContext(coord_problem(coords), xp=np, seed=42)
+    ls = LocalSearchCPUTourTwoOpt(mode="best", max_iterations=10, candidate_k=20)
+    ev = EvaluationCPUCost()
+    steps = []
+    if post_init:
+      steps.append(PostInitLocalSearchStep(local_search=ls, evaluation=ev))
+    if elite:
+      steps.append(EliteOnlyLocalSearchStep(local_search=ls, evaluation=ev, elite_count=elite))
+    if chapter4:
+      init, xo, mut = InitializationCPUPermRandom(seed=42), CrossoverCPUPermOrder(seed=42), MutationCPUPermSwap(seed=42)
+    else:
+      init = InitializationCPUTourNearestNeighbor(k=5, seed=42)
+      xo, mut = CrossoverCPUPermPartiallyMapped(seed=42), MutationCPUPermInversion(seed=42)
+    ga = GeneticAlgorithm(population_size=pop_size, mutation_rate=mutation_rate, seed=42, initialization=init,
+                          selection=SelectionCPUTournament(k=5, seed=42), crossover=xo, mutation=mut,
+                          local_search=ls, evaluation=ev, local_search_stage="post_mutation",
+                          pipeline=steps or None)
+    best, stats = ga.evolve(context=ctx, customers=list(range(len(coords))), max_generations=gens, patience=patience)
+    out[f"ga_{tag}_coords"] = coords
+    out[f"ga_{tag}_meta"] = np.array([pop_size, gens, elite, int(post_init), -1 if patience is None else patience,
+                                      int(chapter4)])
+    out[f"ga_{tag}_rate"] = np.array(mutation_rate)
+    out[f"ga_{tag}_best"] = np.asarray(best, dtype=np.int32)
+    out[f"ga_{tag}_history"] = np.asarray(stats["convergence_history"], dtype=np.float64)
+    out[f"ga_{tag}_gens"] = np.array(stats["generations_completed"])
+    out[f"ga_{tag}_rng"] = np.array([ctx.rng.bit_generator.state["state"]["state"] % (1 << 63)], dtype=np.int64)
+    print(f"ga {tag}: {time.time() - t:.1f}s best={stats['best_fitness']} gens={stats['generations_completed']}")
+
+  run_ga("s1", instances.uniform_instance(100, 91), 64, 30, 0.02, 10**9)
+  run_ga("s2", instances.clustered_instance(200, 8, 30.0, 92), 32, 25, 0.3, None)
+  run_ga("s3", instances.uniform_instance(150, 93), 48, 20, 0.1, 10**9, chapter4=False, elite=6, post_init=True)
+  np.savez_compressed(os.path.join(HERE, "stage.npz"), **out)
+
+
 if __name__ == "__main__":
   root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
   part = sys.argv[2] if len(sys.argv) > 2 else "all"
@@ -375,3 +458,5 @@ if __name__ == "__main__":
     main(root)
   if part in ("all", "ox"):
     main_ox_swap(root)
+  if part in ("all", "stage"):
+    main_stage(root)

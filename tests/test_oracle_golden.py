@@ -165,3 +165,50 @@ def test_oracle_ga_with_ox_and_swap_matches_reference(golden, tag):
   assert np.array_equal(np.asarray(stats["convergence_history"]), g[f"ga_{tag}_history"])
   assert np.array_equal(best, g[f"ga_{tag}_best"])
   assert rng.bit_generator.state["state"]["state"] % (1 << 63) == int(g[f"ga_{tag}_rng"][0])
+
+
+@pytest.mark.parametrize("tag", ["r1", "r2", "r3", "r4", "r5"])
+def test_random_init_matches_reference(golden, tag):
+  import hashlib
+
+  g = golden("stage.npz")
+  n, pop_size, seed = (int(v) for v in g[f"{tag}_meta"])
+  rng = np.random.default_rng(seed)
+  pop = ga_ops.random_init(rng, g[f"{tag}_customers"], pop_size)
+  if f"{tag}_pop" in g:
+    assert np.array_equal(pop, g[f"{tag}_pop"])
+  else:
+    assert hashlib.sha256(np.ascontiguousarray(pop, dtype=np.int32).tobytes()).digest() == g[f"{tag}_digest"].tobytes()
+  assert rng.bit_generator.state["state"]["state"] % (1 << 63) == int(g[f"{tag}_rng_state"][0])
+
+
+def stage_config(g, tag):
+  """GAConfig of a `stage.npz` run: 2-opt on every offspring, in the Chapter-4 configuration
+  (random init, OX, swap) or with NN init, PMX, inversion and the post-init/elite steps."""
+  pop_size, gens, elite, post_init, patience, chapter4 = (int(v) for v in g[f"ga_{tag}_meta"])
+  cfg = ga.GAConfig(population_size=pop_size, mutation_rate=float(g[f"ga_{tag}_rate"]), nn_k=5, tournament_k=5,
+                    local_search=ga.LocalSearchSpec("best", 10, 20), local_search_stage="post_mutation",
+                    post_init=bool(post_init), elite_count=elite or None,
+                    crossover="ox" if chapter4 else "pmx", mutation="swap" if chapter4 else "inversion",
+                    init="random" if chapter4 else "nn")
+  return cfg, gens, (None if patience < 0 else patience)
+
+
+@pytest.mark.parametrize("tag", ["s1", "s2", "s3"])
+def test_oracle_ga_with_post_mutation_stage_matches_reference(golden, tag):
+  g = golden("stage.npz")
+  coords = g[f"ga_{tag}_coords"]
+  cfg, gens, patience = stage_config(g, tag)
+  cache = {}
+
+  def provider(k):
+    if k not in cache:
+      cache[k] = distances.candidate_list(k, coords=coords)
+    return cache[k]
+
+  rng = np.random.default_rng(42)
+  best, _, _, stats, _ = ga.OracleGA(distances.euc2d_matrix(coords), provider, cfg, rng).evolve(gens, patience=patience)
+  assert stats["generations_completed"] == int(g[f"ga_{tag}_gens"])
+  assert np.array_equal(np.asarray(stats["convergence_history"]), g[f"ga_{tag}_history"])
+  assert np.array_equal(best, g[f"ga_{tag}_best"])
+  assert rng.bit_generator.state["state"]["state"] % (1 << 63) == int(g[f"ga_{tag}_rng"][0])

@@ -131,9 +131,15 @@ class FusedBatchSolver:
                max_matrix_dimension: int | None = 4096, use_graph: bool = True,
                tuner: BatchAutotuner | None = None, bucket_bounds: Sequence[int] = DEFAULT_BUCKET_BOUNDS,
                chunk: int = 16, skip_converged: bool = True, concurrent_buckets: bool = True,
-               crossover: str = "pmx", mutation: str = "inversion") -> None:
+               crossover: str = "pmx", mutation: str = "inversion", init: str = "nn",
+               local_search_stage: str = "none") -> None:
     if population_size < 2:
       raise ValueError("population_size must be >= 2")
+    if init not in ("nn", "random"):
+      raise ValueError("init must be 'nn' (nearest neighbour) or 'random' (uniform permutations)")
+    if local_search_stage not in ("none", "post_mutation"):
+      raise ValueError("local_search_stage must be 'none' or 'post_mutation'")
+    self.init, self.stage = init, local_search_stage
     if crossover not in CROSSOVER_CODES:
       raise ValueError(f"crossover must be one of {sorted(CROSSOVER_CODES)}")
     if mutation not in MUTATION_CODES:
@@ -256,18 +262,36 @@ class FusedBatchSolver:
     for s in self._side[: len(self.buckets)]:
       main.wait_stream(s)
 
+  @property
+  def _post_mutation(self) -> bool:
+    return self.stage == "post_mutation"
+
+  @property
+  def _ls_rows(self) -> int:
+    """Rows per instance of the generation's main 2-opt phase (the tuner's work shape)."""
+    return self.P if self._post_mutation else self.elite
+
   def _generation(self) -> None:
     """Enqueue one replay: finish RESUME runs, then one generation of every RUN run."""
     lib = native.load_library()
     st = ctypes.byref(self.state)
     sh = stream_handle()
-    R, U = native.TSPB_BATCH_PHASE_RESUME, native.TSPB_BATCH_PHASE_RUN
+    R, U, O = native.TSPB_BATCH_PHASE_RESUME, native.TSPB_BATCH_PHASE_RUN, native.TSPB_BATCH_PHASE_OFFSPRING
     if self.elite:
       self._per_bucket(lambda b: self._two_opt(st, b, R))
       native.check("tspb_batch_elite_cost", lib.tspb_batch_elite_cost(st, R, sh))
       native.check("tspb_batch_track", lib.tspb_batch_track(st, R, sh))
       self.kernel_launches += 2
-    self._per_bucket(lambda b: self._offspring(st, b))
+
+    def children(b: Bucket) -> None:
+      self._offspring(st, b)
+      if self._post_mutation:  # LocalSearchStep(target="offspring") before evaluation
+        self._two_opt(st, b, O)
+
+    self._per_bucket(children)
+    if self._post_mutation:
+      native.check("tspb_batch_elite_cost", lib.tspb_batch_elite_cost(st, O, sh))
+      self.kernel_launches += 1
     native.check("tspb_batch_survival", lib.tspb_batch_survival(st, sh))
     self.kernel_launches += 3
     if self.elite:
@@ -282,6 +306,8 @@ class FusedBatchSolver:
     per = nb + 3 + 1  # offspring per bucket, survival (3 kernels), track
     if self.elite:
       per += 2 * nb + 3  # two 2-opt phases per bucket, resume cost + track, run cost
+    if self._post_mutation:
+      per += nb + 1  # offspring 2-opt per bucket, offspring cost
     return per
 
   # ------------------------------------------------------------------------ autotuning
@@ -290,8 +316,8 @@ class FusedBatchSolver:
     lib = native.load_library()
     name = torch.cuda.get_device_name()
     for b in self.buckets:
-      if self.elite:
-        units = len(b.items) * self.elite
+      if self._ls_rows:
+        units = len(b.items) * self._ls_rows
         key = self.tuner.key(name, "two_opt", mode=self.ls.mode, k=self.k, iters=int(self.ls.max_iterations),
                              lo=b.lo, hi=b.hi, coords=b.coords, rebuild=b.can_rebuild, units=units)
         threads = [t for t in TWO_OPT_THREADS if lib.tspb_batch_two_opt_occupancy(b.max_n, self._mode, t) > 0]
@@ -332,10 +358,11 @@ class FusedBatchSolver:
     b.coords = True
 
   def _probe_two_opt(self, b: Bucket, threads: int, rebuild: bool = False) -> float:
-    """Elite-shaped 2-opt work of one bucket on scratch copies of the initial tours: the
-    first `elite` rows of every instance, refined for up to max_iterations passes, with
-    the bucket's matrices or (rebuild) distances rebuilt from coordinates."""
-    e = max(self.elite, 2)  # the probe batch needs P >= 2
+    """The generation's 2-opt work shape for one bucket on scratch copies of the initial
+    tours: the first `elite` rows of every instance (every row with the post_mutation
+    stage), refined for up to max_iterations passes, with the bucket's matrices or
+    (rebuild) distances rebuilt from coordinates."""
+    e = max(self._ls_rows, 2)  # the probe batch needs P >= 2
     ns = self.ns
     offs = np.zeros(self.I, dtype=np.int64)
     offs[1:] = np.cumsum([e * n for n in ns])[:-1]
@@ -460,6 +487,22 @@ class FusedBatchSolver:
     torch.cuda.current_stream().synchronize()  # the host buffers above are released on return
     self.kernel_launches += 1
 
+  def _random_init(self, h_jobs, seeds_all: np.ndarray, ns: list[int]) -> None:
+    """Uniform random-permutation populations of every instance in one launch
+    (`tspb_random_init_jobs`, each row as `InitializationCPUPermRandom` builds it)."""
+    P = self.P
+    d_seeds = torch.from_numpy(seeds_all.view(np.int64)).cuda()
+    for i, n in enumerate(ns):
+      job = h_jobs[i]
+      job.n, job.k, job.rows = n, 0, P
+      job.cand = None
+      job.seeds = d_seeds.data_ptr() + i * P * 8
+      job.out = self.pop[0].data_ptr() + self.pop_offsets[i] * 4
+    d_jobs = torch.frombuffer(bytearray(h_jobs), dtype=torch.uint8).cuda()
+    native.call("tspb_random_init_jobs", ptr(d_jobs), self.I, P, max(ns), stream_handle())
+    torch.cuda.current_stream().synchronize()  # the host buffers above are released on return
+    self.kernel_launches += 1
+
   # ------------------------------------------------------------------------ evolve
   def evolve(self, contexts: Sequence[Any], max_generations: int, patience: Any = None):
     """Run every context's GA; returns a list of (best_tour, stats) in context order.
@@ -513,8 +556,9 @@ class FusedBatchSolver:
     rebuildable = []
     t_ops = t_tape = 0.0
     for i, (ctx, n, rng) in enumerate(zip(contexts, ns, rngs)):
-      seeds_all[i] = draw_row_seeds(rng, P)  # nearest_neighbor_init.py:118-121
-      nn_tables.append(np.ascontiguousarray(ctx.get_cpu_candidate_list(self.nn_k), dtype=np.int32))
+      seeds_all[i] = draw_row_seeds(rng, P)  # nearest_neighbor_init.py:118-121, random_init.py:42
+      if self.init == "nn":
+        nn_tables.append(np.ascontiguousarray(ctx.get_cpu_candidate_list(self.nn_k), dtype=np.int32))
       t0 = time.perf_counter()
       ops = operands_for(ctx)
       dist, stride, coords = ops.distance_args(n, self.max_matrix_dimension)
@@ -540,7 +584,10 @@ class FusedBatchSolver:
       inst.patience = int(pat) if pat is not None else int(2 * math.sqrt(n))
       coords_flags.append(dist is None)
     t0 = time.perf_counter()
-    self._nn_init(h_jobs, seeds_all, nn_tables, ns)
+    if self.init == "nn":
+      self._nn_init(h_jobs, seeds_all, nn_tables, ns)
+    else:
+      self._random_init(h_jobs, seeds_all, ns)
     t1 = time.perf_counter()
     self._draw_tapes(rngs, ns)  # after the row seeds, like the reference
     t_nn, t_tape = t1 - t0, time.perf_counter() - t1

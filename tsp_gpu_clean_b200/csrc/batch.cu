@@ -18,6 +18,8 @@
 //   change, so the run goes on. Otherwise the run pauses: the host takes the argsort and
 //   the run finishes that generation in the RESUME phase of a later launch sequence while
 //   the other runs continue;
+// - with local_search_stage="post_mutation" every child is refined before it is evaluated
+//   (genetic_algorithm.py:333-343): the OFFSPRING phase of the same 2-opt kernel;
 // - the elite 2-opt is one persistent launch per size bucket whose CTAs take
 //   (instance, row) units from an atomic counter, largest instances first, with the
 //   bucket's CTA size chosen by the host's autotuner.
@@ -220,6 +222,7 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value)
     if (u >= units) return;
     const int it = (int)(u / (unsigned)rows), e = (int)(u - (unsigned)it * (unsigned)rows);
     const int i = items[it];
+    const bool offspring = phase == TSPB_BATCH_PHASE_OFFSPRING;
     int parity = 0, row = e;
     if (phase != TSPB_BATCH_PHASE_POSTINIT) {
       const int* c = B.ctl + 4 * i;
@@ -233,7 +236,8 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value)
         }
       }
     }
-    uint8_t* clean = B.clean[0] ? clean_buf(B, parity) + (long long)i * B.P + row : nullptr;
+    uint8_t* clean = !B.clean[0] ? nullptr
+                     : (offspring ? B.off_clean : clean_buf(B, parity)) + (long long)i * B.P + row;
     if (clean && *clean) continue;  // a converged local optimum: refining it changes nothing
     const tspb_batch_instance I = B.inst[i];
     const bool layout_ok = LAYOUT != SCAN_GROUPED ||
@@ -243,7 +247,7 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value)
       continue;
     }
     ScanTour T;
-    T.g_tour = pop_buf(B, parity) + I.pop_offset + (long long)row * I.n;
+    T.g_tour = (offspring ? B.off : pop_buf(B, parity)) + I.pop_offset + (long long)row * I.n;
     T.arrays = dsm;
     T.n = I.n;
     T.k = I.k;
@@ -263,10 +267,12 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value)
   }
 }
 
-// Warp per (instance, refined row) of a phase: fitness after the 2-opt.
+// Warp per (instance, refined row) of a phase: fitness after the 2-opt (of the offspring
+// rows into off_fit in the OFFSPRING phase).
 __global__ void batch_elite_cost_kernel(const tspb_batch B, int phase) {
   const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int e_count = B.elite;
+  const bool offspring = phase == TSPB_BATCH_PHASE_OFFSPRING;
+  const int e_count = offspring ? B.P : B.elite;
   if (w >= (long long)B.num_instances * e_count) return;
   const int i = (int)(w / e_count), e = (int)(w - (long long)i * e_count);
   const int* c = B.ctl + 4 * i;
@@ -275,8 +281,9 @@ __global__ void batch_elite_cost_kernel(const tspb_batch B, int phase) {
   const int row = phase == TSPB_BATCH_PHASE_RESUME ? B.host_elites[(long long)i * e_count + e] : e;
   if ((unsigned)row >= (unsigned)B.P) return;
   const tspb_batch_instance I = B.inst[i];
-  const double f = warp_tour_length(pop_buf(B, parity) + I.pop_offset + (long long)row * I.n, I.n, inst_ds(I));
-  if ((threadIdx.x & 31) == 0) fit_buf(B, parity)[(long long)i * B.P + row] = f;
+  const int32_t* tour = (offspring ? B.off : pop_buf(B, parity)) + I.pop_offset + (long long)row * I.n;
+  const double f = warp_tour_length(tour, I.n, inst_ds(I));
+  if ((threadIdx.x & 31) == 0) (offspring ? B.off_fit : fit_buf(B, parity))[(long long)i * B.P + row] = f;
 }
 
 // CTA per instance of a phase: argmin of fitness (first minimum), strict improvement by
@@ -495,9 +502,9 @@ extern "C" int tspb_batch_two_opt(const tspb_batch* b, const int32_t* items, int
                                   int32_t ctas, uint32_t* queue, void* stream) {
   if (!batch_ok(b) || num_items < 0 || max_n < 4 || !queue) return TSPB_ERR_ARG;
   if (flags & ~(TSPB_BATCH_COORDS | TSPB_BATCH_GROUPED)) return TSPB_ERR_ARG;
-  if (phase < TSPB_BATCH_PHASE_POSTINIT || phase > TSPB_BATCH_PHASE_RUN) return TSPB_ERR_ARG;
+  if (phase < TSPB_BATCH_PHASE_POSTINIT || phase > TSPB_BATCH_PHASE_OFFSPRING) return TSPB_ERR_ARG;
   if (mode != TSPB_MODE_BEST && mode != TSPB_MODE_FIRST) return TSPB_ERR_ARG;
-  const int rows = phase == TSPB_BATCH_PHASE_POSTINIT ? b->P : b->elite;
+  const int rows = (phase == TSPB_BATCH_PHASE_POSTINIT || phase == TSPB_BATCH_PHASE_OFFSPRING) ? b->P : b->elite;
   if (num_items == 0 || rows == 0 || max_iterations <= 0) return TSPB_OK;
   if (!items) return TSPB_ERR_ARG;
   if (phase == TSPB_BATCH_PHASE_RESUME && !b->host_elites) return TSPB_ERR_ARG;
@@ -513,10 +520,13 @@ extern "C" int tspb_batch_two_opt(const tspb_batch* b, const int32_t* items, int
 }
 
 extern "C" int tspb_batch_elite_cost(const tspb_batch* b, int32_t phase, void* stream) {
-  if (!batch_ok(b) || (phase != TSPB_BATCH_PHASE_RESUME && phase != TSPB_BATCH_PHASE_RUN)) return TSPB_ERR_ARG;
-  if (b->num_instances == 0 || b->elite == 0 || b->G == 0) return TSPB_OK;
+  if (!batch_ok(b) || (phase != TSPB_BATCH_PHASE_RESUME && phase != TSPB_BATCH_PHASE_RUN &&
+                       phase != TSPB_BATCH_PHASE_OFFSPRING))
+    return TSPB_ERR_ARG;
+  const int rows = phase == TSPB_BATCH_PHASE_OFFSPRING ? b->P : b->elite;
+  if (b->num_instances == 0 || rows == 0 || b->G == 0) return TSPB_OK;
   if (phase == TSPB_BATCH_PHASE_RESUME && !b->host_elites) return TSPB_ERR_ARG;
-  const long long threads = (long long)b->num_instances * b->elite * 32;
+  const long long threads = (long long)b->num_instances * rows * 32;
   if ((threads + 255) / 256 > 0x7fffffffLL) return TSPB_ERR_UNSUPPORTED;
   batch_elite_cost_kernel<<<(int)((threads + 255) / 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(*b, phase);
   return tspb_launch_status();

@@ -120,17 +120,22 @@ class FusedMemeticSolver:
   def __init__(self, population_size: int = 128, mutation_rate: float = 0.05, tournament_k: int = 5, nn_k: int = 5,
                local_search: LocalSearchConfig | None = None, elite_count: int = 16, post_init: bool = True,
                use_graph: bool = True, chunk: int = 16, max_matrix_dimension: int | None = None,
-               engine: str = "batch", crossover: str = "pmx", mutation: str = "inversion") -> None:
+               engine: str = "batch", crossover: str = "pmx", mutation: str = "inversion", init: str = "nn",
+               local_search_stage: str = "none") -> None:
     if population_size < 2:
       raise ValueError("population_size must be >= 2")
     if engine not in ("batch", "single"):
       raise ValueError("engine must be 'batch' (the multi-instance engine with one run) or 'single'")
     if crossover not in ("pmx", "ox") or mutation not in ("inversion", "swap"):
       raise ValueError("crossover must be 'pmx' or 'ox', mutation 'inversion' or 'swap'")
-    if engine == "single" and (crossover, mutation) != ("pmx", "inversion"):
-      raise ValueError("the single-run engine runs PMX with inversion; use engine='batch' for OX or swap")
+    if init not in ("nn", "random") or local_search_stage not in ("none", "post_mutation"):
+      raise ValueError("init must be 'nn' or 'random', local_search_stage 'none' or 'post_mutation'")
+    if engine == "single" and (crossover, mutation, init, local_search_stage) != ("pmx", "inversion", "nn", "none"):
+      raise ValueError("the single-run engine runs NN init, PMX and inversion with the elite/post-init steps; "
+                       "use engine='batch' for OX, swap, random init or the post_mutation stage")
     self.engine = engine
     self.crossover, self.mutation = crossover, mutation
+    self.init, self.stage = init, local_search_stage
     self.P = population_size
     self.rate = mutation_rate
     self.kt = tournament_k
@@ -346,7 +351,8 @@ class FusedMemeticSolver:
     solver = FusedBatchSolver(population_size=self.P, mutation_rate=self.rate, tournament_k=self.kt, nn_k=self.nn_k,
                               local_search=self.ls, elite_count=self.elite, post_init=self.post_init,
                               max_matrix_dimension=self.max_matrix_dimension, use_graph=self.use_graph,
-                              chunk=self.chunk, crossover=self.crossover, mutation=self.mutation)
+                              chunk=self.chunk, crossover=self.crossover, mutation=self.mutation, init=self.init,
+                              local_search_stage=self.stage)
     (best, stats), = solver.evolve([context], max_generations, patience=patience)
     self.final_population = solver.final_population[0]
     self.final_fitness = solver.final_fitness[0]

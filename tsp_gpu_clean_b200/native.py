@@ -71,6 +71,8 @@ SIGNATURES: dict[str, tuple] = {
   "tspb_select_topk": (ctypes.c_int, [_p, _p, _i32, _i32, _i32, _p, _p]),
   "tspb_nn_init": (ctypes.c_int, [_p, _i32, _p, _i32, _i32, _p, _i32, _i32, _p, _sz, _p, _p]),
   "tspb_nn_init_jobs": (ctypes.c_int, [_p, _i32, _i32, _p, _p, _p]),
+  "tspb_random_init": (ctypes.c_int, [_p, _i32, _i32, _p, _p, _p]),
+  "tspb_random_init_jobs": (ctypes.c_int, [_p, _i32, _i32, _i32, _p]),
   "tspb_tape_draw_host": (ctypes.c_int, [_p, _i32, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _p]),
   "tspb_tape_draw": (ctypes.c_int, [_p, _p, _i32, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _p, _p]),
   "tspb_batch_init": (ctypes.c_int, [_p, _i32, _i32, _p]),
@@ -90,6 +92,7 @@ TSPB_BATCH_DONE = 4
 TSPB_BATCH_PHASE_POSTINIT = 0
 TSPB_BATCH_PHASE_RESUME = 1
 TSPB_BATCH_PHASE_RUN = 2
+TSPB_BATCH_PHASE_OFFSPRING = 3
 TSPB_XOVER_PMX = 0
 TSPB_XOVER_OX = 1
 TSPB_MUT_INVERSION = 0

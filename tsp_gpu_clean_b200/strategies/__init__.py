@@ -2,7 +2,7 @@
 
 from __future__ import annotations
 
-from .initialization import InitializationB200TourNearestNeighbor
+from .initialization import InitializationB200PermRandom, InitializationB200TourNearestNeighbor
 from .local_search import LocalSearchB200TourTwoOpt
 from .operators import (
   CrossoverB200PermOrder,
@@ -17,6 +17,7 @@ STRATEGY_REGISTRY: dict[str, type] = {
   "CrossoverB200PermOrder": CrossoverB200PermOrder,
   "CrossoverB200PermPartiallyMapped": CrossoverB200PermPartiallyMapped,
   "EvaluationB200Cost": EvaluationB200Cost,
+  "InitializationB200PermRandom": InitializationB200PermRandom,
   "InitializationB200TourNearestNeighbor": InitializationB200TourNearestNeighbor,
   "LocalSearchB200TourTwoOpt": LocalSearchB200TourTwoOpt,
   "MutationB200PermInversion": MutationB200PermInversion,
@@ -53,6 +54,7 @@ __all__ = [
   "CrossoverB200PermOrder",
   "CrossoverB200PermPartiallyMapped",
   "EvaluationB200Cost",
+  "InitializationB200PermRandom",
   "InitializationB200TourNearestNeighbor",
   "LocalSearchB200TourTwoOpt",
   "MutationB200PermInversion",

@@ -1,10 +1,15 @@
-"""B200 GRASP nearest-neighbour initialization (drop-in for the reference's NN initializers).
+"""B200 initial populations (drop-ins for the reference's initializers).
 
-`InitializationB200TourNearestNeighbor(k, seed, return_gpu)` mirrors
-`InitializationCPUTourNearestNeighbor` / `InitializationGPUTourNearestNeighbor`
-(`src/algorithms/strategies/initialization/nearest_neighbor_init.py:102-238`): the row seeds
-are drawn on the host from `context.rng` exactly as `draw_row_seeds` does
-(`src/utils/splitmix64.py:21-25`), then one thread per row builds the tour on the GPU.
+- `InitializationB200TourNearestNeighbor(k, seed, return_gpu)` mirrors
+  `InitializationCPUTourNearestNeighbor` / `InitializationGPUTourNearestNeighbor`
+  (`src/algorithms/strategies/initialization/nearest_neighbor_init.py:102-238`): one thread
+  per row builds the GRASP tour on the GPU.
+- `InitializationB200PermRandom(seed, return_gpu)` mirrors `InitializationCPUPermRandom` /
+  `InitializationGPUPermRandom` (`src/algorithms/strategies/initialization/random_init.py:24-120`):
+  one CTA per row shuffles the customer list on the GPU.
+
+Both draw their row seeds on the host from `context.rng` exactly as `draw_row_seeds` does
+(`src/utils/splitmix64.py:21-25`); each row then follows its own SplitMix64 stream.
 """
 
 from __future__ import annotations
@@ -65,6 +70,41 @@ class InitializationB200TourNearestNeighbor(StrategyBase):
     out = torch.empty((population_size, n), dtype=torch.int32, device="cuda")
     native.call("tspb_nn_init", ptr(d_cust), n, ptr(d_cand), rows, kk, ptr(d_seeds), population_size, max_node,
                 ptr(self._ws), need, ptr(out), stream_handle())
+    self.kernel_launches += 1
+    if self.return_gpu:
+      return out
+    host = out.cpu().numpy()
+    self.d2h_bytes += host.nbytes
+    return host
+
+
+class InitializationB200PermRandom(StrategyBase):
+  """Uniform random permutations of `customers`, bit-identical to `InitializationCPUPermRandom`
+  (Fisher-Yates from the last position down, SplitMix64 bounded draws per row)."""
+
+  def __init__(self, seed: Any = None, return_gpu: bool = False) -> None:
+    super().__init__(seed)
+    self.return_gpu = return_gpu
+
+  def _warmup_impl(self, context: Any) -> None:
+    self.initialize(list(range(max(1, context.dimension))), 2, context)
+
+  @time_strategy
+  def initialize(self, customers: Any, population_size: int, context: Any = None) -> Any:
+    if population_size < 0:
+      raise ValueError(f"population_size must be >= 0, got {population_size}")
+    require_gpu()
+    cust = np.ascontiguousarray(customers, dtype=np.int32)
+    n = int(cust.size)
+    seeds = draw_row_seeds(resolve_rng(context, self.rng), population_size)
+    if population_size == 0 or n == 0:
+      empty = torch.empty((population_size, n), dtype=torch.int32, device="cuda")
+      return empty if self.return_gpu else np.empty((population_size, n), dtype=np.int32)
+    d_cust = device_tensor(cust, torch.int32)
+    d_seeds = torch.from_numpy(seeds.view(np.int64).copy()).to("cuda")
+    self.h2d_bytes += cust.nbytes + seeds.nbytes
+    out = torch.empty((population_size, n), dtype=torch.int32, device="cuda")
+    native.call("tspb_random_init", ptr(d_seeds), population_size, n, ptr(d_cust), ptr(out), stream_handle())
     self.kernel_launches += 1
     if self.return_gpu:
       return out
