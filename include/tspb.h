@@ -364,6 +364,8 @@ int tspb_generation_track(const double* fit, const int32_t* pop, int32_t P, int3
 #define TSPB_BATCH_PAUSED 2
 #define TSPB_BATCH_RESUME 3
 #define TSPB_BATCH_DONE 4
+#define TSPB_BATCH_HIT_OPTIMAL 5  /* best <= optimal + 1e-6 (stopped early) */
+#define TSPB_BATCH_NEAR_OPTIMAL 6 /* (best - optimal) / optimal * 100 < 1 (stopped early) */
 
 #define TSPB_BATCH_PHASE_POSTINIT 0
 #define TSPB_BATCH_PHASE_RESUME 1
@@ -380,6 +382,8 @@ typedef struct tspb_batch_instance {
   const double* coords;         /* n x 2 float64; required when dist is NULL */
   const uint32_t* cand_packed;  /* n x k words c | d(a, c) << 16 (tspb_candidate_pack) */
   int64_t patience;             /* generations without a strict improvement before STOPPED */
+  double optimal;               /* known optimal cost (> 0) for the early stops of
+                                   genetic_algorithm.py:894-905, else 0 */
 } tspb_batch_instance;
 
 typedef struct tspb_batch {
@@ -444,8 +448,9 @@ int tspb_batch_two_opt(const tspb_batch* b, const int32_t* items, int32_t num_it
 int tspb_batch_two_opt_occupancy(int32_t max_n, int32_t mode, int32_t threads);
 /* Fitness of the refined rows of a phase (RESUME, RUN, or OFFSPRING into off_fit). */
 int tspb_batch_elite_cost(const tspb_batch* b, int32_t phase, void* stream);
-/* Best tracking, history, patience and the generation counter of a phase's instances:
- * RUN/RESUME -> RUN, STOPPED or DONE (genetic_algorithm.py:876-910). */
+/* Best tracking, history, early stops and the generation counter of a phase's instances:
+ * RUN/RESUME -> HIT_OPTIMAL, NEAR_OPTIMAL, STOPPED (patience), DONE or RUN, checked in
+ * that order (genetic_algorithm.py:876-910). */
 int tspb_batch_track(const tspb_batch* b, int32_t phase, void* stream);
 
 /*

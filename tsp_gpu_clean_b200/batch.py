@@ -115,6 +115,12 @@ CROSSOVER_CODES = {"pmx": native.TSPB_XOVER_PMX, "ox": native.TSPB_XOVER_OX}
 MUTATION_CODES = {"inversion": native.TSPB_MUT_INVERSION, "swap": native.TSPB_MUT_SWAP}
 
 
+# Terminal states of a run that stopped early and the reference's stop_reason for each
+# (genetic_algorithm.py:894-910); a run in state DONE ran every generation.
+STOP_REASONS = {native.TSPB_BATCH_HIT_OPTIMAL: "hit_optimal", native.TSPB_BATCH_NEAR_OPTIMAL: "within_1pct_optimal",
+                native.TSPB_BATCH_STOPPED: "no_improvements"}
+
+
 def elite_rows(fitness: np.ndarray, elite: int) -> np.ndarray:
   """Rows of `argsort(fitness)[:elite]` for every row of an (m, P) fitness array.
 
@@ -504,11 +510,13 @@ class FusedBatchSolver:
     self.kernel_launches += 1
 
   # ------------------------------------------------------------------------ evolve
-  def evolve(self, contexts: Sequence[Any], max_generations: int, patience: Any = None):
+  def evolve(self, contexts: Sequence[Any], max_generations: int, patience: Any = None, optimal_cost: Any = None):
     """Run every context's GA; returns a list of (best_tour, stats) in context order.
 
     `patience`: one value for every run, or one per context; None means the reference's
-    default int(2 * sqrt(n)) (`genetic_algorithm.py:815-816`)."""
+    default int(2 * sqrt(n)) (`genetic_algorithm.py:815-816`). `optimal_cost`: None, one
+    value or one per context; a run whose best reaches it, or comes within 1 % of it,
+    stops early (`genetic_algorithm.py:894-905`)."""
     require_gpu()
     t_start = time.perf_counter()
     P, G, k = self.P, int(max_generations), int(self.ls.candidate_k)
@@ -582,6 +590,8 @@ class FusedBatchSolver:
       inst.cand_packed = tabs.packed.data_ptr()
       pat = patience[i] if isinstance(patience, (list, tuple, np.ndarray)) else patience
       inst.patience = int(pat) if pat is not None else int(2 * math.sqrt(n))
+      opt = optimal_cost[i] if isinstance(optimal_cost, (list, tuple, np.ndarray)) else optimal_cost
+      inst.optimal = float(opt) if opt is not None and opt > 0 else 0.0
       coords_flags.append(dist is None)
     t0 = time.perf_counter()
     if self.init == "nn":
@@ -701,8 +711,8 @@ class FusedBatchSolver:
         "best_fitness": float(best_cost[i]),
         "best_is_feasible": True,
         "generations_completed": done,
-        "stopped_early": done < G,
-        "stop_reason": "no_improvements" if done < G else "max_generations",
+        "stopped_early": int(ctl[i, 1]) in STOP_REASONS,
+        "stop_reason": STOP_REASONS.get(int(ctl[i, 1]), "max_generations"),
         "convergence_history": history[i, : done + 1].tolist(),
         "host_elite_generations": int(host_elite_gens[i]),
         "elite_edge_ties": int(ties[i, :done].sum()) if G > 0 else 0,

@@ -343,7 +343,18 @@ __global__ void __launch_bounds__(128) batch_track_kernel(const tspb_batch B, in
     c[2] = stall;
     c[3] = g + 1;
     c[0] = g + 1;
-    c[1] = stall >= I.patience ? TSPB_BATCH_STOPPED : (g + 1 >= B.G ? TSPB_BATCH_DONE : TSPB_BATCH_RUN);
+    // early stops in the reference's order: a known optimum reached or within 1 %, then
+    // patience (the arithmetic spelled out so that no step is contracted)
+    const double opt = I.optimal;
+    int next = g + 1 >= B.G ? TSPB_BATCH_DONE : TSPB_BATCH_RUN;
+    if (stall >= I.patience) next = TSPB_BATCH_STOPPED;
+    if (opt > 0.0) {
+      if (best <= __dadd_rn(opt, 1e-6))
+        next = TSPB_BATCH_HIT_OPTIMAL;
+      else if (__dmul_rn(__ddiv_rn(__dsub_rn(best, opt), opt), 100.0) < 1.0)
+        next = TSPB_BATCH_NEAR_OPTIMAL;
+    }
+    c[1] = next;
   }
   __syncthreads();
   if (improve) {

@@ -108,6 +108,17 @@ def draw_generation_tape_numpy(rng: np.random.Generator, G: int, P: int, kt: int
   return (tourn, cut_a, cut_b, u, inv_a, inv_b), states
 
 
+def trailing_stall(history: list) -> int:
+  """Generations since the last strict improvement: the best-so-far history changes only on
+  an improvement larger than 1e-6, so this is the count of trailing unchanged entries."""
+  k = 0
+  for a, b in zip(reversed(history[:-1]), reversed(history[1:])):
+    if a != b:
+      break
+    k += 1
+  return k
+
+
 @dataclass
 class LocalSearchConfig:
   mode: str = "best"
@@ -213,14 +224,20 @@ class FusedMemeticSolver:
     self.host_elite_generations += 1
 
   # -------------------------------------------------------------------------- evolve
-  def evolve(self, context: Any, customers: Any, max_generations: int, patience: int | None = None):
+  def evolve(self, context: Any, customers: Any, max_generations: int, patience: int | None = None,
+             optimal_cost: float | None = None):
+    """One GA run; returns (best_tour, stats) like `GeneticAlgorithm.evolve`
+    (`genetic_algorithm.py:789-965`). `optimal_cost` (batch engine) stops the run when its
+    best reaches the known optimum or comes within 1 % of it."""
     require_gpu()
     t_start = time.perf_counter()
     n = len(customers)
     if n < 4 or n != int(context.dimension) or list(customers) != list(range(n)):
       raise ValueError("FusedMemeticSolver needs the full tour customers = range(dimension) with dimension >= 4")
     if self.engine == "batch":
-      return self._evolve_batch(context, max_generations, patience)
+      return self._evolve_batch(context, max_generations, patience, optimal_cost)
+    if optimal_cost is not None and optimal_cost > 0:
+      raise NotImplementedError("the single-run engine has no optimal-cost stop; use engine='batch'")
     if patience is None:
       patience = int(2 * math.sqrt(n))
     self.n, self.patience = n, patience
@@ -335,15 +352,16 @@ class FusedMemeticSolver:
       "best_fitness": best_cost,
       "best_is_feasible": True,
       "generations_completed": done,
-      "stopped_early": done < G,
-      "stop_reason": "no_improvements" if done < G else "max_generations",
+      # patience can also run out exactly at the last generation (genetic_algorithm.py:906-910)
+      "stopped_early": done < G or trailing_stall(history) >= patience,
+      "stop_reason": "no_improvements" if done < G or trailing_stall(history) >= patience else "max_generations",
       "convergence_history": history,
       "kernel_launches": self.kernel_launches,
       "host_elite_generations": self.host_elite_generations,
     }
     return best_tour, stats
 
-  def _evolve_batch(self, context: Any, max_generations: int, patience: int | None):
+  def _evolve_batch(self, context: Any, max_generations: int, patience: int | None, optimal_cost: float | None):
     """The run as a one-instance batch (`batch.FusedBatchSolver`): the persistent 2-opt,
     converged-row skipping and device-settled elite ties of the batch engine, same results."""
     from .batch import FusedBatchSolver
@@ -353,7 +371,7 @@ class FusedMemeticSolver:
                               max_matrix_dimension=self.max_matrix_dimension, use_graph=self.use_graph,
                               chunk=self.chunk, crossover=self.crossover, mutation=self.mutation, init=self.init,
                               local_search_stage=self.stage)
-    (best, stats), = solver.evolve([context], max_generations, patience=patience)
+    (best, stats), = solver.evolve([context], max_generations, patience=patience, optimal_cost=optimal_cost)
     self.final_population = solver.final_population[0]
     self.final_fitness = solver.final_fitness[0]
     self.last_timing = solver.last_timing

@@ -89,6 +89,8 @@ TSPB_BATCH_STOPPED = 1
 TSPB_BATCH_PAUSED = 2
 TSPB_BATCH_RESUME = 3
 TSPB_BATCH_DONE = 4
+TSPB_BATCH_HIT_OPTIMAL = 5
+TSPB_BATCH_NEAR_OPTIMAL = 6
 TSPB_BATCH_PHASE_POSTINIT = 0
 TSPB_BATCH_PHASE_RESUME = 1
 TSPB_BATCH_PHASE_RUN = 2
@@ -133,7 +135,7 @@ class BatchInstance(ctypes.Structure):
   """`tspb_batch_instance` of include/tspb.h."""
 
   _fields_ = [("n", _i32), ("k", _i32), ("pop_offset", _i64), ("node_offset", _i64), ("dist", _p),
-              ("dist_stride", _i64), ("coords", _p), ("cand_packed", _p), ("patience", _i64)]
+              ("dist_stride", _i64), ("coords", _p), ("cand_packed", _p), ("patience", _i64), ("optimal", _f64)]
 
 
 class BatchState(ctypes.Structure):
