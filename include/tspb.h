@@ -254,6 +254,30 @@ typedef struct tspb_nn_job {
 int tspb_nn_init_jobs(const tspb_nn_job* jobs, int32_t num_jobs, int32_t max_rows, int32_t* workspace,
                       const int64_t* ws_offsets, void* stream);
 
+/* Coordinate-based TSPLIB edge weight types (src/distances/matrix.py:39-41). */
+#define TSPB_EDGE_EUC_2D 0
+#define TSPB_EDGE_EUC_3D 1
+#define TSPB_EDGE_MAN_2D 2
+#define TSPB_EDGE_MAN_3D 3
+#define TSPB_EDGE_MAX_2D 4
+#define TSPB_EDGE_MAX_3D 5
+#define TSPB_EDGE_CEIL_2D 6
+#define TSPB_EDGE_ATT 7
+#define TSPB_EDGE_GEO 8
+#define TSPB_EDGE_XRAY1 9
+
+/*
+ * Dense n x n int32 distance matrix (row stride ld) of one TSPLIB edge type from n x dim
+ * float64 coordinates (dim 2 or 3; XRAY1 needs 3; the planar and 3-D formulas run over
+ * all dim columns, GEO reads DDD.MM latitude and longitude from columns 0 and 1), zero
+ * diagonal. Replaces compute_distance_matrix (src/distances/matrix.py:44-131, 214-273)
+ * and the device formulas of pairwise_device.cuh; bit-identical for every type but GEO,
+ * whose cos/acos may differ from the host's in the last bit (an entry changes only when
+ * its value lies within about 1e-11 of an integer before truncation).
+ */
+int tspb_distance_matrix(const double* coords, int32_t n, int32_t dim, int32_t edge_type, int32_t* out, int64_t ld,
+                         void* stream);
+
 /*
  * Uniform random-permutation initial population, CTA per row: row r is `customers`
  * (n entries; NULL means 0..n-1) shuffled by Fisher-Yates from position n-1 down to 1,

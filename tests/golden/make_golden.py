@@ -17,6 +17,8 @@ Outputs (NumPy `.npz`, committed next to this script):
                        local optimum in best and first mode, with pass and pair counts;
 - `ox_swap.npz`        Order Crossover and swap mutation batches, and two GA runs with them
                        (`python make_golden.py <reference root> ox` regenerates only this file)
+- `distances.npz`      distance matrices and k-NN tables of every coordinate-based TSPLIB
+                       edge type on seeded synthetic coordinates (`... dist`)
 - `stage.npz`          random-permutation populations, and GA runs with 2-opt on every
                        offspring (`post_mutation`), two in the Chapter-4 configuration
                        (`... stage` regenerates only this file)
@@ -451,6 +453,53 @@ def main_stage(ref_root: str) -> None:
   np.savez_compressed(os.path.join(HERE, "stage.npz"), **out)
 
 
+def dist_coords(edge_type: str, n: int, seed: int) -> np.ndarray:
+  """Seeded synthetic coordinates for one TSPLIB edge type: planar or 3-D points in
+  [0, 1000], ATT-like coordinates in [0, 8000], GEO DDD.MM latitudes and longitudes, and
+  XRAY1 motor positions (phi in [0, 360), chi and two-theta in [0, 100])."""
+  rng = np.random.default_rng(seed)
+  if edge_type == "GEO":
+    lat = rng.integers(-89, 90, n) + np.sign(rng.uniform(-1, 1, n)) * np.round(rng.uniform(0, 0.5999, n), 2)
+    lon = rng.integers(-179, 180, n) + np.sign(rng.uniform(-1, 1, n)) * np.round(rng.uniform(0, 0.5999, n), 2)
+    return np.stack([lat, lon], axis=1)
+  if edge_type == "XRAY1":
+    return np.stack([rng.uniform(0, 360, n), rng.uniform(0, 100, n), rng.uniform(0, 100, n)], axis=1)
+  if edge_type == "ATT":
+    return np.round(rng.uniform(0, 8000, (n, 2)))
+  dim = 3 if edge_type.endswith("_3D") else 2
+  return rng.uniform(0, 1000, (n, dim))
+
+
+DIST_TYPES = ("EUC_2D", "EUC_3D", "MAN_2D", "MAN_3D", "MAX_2D", "MAX_3D", "CEIL_2D", "ATT", "GEO", "XRAY1")
+
+
+def main_dist(ref_root: str) -> None:
+  """`distances.npz`: the reference's `compute_distance_matrix` and `compute_candidate_list`
+  (`src/distances/matrix.py:140-273`) for every coordinate-based TSPLIB edge type, on seeded
+  synthetic coordinates: full matrices and 8-NN tables at n = 120, digests of the matrix
+  and the 10-NN table at n = 2500 (the chunked path; its coordinates are regenerated by
+  `dist_coords`)."""
+  _setup(ref_root)
+  from distances.matrix import compute_candidate_list, compute_distance_matrix
+
+  out: dict[str, np.ndarray] = {}
+  for j, et in enumerate(DIST_TYPES):
+    for n, full in ((120, True), (2500, False)):
+      c = dist_coords(et, n, 700 + 10 * j + (n > 1000))
+      d = compute_distance_matrix(c, et)
+      key = f"{et}_{n}"
+      if full:
+        out[f"{key}_coords"] = c
+        out[f"{key}_matrix"] = np.asarray(d, dtype=np.int32)
+        out[f"{key}_knn"] = np.asarray(compute_candidate_list(c, et, 8), dtype=np.int32)
+      else:
+        knn = np.ascontiguousarray(compute_candidate_list(c, et, 10), dtype=np.int32)
+        out[f"{key}_digest"] = np.frombuffer(hashlib.sha256(np.ascontiguousarray(d, dtype=np.int32).tobytes())
+                                             .digest(), dtype=np.uint8)
+        out[f"{key}_knn_digest"] = np.frombuffer(hashlib.sha256(knn.tobytes()).digest(), dtype=np.uint8)
+  np.savez_compressed(os.path.join(HERE, "distances.npz"), **out)
+
+
 if __name__ == "__main__":
   root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
   part = sys.argv[2] if len(sys.argv) > 2 else "all"
@@ -460,3 +509,5 @@ if __name__ == "__main__":
     main_ox_swap(root)
   if part in ("all", "stage"):
     main_stage(root)
+  if part in ("all", "dist"):
+    main_dist(root)

@@ -212,3 +212,24 @@ def test_oracle_ga_with_post_mutation_stage_matches_reference(golden, tag):
   assert np.array_equal(np.asarray(stats["convergence_history"]), g[f"ga_{tag}_history"])
   assert np.array_equal(best, g[f"ga_{tag}_best"])
   assert rng.bit_generator.state["state"]["state"] % (1 << 63) == int(g[f"ga_{tag}_rng"][0])
+
+
+DIST_TYPES = ("EUC_2D", "EUC_3D", "MAN_2D", "MAN_3D", "MAX_2D", "MAX_3D", "CEIL_2D", "ATT", "GEO", "XRAY1")
+
+
+@pytest.mark.parametrize("edge_type", DIST_TYPES)
+def test_distance_types_match_reference(golden, edge_type):
+  import hashlib
+
+  from tests.golden.make_golden import dist_coords
+
+  g = golden("distances.npz")
+  c = g[f"{edge_type}_120_coords"]
+  assert np.array_equal(distances.distance_matrix(c, edge_type), g[f"{edge_type}_120_matrix"])
+  assert np.array_equal(distances.candidate_list(8, coords=c, edge_type=edge_type), g[f"{edge_type}_120_knn"])
+  j = DIST_TYPES.index(edge_type)
+  c = dist_coords(edge_type, 2500, 700 + 10 * j + 1)
+  d = distances.distance_matrix(c, edge_type)
+  assert hashlib.sha256(d.tobytes()).digest() == g[f"{edge_type}_2500_digest"].tobytes()
+  knn = np.ascontiguousarray(distances.candidate_list(10, coords=c, edge_type=edge_type))
+  assert hashlib.sha256(knn.tobytes()).digest() == g[f"{edge_type}_2500_knn_digest"].tobytes()

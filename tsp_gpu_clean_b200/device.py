@@ -181,6 +181,24 @@ class DeviceOperands:
 
         call("tspb_euc2d_matrix", ptr(self.coords()), n, ptr(d), n, stream_handle())
       self._dist = d
+    if self._dist is None and self._tsplib_on_device():
+      # Every other coordinate type (ATT, GEO, CEIL_2D, MAN/MAX, 3-D, XRAY1) is built in HBM
+      # by tspb_distance_matrix; its largest entry is checked against the int32 gain bound.
+      from .native import EDGE_TYPE_CODES, call
+
+      prob = self.context.problem
+      c = np.ascontiguousarray(prob.coordinates, dtype=np.float64)
+      n, dim = int(c.shape[0]), int(c.shape[1])
+      check_free(n * n * 4, f"dense distance matrix (n={n})")
+      d = torch.empty((n, n), dtype=torch.int32, device="cuda")
+      if n:
+        dc = device_tensor(c, torch.float64)
+        self.h2d_bytes += c.nbytes
+        call("tspb_distance_matrix", ptr(dc), n, dim, EDGE_TYPE_CODES[prob.edge_type], ptr(d), n, stream_handle())
+        lo, hi = int(d.min().item()), int(d.max().item())
+        if hi > MAX_DISTANCE or lo < 0:
+          raise ValueError("distances outside [0, 2^30) are not supported by the int32 gain kernels")
+      self._dist = d
     if self._dist is None:
       D = self.context.get_cpu_distances()
       D = np.ascontiguousarray(D, dtype=np.int32)
@@ -190,6 +208,16 @@ class DeviceOperands:
       self._dist = device_tensor(D, torch.int32)
       self.h2d_bytes += D.nbytes
     return self._dist
+
+  def _tsplib_on_device(self) -> bool:
+    from .native import EDGE_TYPE_CODES
+
+    prob = self.context.problem
+    c = getattr(prob, "coordinates", None)
+    if getattr(prob, "distances", None) is not None or c is None:
+      return False
+    shape = np.shape(c)
+    return getattr(prob, "edge_type", "EUC_2D") in EDGE_TYPE_CODES and len(shape) == 2 and shape[1] in (2, 3)
 
   def _euc2d_on_device(self) -> bool:
     prob = self.context.problem

@@ -72,6 +72,7 @@ SIGNATURES: dict[str, tuple] = {
   "tspb_nn_init": (ctypes.c_int, [_p, _i32, _p, _i32, _i32, _p, _i32, _i32, _p, _sz, _p, _p]),
   "tspb_nn_init_jobs": (ctypes.c_int, [_p, _i32, _i32, _p, _p, _p]),
   "tspb_random_init": (ctypes.c_int, [_p, _i32, _i32, _p, _p, _p]),
+  "tspb_distance_matrix": (ctypes.c_int, [_p, _i32, _i32, _i32, _p, _i64, _p]),
   "tspb_random_init_jobs": (ctypes.c_int, [_p, _i32, _i32, _i32, _p]),
   "tspb_tape_draw_host": (ctypes.c_int, [_p, _i32, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _p]),
   "tspb_tape_draw": (ctypes.c_int, [_p, _p, _i32, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _p, _p]),
@@ -95,6 +96,9 @@ TSPB_BATCH_PHASE_POSTINIT = 0
 TSPB_BATCH_PHASE_RESUME = 1
 TSPB_BATCH_PHASE_RUN = 2
 TSPB_BATCH_PHASE_OFFSPRING = 3
+# Coordinate-based TSPLIB edge types of tspb_distance_matrix.
+EDGE_TYPE_CODES = {"EUC_2D": 0, "EUC_3D": 1, "MAN_2D": 2, "MAN_3D": 3, "MAX_2D": 4, "MAX_3D": 5, "CEIL_2D": 6,
+                   "ATT": 7, "GEO": 8, "XRAY1": 9}
 TSPB_XOVER_PMX = 0
 TSPB_XOVER_OX = 1
 TSPB_MUT_INVERSION = 0

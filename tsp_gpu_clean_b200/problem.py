@@ -46,9 +46,12 @@ class Problem:
     return self.problem_type in VRP_PROBLEM_TYPES
 
   @classmethod
-  def from_coordinates(cls, coords: np.ndarray, name: str = "synthetic") -> "Problem":
+  def from_coordinates(cls, coords: np.ndarray, name: str = "synthetic", edge_type: str = "EUC_2D") -> "Problem":
     coords = np.asarray(coords, dtype=np.float64)
-    return cls(name=name, dimension=len(coords), problem_type="TSP", edge_type="EUC_2D", coordinates=coords, distances=None)
+    if edge_type not in COORDINATE_EDGE_TYPES:
+      raise ValueError(f"unsupported coordinate edge type {edge_type!r}; supported: {sorted(COORDINATE_EDGE_TYPES)}")
+    return cls(name=name, dimension=len(coords), problem_type="TSP", edge_type=edge_type, coordinates=coords,
+               distances=None)
 
   @classmethod
   def from_matrix(cls, dist: np.ndarray, name: str = "explicit") -> "Problem":
@@ -80,26 +83,65 @@ def resolve_rng(context: Any = None, fallback: Any = None) -> np.random.Generato
   return make_rng(fallback)
 
 
+COORDINATE_EDGE_TYPES = frozenset(("EUC_2D", "EUC_3D", "MAN_2D", "MAN_3D", "MAX_2D", "MAX_3D", "CEIL_2D", "ATT", "GEO",
+                                   "XRAY1"))
+
+
+def _geo_radians(x: np.ndarray) -> np.ndarray:
+  deg = np.trunc(x)
+  return 3.141592 * (deg + 5.0 * (x - deg) / 3.0) / 180.0
+
+
+def distance_block(rows: np.ndarray, coords: np.ndarray, edge_type: str = "EUC_2D") -> np.ndarray:
+  """`(len(rows), n)` int64 block of a TSPLIB coordinate type, as `_distance_block` computes
+  it (`matrix.py:44-131`); the context's k-NN tables are built from these blocks."""
+  if edge_type == "XRAY1":
+    phi = np.abs(rows[:, None, 0] - coords[None, :, 0])
+    cost = np.maximum(np.maximum(np.minimum(phi, np.abs(phi - 360.0)), np.abs(rows[:, None, 1] - coords[None, :, 1])),
+                      np.abs(rows[:, None, 2] - coords[None, :, 2]))
+    return np.trunc(100.0 * cost + 0.5).astype(np.int32).astype(np.int64)
+  if edge_type == "GEO":
+    la, lo = _geo_radians(rows[:, 0])[:, None], _geo_radians(rows[:, 1])[:, None]
+    lb, lp = _geo_radians(coords[:, 0])[None, :], _geo_radians(coords[:, 1])[None, :]
+    q1, q2, q3 = np.cos(lo - lp), np.cos(la - lb), np.cos(la + lb)
+    return (6378.388 * np.arccos(np.clip(0.5 * ((1.0 + q1) * q2 - (1.0 - q1) * q3), -1.0, 1.0)) + 1.0).astype(np.int64)
+  diff = rows[:, None, :] - coords[None, :, :]
+  if edge_type in ("EUC_2D", "EUC_3D"):
+    return (np.sqrt(np.sum(diff * diff, axis=2)) + 0.5).astype(np.int64)
+  if edge_type == "CEIL_2D":
+    return np.ceil(np.sqrt(np.sum(diff * diff, axis=2))).astype(np.int64)
+  if edge_type == "ATT":
+    r = np.sqrt(np.sum(diff * diff, axis=2) / 10.0)
+    t = (r + 0.5).astype(np.int64)
+    return np.where(t < r, t + 1, t)
+  if edge_type in ("MAN_2D", "MAN_3D"):
+    return (np.sum(np.abs(diff), axis=2) + 0.5).astype(np.int64)
+  if edge_type in ("MAX_2D", "MAX_3D"):
+    return (np.max(np.abs(diff), axis=2) + 0.5).astype(np.int64)
+  raise ValueError(f"unsupported coordinate edge type {edge_type!r}")
+
+
 def euc2d_block(rows: np.ndarray, coords: np.ndarray) -> np.ndarray:
   """EUC_2D block `nint(sqrt(dx^2 + dy^2))` as int64 (`matrix.py:82-86`)."""
-  diff = rows[:, None, :] - coords[None, :, :]
-  return (np.sqrt(np.sum(diff * diff, axis=2)) + 0.5).astype(np.int64)
+  return distance_block(rows, coords, "EUC_2D")
 
 
-def compute_distance_matrix(coords: np.ndarray) -> np.ndarray:
-  """Host EUC_2D matrix, int32, zero diagonal (`matrix.py:214-273`)."""
+def compute_distance_matrix(coords: np.ndarray, edge_type: str = "EUC_2D") -> np.ndarray:
+  """Host matrix of a coordinate type, int32, zero diagonal (`matrix.py:214-273`); the
+  device builds the same matrix with `tspb_distance_matrix`."""
   coords = np.asarray(coords, dtype=np.float64)
   n = coords.shape[0]
   if n <= 2048:
-    d = euc2d_block(coords, coords)
+    d = distance_block(coords, coords, edge_type)
   else:
-    d = np.concatenate([euc2d_block(coords[s : s + 512], coords) for s in range(0, n, 512)], axis=0)
+    d = np.concatenate([distance_block(coords[s : s + 512], coords, edge_type) for s in range(0, n, 512)], axis=0)
   out = d.astype(np.int32)
   np.fill_diagonal(out, 0)
   return out
 
 
-def compute_candidate_list(k: int, distances: np.ndarray | None = None, coords: np.ndarray | None = None) -> np.ndarray:
+def compute_candidate_list(k: int, distances: np.ndarray | None = None, coords: np.ndarray | None = None,
+                           edge_type: str = "EUC_2D") -> np.ndarray:
   """Host k-NN table `(n, min(k, n-1))` int32 (`matrix.py:140-211`)."""
   n = int(distances.shape[0] if distances is not None else coords.shape[0])
   if n <= 1 or k <= 0:
@@ -112,7 +154,8 @@ def compute_candidate_list(k: int, distances: np.ndarray | None = None, coords: 
     if distances is not None:
       block = np.asarray(distances[s:e], dtype=np.int64)
     else:
-      block = euc2d_block(np.asarray(coords[s:e], dtype=np.float64), np.asarray(coords, dtype=np.float64))
+      block = distance_block(np.asarray(coords[s:e], dtype=np.float64), np.asarray(coords, dtype=np.float64),
+                             edge_type)
     r = np.arange(e - s)
     block[r, np.arange(s, e)] = big
     cols = np.argpartition(block, k_eff, axis=1)[:, :k_eff]
@@ -158,7 +201,7 @@ class ProblemContext:
       if self.problem.distances is not None:
         self._cpu_distances = self.problem.distances
       else:
-        self._cpu_distances = compute_distance_matrix(self.problem.coordinates)
+        self._cpu_distances = compute_distance_matrix(self.problem.coordinates, self.problem.edge_type)
     return self._cpu_distances
 
   def get_cpu_coordinates(self) -> np.ndarray | None:
@@ -170,7 +213,7 @@ class ProblemContext:
       if self.problem.distances is not None:
         cached = compute_candidate_list(k, distances=self.problem.distances)
       else:
-        cached = compute_candidate_list(k, coords=self.problem.coordinates)
+        cached = compute_candidate_list(k, coords=self.problem.coordinates, edge_type=self.problem.edge_type)
       self._cpu_candidate_lists[k] = cached
     return cached
 
