@@ -254,6 +254,23 @@ typedef struct tspb_nn_job {
 int tspb_nn_init_jobs(const tspb_nn_job* jobs, int32_t num_jobs, int32_t max_rows, int32_t* workspace,
                       const int64_t* ws_offsets, void* stream);
 
+/*
+ * Exhaustive steepest-descent 3-opt of open (cyclic TSP) tours in place, up to
+ * max_iterations passes each, bit-identical to the reference's CPU 3-opt
+ * (cpu_three_opt_best_move / cpu_three_opt_refine,
+ * benchmark_scripts/experiments-and-examples/experiment-comparing-3opt-and-2opt/gpu_three_opt.py:143-277;
+ * the GPU strategy LocalSearchGPUThreeOpt(mode="batch"/"naive") of the same file). Distances
+ * from `dist` (n x dist_stride) or rebuilt from EUC_2D `coords`. One CTA per tour, `threads`
+ * 128, 256 or 512; n <= 4096 (one pass is n^3/6 triples). For n above 220 each CTA needs n*n int32 of `workspace`
+ * (tspb_three_opt_workspace_bytes); fewer CTAs are launched when the workspace holds fewer
+ * tours (TSPB_ERR_WORKSPACE when it holds none). stats (optional): [tours][3] passes, moves,
+ * (triple, case) candidates evaluated.
+ */
+int tspb_three_opt(int32_t* tours, int32_t num_tours, int32_t n, const int32_t* dist, int64_t dist_stride,
+                   const double* coords, int64_t max_iterations, int32_t threads, int32_t* workspace,
+                   size_t workspace_bytes, int32_t* status, int64_t* stats, void* stream);
+int tspb_three_opt_workspace_bytes(int32_t n, int32_t ctas, size_t* bytes);
+
 /* Coordinate-based TSPLIB edge weight types (src/distances/matrix.py:39-41). */
 #define TSPB_EDGE_EUC_2D 0
 #define TSPB_EDGE_EUC_3D 1

@@ -19,6 +19,8 @@ Outputs (NumPy `.npz`, committed next to this script):
                        (`python make_golden.py <reference root> ox` regenerates only this file)
 - `distances.npz`      distance matrices and k-NN tables of every coordinate-based TSPLIB
                        edge type on seeded synthetic coordinates (`... dist`)
+- `three_opt.npz`      exhaustive steepest 3-opt moves and refinements of the reference's
+                       CPU 3-opt (`... three_opt`)
 - `stage.npz`          random-permutation populations, and GA runs with 2-opt on every
                        offspring (`post_mutation`), two in the Chapter-4 configuration
                        (`... stage` regenerates only this file)
@@ -500,6 +502,48 @@ def main_dist(ref_root: str) -> None:
   np.savez_compressed(os.path.join(HERE, "distances.npz"), **out)
 
 
+def main_three_opt(ref_root: str) -> None:
+  """`three_opt.npz`: the reference's exhaustive CPU 3-opt (`cpu_three_opt_best_move`,
+  `cpu_three_opt_refine` of its 3-opt experiment,
+  `benchmark_scripts/experiments-and-examples/experiment-comparing-3opt-and-2opt/gpu_three_opt.py:133-277`)
+  on open tours of uniform and integer-lattice instances (the lattices tie many deltas):
+  the steepest move of every input tour and the tours after 1, 3 and unlimited passes."""
+  _setup(ref_root)
+  import importlib.util
+
+  path = os.path.join(ref_root, "benchmark_scripts", "experiments-and-examples",
+                      "experiment-comparing-3opt-and-2opt", "gpu_three_opt.py")
+  spec = importlib.util.spec_from_file_location("reference_gpu_three_opt", path)
+  mod = importlib.util.module_from_spec(spec)
+  spec.loader.exec_module(mod)
+  from tsp_gpu_clean_b200 import instances
+
+  out: dict[str, np.ndarray] = {}
+  cases = [("u5", instances.uniform_instance(5, 51), 6), ("u6", instances.uniform_instance(6, 52), 6),
+           ("u9", instances.uniform_instance(9, 53), 6), ("u16", instances.uniform_instance(16, 54), 5),
+           ("u40", instances.uniform_instance(40, 55), 3), ("lat16", None, 5), ("lat36", None, 3)]
+  for tag, coords, tours_n in cases:
+    t = time.time()
+    if coords is None:
+      side = int(tag[3:]) ** 0.5
+      side = int(round(side))
+      coords = np.array([[10.0 * x, 10.0 * y] for x in range(side) for y in range(side)])
+    n = len(coords)
+    diff = coords[:, None, :] - coords[None, :, :]
+    D = (np.sqrt((diff * diff).sum(axis=2)) + 0.5).astype(np.int32)
+    np.fill_diagonal(D, 0)
+    tours = instances.random_tours(n, tours_n, 900 + n)
+    out[f"{tag}_coords"] = coords
+    out[f"{tag}_tours"] = tours
+    out[f"{tag}_best"] = np.array([mod.cpu_three_opt_best_move(tt, D, is_closed=False) for tt in tours],
+                                  dtype=np.int64)
+    for iters in (1, 3, 1000):
+      out[f"{tag}_refined{iters}"] = np.stack([mod.cpu_three_opt_refine(tt, D, max_iterations=iters, is_closed=False)
+                                               for tt in tours]).astype(np.int32)
+    print(f"3-opt {tag}: {time.time() - t:.1f}s")
+  np.savez_compressed(os.path.join(HERE, "three_opt.npz"), **out)
+
+
 if __name__ == "__main__":
   root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
   part = sys.argv[2] if len(sys.argv) > 2 else "all"
@@ -511,3 +555,5 @@ if __name__ == "__main__":
     main_stage(root)
   if part in ("all", "dist"):
     main_dist(root)
+  if part in ("all", "three_opt"):
+    main_three_opt(root)

@@ -233,3 +233,27 @@ def test_distance_types_match_reference(golden, edge_type):
   assert hashlib.sha256(d.tobytes()).digest() == g[f"{edge_type}_2500_digest"].tobytes()
   knn = np.ascontiguousarray(distances.candidate_list(10, coords=c, edge_type=edge_type))
   assert hashlib.sha256(knn.tobytes()).digest() == g[f"{edge_type}_2500_knn_digest"].tobytes()
+
+
+THREE_OPT_TAGS = ["u5", "u6", "u9", "u16", "u40", "lat16", "lat36"]
+
+
+def _three_opt_matrix(coords):
+  diff = coords[:, None, :] - coords[None, :, :]
+  d = (np.sqrt((diff * diff).sum(axis=2)) + 0.5).astype(np.int32)
+  np.fill_diagonal(d, 0)
+  return d
+
+
+@pytest.mark.parametrize("tag", THREE_OPT_TAGS)
+def test_three_opt_matches_reference(golden, tag):
+  from oracle import three_opt
+
+  g = golden("three_opt.npz")
+  D = _three_opt_matrix(g[f"{tag}_coords"])
+  assert np.array_equal(D, distances.euc2d_matrix(g[f"{tag}_coords"]))
+  for t, want in zip(g[f"{tag}_tours"], g[f"{tag}_best"]):
+    assert tuple(three_opt.best_move(t, D)) == tuple(int(v) for v in want)
+  for iters in (1, 3, 1000):
+    got, _ = three_opt.improve_batch(g[f"{tag}_tours"], D, iters)
+    assert np.array_equal(got, g[f"{tag}_refined{iters}"]), iters
