@@ -98,10 +98,18 @@ class ClockSampler:
     self.proc = None
 
   def __enter__(self):
+    """Start sampling and wait for the first sample: nvidia-smi's start-up (NVML
+    initialisation) then lies before the timed region instead of inside it."""
+    import select
+
+    self.first = []
     try:
       self.proc = subprocess.Popen(
         ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+      ready, _, _ = select.select([self.proc.stdout], [], [], 5.0)
+      if ready:
+        self.first.append(self.proc.stdout.readline())
     except Exception:
       self.proc = None
     return self
@@ -115,7 +123,7 @@ class ClockSampler:
       except Exception:
         self.proc.kill()
         out = ""
-      self.lines = [ln for ln in out.splitlines() if ln.strip()]
+      self.lines = [ln for ln in self.first + out.splitlines() if ln.strip()]
 
   def summary(self) -> dict:
     sm, mx, reasons = [], 0.0, set()

@@ -503,6 +503,11 @@ int tspb_batch_track(const tspb_batch* b, int32_t phase, void* stream);
  */
 int tspb_knn(const int32_t* dist, int64_t dist_stride, const double* coords, int32_t n, int32_t k,
              int32_t* out, void* stream);
+/* The same table (k + 1 <= 64) and ties[u] = 1 where the k-th and (k+1)-th nearest
+ * distances of u are equal: only those rows can differ from the reference's argpartition,
+ * every other row equals compute_candidate_list's. */
+int tspb_knn_ties(const int32_t* dist, int64_t dist_stride, const double* coords, int32_t n, int32_t k,
+                  int32_t* out, int32_t* ties, void* stream);
 
 /*
  * Learned candidate lists (no reference counterpart: the reference uses plain k-NN).

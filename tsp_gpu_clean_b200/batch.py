@@ -48,7 +48,7 @@ import numpy as np
 
 from . import native
 from .autotune import BatchAutotuner
-from .device import operands_for, ptr, require_gpu, stream_handle, torch
+from .device import candidate_list, operands_for, ptr, require_gpu, stream_handle, torch
 from .fused import LocalSearchConfig, draw_generation_tape
 from .problem import resolve_rng
 from .strategies.initialization import draw_row_seeds
@@ -566,11 +566,11 @@ class FusedBatchSolver:
     for i, (ctx, n, rng) in enumerate(zip(contexts, ns, rngs)):
       seeds_all[i] = draw_row_seeds(rng, P)  # nearest_neighbor_init.py:118-121, random_init.py:42
       if self.init == "nn":
-        nn_tables.append(np.ascontiguousarray(ctx.get_cpu_candidate_list(self.nn_k), dtype=np.int32))
+        nn_tables.append(np.ascontiguousarray(candidate_list(ctx, self.nn_k), dtype=np.int32))
       t0 = time.perf_counter()
       ops = operands_for(ctx)
       dist, stride, coords = ops.distance_args(n, self.max_matrix_dimension)
-      tabs = ops.candidates(k, ctx.get_cpu_candidate_list(k), n, self.max_matrix_dimension)
+      tabs = ops.candidates(k, candidate_list(ctx, k), n, self.max_matrix_dimension)
       if tabs.packed is None:
         raise ValueError(f"instance {i}: k-NN table does not pack into 16-bit ids and distances")
       t_ops += time.perf_counter() - t0

@@ -275,6 +275,62 @@ class DeviceOperands:
     return tables
 
 
+def _host_knn_rows(context, rows: np.ndarray, k_eff: int) -> np.ndarray:
+  """Rows of the reference's k-NN table computed by its own procedure (`matrix.py:177-211`:
+  self masked with the largest int64, argpartition, then lexsort by (distance, id)).
+  NumPy partitions every row of a block independently, so a row's result does not depend
+  on the other rows of the block it is computed with."""
+  from .problem import distance_block
+
+  prob = context.problem
+  if getattr(prob, "distances", None) is not None:
+    block = np.asarray(prob.distances[rows], dtype=np.int64)
+  else:
+    c = np.asarray(prob.coordinates, dtype=np.float64)
+    block = distance_block(c[rows], c, getattr(prob, "edge_type", "EUC_2D")).astype(np.int64)
+  r = np.arange(len(rows))
+  block[r, rows] = np.iinfo(np.int64).max
+  cols = np.argpartition(block, k_eff, axis=1)[:, :k_eff]
+  cd = block[r[:, None], cols]
+  order = np.lexsort((cols, cd), axis=1)
+  return cols[r[:, None], order].astype(np.int32)
+
+
+def candidate_list(context, k: int) -> np.ndarray:
+  """The context's k-NN table `get_cpu_candidate_list(k)` (`problem_context.py:420-454`),
+  built on the device: `tspb_knn_ties` gives every row ordered by (distance, id) and flags
+  the rows with a tie at the k-th boundary, the only rows where the reference's
+  argpartition may pick other tied nodes; those rows are taken from the reference's own
+  procedure on the host. The table is stored in the context's candidate cache, so the
+  host API and every strategy bound to the context see the same table."""
+  cache = getattr(context, "_cpu_candidate_lists", None)
+  if cache is not None and k in cache:
+    return cache[k]
+  n = int(context.dimension)
+  prob = context.problem
+  usable = (cache is not None and n > 1 and 0 < k and min(k, n - 1) + 1 <= 64
+            and (getattr(prob, "distances", None) is not None or getattr(prob, "coordinates", None) is not None))
+  if not usable:
+    return context.get_cpu_candidate_list(k)
+  from .native import call
+
+  k_eff = min(k, n - 1)
+  ops = operands_for(context)
+  dist, stride, coords = ops.distance_args(n, None)
+  out = torch.empty((n, k_eff), dtype=torch.int32, device="cuda")
+  ties = torch.zeros(n, dtype=torch.int32, device="cuda")
+  if k_eff == n - 1:  # every other node: no (k+1)-th entry, no boundary
+    call("tspb_knn", ptr(dist), stride, ptr(coords), n, k_eff, ptr(out), stream_handle())
+  else:
+    call("tspb_knn_ties", ptr(dist), stride, ptr(coords), n, k_eff, ptr(out), ptr(ties), stream_handle())
+  table = out.cpu().numpy()
+  tied = np.nonzero(ties.cpu().numpy())[0]
+  if tied.size:
+    table[tied] = _host_knn_rows(context, tied, k_eff)
+  cache[k] = table
+  return table
+
+
 _operands: "weakref.WeakKeyDictionary[Any, DeviceOperands]" = weakref.WeakKeyDictionary()
 
 

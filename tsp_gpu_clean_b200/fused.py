@@ -45,7 +45,7 @@ from typing import Any
 import numpy as np
 
 from . import native
-from .device import auto_threads, operands_for, ptr, require_gpu, stream_handle, torch
+from .device import auto_threads, candidate_list, operands_for, ptr, require_gpu, stream_handle, torch
 from .problem import resolve_rng
 from .routes import sample_distinct_pairs
 from .strategies.initialization import InitializationB200TourNearestNeighbor
@@ -253,7 +253,7 @@ class FusedMemeticSolver:
     self.k = 0
     ls = self.ls
     if ls.candidate_k:
-      tabs = ops.candidates(int(ls.candidate_k), context.get_cpu_candidate_list(int(ls.candidate_k)), n,
+      tabs = ops.candidates(int(ls.candidate_k), candidate_list(context, int(ls.candidate_k)), n,
                             self.max_matrix_dimension)
       self.cand, self.cand_dist, self.packed, self.k = tabs.cand, tabs.cand_dist, tabs.packed, tabs.k
     lib = native.load_library()

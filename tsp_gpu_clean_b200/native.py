@@ -62,6 +62,7 @@ SIGNATURES: dict[str, tuple] = {
   "tspb_generation_elite_cost": (ctypes.c_int, [_p, _i32, _i32, _p, _i64, _p, _p, _p, _p]),
   "tspb_generation_track": (ctypes.c_int, [_p, _p, _i32, _i32, _p, _p, _p, _i64, _p, _p, _p, _p, _p]),
   "tspb_knn": (ctypes.c_int, [_p, _i64, _p, _i32, _i32, _p, _p]),
+  "tspb_knn_ties": (ctypes.c_int, [_p, _i64, _p, _i32, _i32, _p, _p, _p]),
   "tspb_mlp_param_count": (ctypes.c_int, []),
   "tspb_edge_features": (ctypes.c_int, [_p, _i32, _p, _i32, _p, _i64, _p, _p, _p, _p]),
   "tspb_mlp_infer": (ctypes.c_int, [_p, _p, _i64, _p, _p]),

@@ -19,7 +19,7 @@ from typing import Any
 import numpy as np
 
 from .. import native
-from ..device import device_tensor, ptr, require_gpu, stream_handle, torch
+from ..device import candidate_list, device_tensor, ptr, require_gpu, stream_handle, torch
 from ..phase_timer import time_strategy
 from ..problem import resolve_rng
 from .base import StrategyBase
@@ -57,7 +57,7 @@ class InitializationB200TourNearestNeighbor(StrategyBase):
     if population_size == 0 or n == 0:
       empty = torch.empty((population_size, n), dtype=torch.int32, device="cuda")
       return empty if self.return_gpu else np.empty((population_size, n), dtype=np.int32)
-    cand = np.ascontiguousarray(context.get_cpu_candidate_list(self.k), dtype=np.int32)
+    cand = np.ascontiguousarray(candidate_list(context, self.k), dtype=np.int32)
     rows, kk = (cand.shape[0], cand.shape[1]) if cand.ndim == 2 else (0, 0)
     max_node = int(cust.max())
     d_cust = device_tensor(cust, torch.int32)

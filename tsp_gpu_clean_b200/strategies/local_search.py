@@ -21,7 +21,17 @@ from typing import Any
 import numpy as np
 
 from .. import native
-from ..device import PinnedStager, Workspace, auto_threads, operands_for, ptr, require_gpu, stream_handle, torch
+from ..device import (
+  PinnedStager,
+  Workspace,
+  auto_threads,
+  candidate_list,
+  operands_for,
+  ptr,
+  require_gpu,
+  stream_handle,
+  torch,
+)
 from ..errors import NotPermutationError
 from ..phase_timer import time_strategy
 from ..routes import ensure_routes_batch, restore_shape
@@ -80,7 +90,7 @@ class LocalSearchB200TourTwoOpt(StrategyBase):
       return None
     if str(context.problem.problem_type) in {"CVRP", "OVRP", "DCVRP"}:
       return None
-    table = context.get_cpu_candidate_list(k)
+    table = candidate_list(context, k)
     if host_batch is not None and host_batch.size and int(host_batch.max()) >= table.shape[0]:
       return None
     return table

@@ -24,7 +24,17 @@ from typing import Any
 import numpy as np
 
 from .. import native
-from ..device import PinnedStager, device_tensor, is_device_array, operands_for, ptr, require_gpu, stream_handle, torch
+from ..device import (
+  PinnedStager,
+  candidate_list,
+  device_tensor,
+  is_device_array,
+  operands_for,
+  ptr,
+  require_gpu,
+  stream_handle,
+  torch,
+)
 from ..errors import NotPermutationError
 from ..phase_timer import time_strategy
 from ..problem import resolve_rng
@@ -267,7 +277,7 @@ class MutationB200PermInversion(StrategyBase):
 
   def _candidate_positions(self, rng, batch, low, high, context):
     """Second cut from a k-NN neighbour of the first city (`route_helpers.py:183-231`)."""
-    cand = context.get_cpu_candidate_list(self.candidate_k)
+    cand = candidate_list(context, self.candidate_k)
     host = batch.cpu().numpy() if is_device_array(batch) else np.asarray(batch)
     num = host.shape[0]
     pos1 = np.zeros(num, dtype=np.int32)
