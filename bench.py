@@ -223,8 +223,11 @@ def run_gpu(args, pool) -> dict | None:
   dist_t, stride, _ = ops.distance_args(n)
   tabs = ops.candidates(K_CAND, ctx.get_cpu_candidate_list(K_CAND), n)
   k = tabs.k
-  rev_off = tabs.rev_off if args.kernel == "cached" else None
-  rev_idx = tabs.rev_idx if args.kernel == "cached" else None
+  # the reverse index selects the cached kernel, or (with the packed table) the incremental
+  # restart of the scan kernel's first mode
+  use_rev = args.kernel == "cached" or (args.kernel == "scan" and args.first_restart == "incremental")
+  rev_off = tabs.rev_off if use_rev else None
+  rev_idx = tabs.rev_idx if use_rev else None
   packed = tabs.packed if args.kernel == "scan" else None
   pristine = torch.from_numpy(tours_np).cuda()
   work = torch.empty_like(pristine)
@@ -281,6 +284,7 @@ def run_gpu(args, pool) -> dict | None:
                                               threads_per_block=args.threads) for m in modes}
   for s_ in strategies.values():
     s_.kernel = args.kernel
+    s_.incremental_first = args.first_restart == "incremental"
   for m in modes:
     strategies[m].improve_batch(tours_np, ctx)  # warm
   torch.cuda.synchronize()
@@ -758,6 +762,8 @@ def main(argv=None) -> int:
   ap.add_argument("--mode", default="both", choices=["both", "best", "first"])
   ap.add_argument("--threads", type=int, default=128)
   ap.add_argument("--kernel", default="scan", choices=["scan", "scan_unpacked", "cached"])
+  ap.add_argument("--first-restart", default="incremental", choices=["incremental", "full"],
+                  help="first mode: restart each pass from the affected entries and row bi, or rescan from entry 0")
   ap.add_argument("--cpu-workers", type=int, default=0, help="0: all host cores, capped at 64")
   ap.add_argument("--no-cpu-baseline", action="store_true")
   ap.add_argument("--workload", default="two_opt", choices=["two_opt", "learned", "uneven", *GA_WORKLOADS])

@@ -57,10 +57,14 @@ size_t tspb_two_opt_workspace_bytes(int32_t num_tours, int32_t n, int32_t k, int
  * Cyclic TSP topology. `cand` (n x k, k-NN table) selects candidate mode; NULL selects
  * the exhaustive scan. `cand_dist` (n x k, optional) holds d(a, cand[a][r]).
  * Candidate best/first run the rescan kernel (block sizes 64, 128, 256 or 512) unless
- * `rev_off`/`rev_idx` (from tspb_candidate_reverse_index) are given, which select the
- * cached kernel: per-row keys and pair counts kept exactly across passes and refreshed
- * only where a reversal can change them. `cand_packed` (optional, from
- * tspb_candidate_pack) lets the rescan kernel read id and distance in one word.
+ * `rev_off`/`rev_idx` (from tspb_candidate_reverse_index) are given without
+ * `cand_packed`, which selects the cached kernel: per-row keys and pair counts kept
+ * exactly across passes and refreshed only where a reversal can change them.
+ * `cand_packed` (optional, from tspb_candidate_pack) lets the rescan kernel read id and
+ * distance in one word; given together with `rev_off`/`rev_idx`, first mode restarts
+ * incrementally: after a move with window [bi, bj] a pass evaluates only the entries of
+ * rows before bi whose candidate lies in the window, then scans from row bi (the other
+ * entries before bi cannot have changed). Results and stats[0..2] are the same either way.
  * Distances come from `dist` when non-NULL, else are rebuilt from `coords` in FP64
  * with TSPLIB EUC_2D rounding. `max_iterations` bounds the passes per tour.
  * `stats` (optional, num_tours x 4 int64): passes, pairs evaluated by the reference

@@ -247,3 +247,44 @@ def test_table_layouts_agree(b200, mode, k, threads):
   want, st = _LAYOUT_ORACLE[key]
   assert np.array_equal(outs[1][0], want)
   assert np.array_equal(outs[1][1][:, :3], st)
+
+
+@pytest.mark.parametrize("k,threads", [(20, 128), (8, 256), (7, 64), (12, 512)])
+@pytest.mark.parametrize("max_iter", [10**9, 37])
+def test_first_mode_incremental_restart_matches_full_rescan(b200, k, threads, max_iter):
+  """First mode restarting from the affected entries and the move's row gives the tours
+  and pass/pair/move counts of the full rescan from entry 0 and of the oracle, on a
+  clustered, a uniform and a tie-heavy lattice instance, with grouped (k % 4 == 0) and
+  plain packed tables."""
+  import torch
+
+  from tsp_gpu_clean_b200 import native
+  from tsp_gpu_clean_b200.device import operands_for, ptr, stream_handle
+
+  side = 17
+  lattice = np.array([[5.0 * x, 5.0 * y] for x in range(side) for y in range(side)])
+  for coords in (instances.clustered_instance(300, 10, 30.0, 71), instances.uniform_instance(180, 72), lattice):
+    n, T = len(coords), 12
+    tours = instances.random_tours(n, T, 73 + n)
+    ctx = _ctx(b200, coords=coords)
+    ops = operands_for(ctx)
+    dist, stride, _ = ops.distance_args(n, None)
+    tabs = ops.candidates(k, ctx.get_cpu_candidate_list(k), n, None)
+    lib = native.load_library()
+    outs = []
+    for rev in (False, True):
+      work = torch.from_numpy(tours).cuda()
+      stats = torch.zeros((T, 4), dtype=torch.int64, device="cuda")
+      status = torch.zeros(T, dtype=torch.int32, device="cuda")
+      rc = lib.tspb_two_opt(ptr(work), T, n, ptr(dist), stride, None, ptr(tabs.cand), ptr(tabs.cand_dist),
+                            ptr(tabs.rev_off) if rev else None, ptr(tabs.rev_idx) if rev else None, ptr(tabs.packed),
+                            tabs.k, native.MODE_CODES["first"], max_iter, threads, ptr(stats), ptr(status), None, 0,
+                            stream_handle())
+      native.check("tspb_two_opt", rc)
+      assert int(status.max().item()) == 0
+      outs.append((work.cpu().numpy(), stats.cpu().numpy()))
+    assert np.array_equal(outs[0][0], outs[1][0]), n
+    assert np.array_equal(outs[0][1][:, :3], outs[1][1][:, :3]), n
+    want, st = otwo.improve_batch(tours, odist.euc2d_matrix(coords), ctx.get_cpu_candidate_list(k), "first", max_iter)
+    assert np.array_equal(outs[1][0], want), n
+    assert np.array_equal(outs[1][1][:, :3], st), n

@@ -489,7 +489,8 @@ static int two_opt_impl(int32_t* tours, int32_t num_tours, int32_t n, const int3
   if (dist != nullptr && dist_stride < n) return TSPB_ERR_ARG;
   int threads = block_threads > 0 ? block_threads : 256;
   if (threads % 32 != 0 || threads > 1024) return TSPB_ERR_ARG;
-  if (use_cand && mode != TSPB_MODE_MULTI_MOVE && (rev_off == nullptr || rev_idx == nullptr)) {
+  const bool has_rev = rev_off != nullptr && rev_idx != nullptr;
+  if (use_cand && mode != TSPB_MODE_MULTI_MOVE && (!has_rev || cand_packed != nullptr)) {
     if (threads != 64 && threads != 128 && threads != 256 && threads != 512) return TSPB_ERR_ARG;
     const size_t need = two_opt_scan_tour_bytes(n, mode);
     const size_t per = need <= (size_t)smem_optin() - 2048 ? 0 : align256(need);
@@ -513,6 +514,10 @@ static int two_opt_impl(int32_t* tours, int32_t num_tours, int32_t n, const int3
     c.ws_tour_bytes = per;
     c.arrays_in_smem = per == 0 ? 1 : 0;
     c.skip = skip;
+    if (has_rev && mode == TSPB_MODE_FIRST) {  // incremental restart of first mode
+      c.rev_off = rev_off;
+      c.rev_idx = rev_idx;
+    }
     return launch_two_opt_scan(c, mode, threads, st);
   }
   if (use_cand && rev_off != nullptr && rev_idx != nullptr && mode != TSPB_MODE_MULTI_MOVE) {

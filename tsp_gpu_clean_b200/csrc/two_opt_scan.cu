@@ -34,6 +34,8 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value) two_op
   T.accumulate = 0;
   T.moved = nullptr;
   T.converged = nullptr;
+  T.rev_off = A.rev_off;
+  T.rev_idx = A.rev_idx;
   scan_tour<MODE, THREADS, U, LAYOUT>(T, S);
 }
 

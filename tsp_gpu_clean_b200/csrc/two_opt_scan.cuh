@@ -17,6 +17,14 @@
 // best keeps a per-thread (gain, i*k + r) minimum and reduces once per pass. first
 // publishes the smallest improving index of a round with a shared atomicMin; once set,
 // later rounds only count the pairs the reference still evaluates (validity, no gains).
+//
+// first with the reverse k-NN index (incremental restart): the reference restarts every
+// pass at entry 0. After a move with window [bi, bj] (the first improving entry was in row
+// bi, so every entry before it was non-improving), an entry (i, r) of a row i < bi keeps
+// a = t[i], succ[a] and eout[a]; it changes only when its candidate c lies in positions
+// [bi, bj], where pos/succ/eout of c may have changed. The next pass therefore evaluates
+// just those affected entries (found through the reverse index) and, when none improves,
+// scans from row bi on: the first improving entry it finds is the reference's.
 #pragma once
 
 #include "two_opt.cuh"
@@ -58,6 +66,8 @@ struct ScanTour {
   int32_t* moved;    // optional: 1 when at least one move was applied, else 0
   uint8_t* converged;  // optional: 1 when the refinement ended on a pass without an improving
                        // move (the tour is then a fixed point of any further refinement)
+  const int32_t* rev_off = nullptr;  // optional (first mode): CSR reverse k-NN index, n + 1 offsets
+  const int32_t* rev_idx = nullptr;  // flat entries a * k + r grouped by candidate node
 };
 
 // k-NN table layouts of scan_tour: plain int32 candidates (+ optional distances), packed
@@ -182,6 +192,8 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
   int err = TSPB_OK;
   bool converged = false;  // the last pass found no improving move: a local optimum
   const long long t_start = clock64();
+  const bool incremental = MODE == TSPB_MODE_FIRST && T.rev_off != nullptr && T.rev_idx != nullptr;
+  int win_lo = -1, win_hi = -1;  // window [bi, bj] of the last move (incremental first mode)
 
   while (passes < T.max_iter) {
     if (tid == 0) {
@@ -198,10 +210,39 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
     int bgain = 0;            // best: smallest gain of this thread (strictly below 0 to count)
     unsigned bidx = NO_IDX;   // and its scan index (first in thread order wins ties)
     int cnt = 0, evals = 0;
-    if constexpr (GROUPED) {
+    int start_row = 0;        // first row of this pass's scan
+    bool found = false;       // the affected entries already hold the first improving one
+    if (incremental && win_lo >= 0 && 2 * (win_hi - win_lo + 1) <= win_lo) {
+      // affected entries of rows < win_lo: candidate c at a position of the window
+      const int lane = tid & 31, wid = tid >> 5;
+      constexpr int NW = THREADS / 32;
+      for (int q = win_lo + wid; q <= win_hi; q += NW) {
+        const int c = tour[q];
+        const int s0 = __ldg(T.rev_off + c), s1 = __ldg(T.rev_off + c + 1);
+        const int sc = succ[c], ec = eout[c];
+        for (int sx = s0 + lane; sx < s1; sx += 32) {
+          const int e = __ldg(T.rev_idx + sx);
+          const int a = e / k;
+          const int i = pos[a];
+          if (i >= win_lo) continue;  // rows from win_lo on are scanned below
+          if ((unsigned)(q - (i + 2)) >= (unsigned)(n - (i == 0) - (i + 2))) continue;
+          ++evals;
+          const int dac = PACKED ? (int)(__ldg(packed + e) >> 16) : (cdist ? __ldg(cdist + e) : ds(a, c));
+          const int sa = succ[a];
+          const int dbd = dist ? __ldcg(dist + ((unsigned)sa * stride + (unsigned)sc)) : ds(sa, sc);
+          if ((dac - eout[a]) + (dbd - ec) < 0) atomicMin(&S.first, (unsigned)(i * k + (e - a * k)));
+        }
+      }
+      __syncthreads();
+      found = S.first != NO_IDX;
+      start_row = win_lo;
+    }
+    if (found) {
+      // nothing to scan: the smallest improving affected entry is the first of the pass
+    } else if constexpr (GROUPED) {
       // entries [e0 + tid*U, e0 + tid*U + U) of round e0 lie in row gi, columns gr..gr+U-1
-      int gi = g_row0, gr = g_col0;
-      for (int e0 = 0; e0 < E; e0 += STEP) {
+      int gi = g_row0 + start_row, gr = g_col0;
+      for (int e0 = start_row * k; e0 < E; e0 += STEP) {
         const int eb = e0 + tid * U;
         if (eb < E) {
           const int a = tour[gi];
@@ -253,11 +294,11 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
     int ri[U], rr[U], ee[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      ee[u] = u * THREADS + tid;
+      ee[u] = start_row * k + u * THREADS + tid;
       ri[u] = ee[u] / k;
       rr[u] = ee[u] - ri[u] * k;
     }
-    for (int e0 = 0; e0 < E; e0 += STEP) {
+    for (int e0 = start_row * k; e0 < E; e0 += STEP) {
       int a[U], c[U], cd[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) a[u] = ee[u] < E ? tour[ri[u]] : -1;
@@ -372,6 +413,8 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
     }
     __syncthreads();
     ++moves;
+    win_lo = bi;
+    win_hi = bj;
     if (MODE == TSPB_MODE_FIRST) {
       // Only rows [bi, bj] (and row 0 when bj == n-1) can change their valid count.
       const int r_hi = bj < rows - 1 ? bj : rows - 1;

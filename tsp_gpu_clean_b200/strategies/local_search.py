@@ -74,6 +74,9 @@ class LocalSearchB200TourTwoOpt(StrategyBase):
     #: (same kernel, separate id/distance arrays) or "cached" (exact incremental row keys).
     #: All give identical results; the choice is a performance knob.
     self.kernel = "scan"
+    #: first mode on the scan kernel: restart each pass from the entries a move can have
+    #: changed and the move's row (same results as rescanning from entry 0).
+    self.incremental_first = True
     self.last_stats: np.ndarray | None = None
     self._workspace = Workspace()
     self._stager = PinnedStager()
@@ -139,9 +142,10 @@ class LocalSearchB200TourTwoOpt(StrategyBase):
     cand = tabs.cand if tabs is not None else None
     cand_dist = tabs.cand_dist if tabs is not None else None
     cached = tabs is not None and self.kernel == "cached"
-    rev_off = tabs.rev_off if cached else None
-    rev_idx = tabs.rev_idx if cached else None
     packed = tabs.packed if tabs is not None and self.kernel == "scan" else None
+    use_rev = cached or (packed is not None and self.mode == "first" and self.incremental_first)
+    rev_off = tabs.rev_off if use_rev else None
+    rev_idx = tabs.rev_idx if use_rev else None
     native.call(
       "tspb_two_opt", ptr(d_tours), num, n, ptr(dist), stride, ptr(coords), ptr(cand), ptr(cand_dist), ptr(rev_off),
       ptr(rev_idx), ptr(packed), k, mode,
