@@ -221,6 +221,9 @@ def run_gpu(args, pool) -> dict | None:
   ctx = ProblemContext(Problem.from_coordinates(coords, "c2"), seed=0)
   ops = operands_for(ctx)
   dist_t, stride, _ = ops.distance_args(n)
+  coords_t = None
+  if args.distances == "coords":  # the same int32 EUC_2D values, rebuilt in FP64 from L1-resident coordinates
+    dist_t, stride, coords_t = None, 0, ops.coords()
   tabs = ops.candidates(K_CAND, ctx.get_cpu_candidate_list(K_CAND), n)
   k = tabs.k
   # the reverse index selects the cached kernel, or (with the packed table) the incremental
@@ -241,7 +244,8 @@ def run_gpu(args, pool) -> dict | None:
     for m in modes:
       work.copy_(pristine)
       ev_pairs[m][0].record(stream)
-      rc = lib.tspb_two_opt(ptr(work), args.tours, n, ptr(dist_t), stride, None, ptr(tabs.cand), ptr(tabs.cand_dist),
+      rc = lib.tspb_two_opt(ptr(work), args.tours, n, ptr(dist_t), stride, ptr(coords_t), ptr(tabs.cand),
+                            ptr(tabs.cand_dist),
                             ptr(rev_off), ptr(rev_idx), ptr(packed), k,
                             native.MODE_CODES[m], args.max_iter, args.threads, ptr(stats[m]), ptr(status), None, 0,
                             stream_handle())
@@ -762,6 +766,8 @@ def main(argv=None) -> int:
   ap.add_argument("--mode", default="both", choices=["both", "best", "first"])
   ap.add_argument("--threads", type=int, default=128)
   ap.add_argument("--kernel", default="scan", choices=["scan", "scan_unpacked", "cached"])
+  ap.add_argument("--distances", default="matrix", choices=["matrix", "coords"],
+                  help="two_opt: read the int32 matrix, or rebuild each distance from FP64 coordinates")
   ap.add_argument("--first-restart", default="incremental", choices=["incremental", "full"],
                   help="first mode: restart each pass from the affected entries and row bi, or rescan from entry 0")
   ap.add_argument("--cpu-workers", type=int, default=0, help="0: all host cores, capped at 64")
@@ -802,7 +808,8 @@ def main(argv=None) -> int:
                         "1000-city 20-cluster EUC_2D instance",
             "tours": args.tours, "n": instances.C2_N, "k": K_CAND, "modes": list(MODES if args.mode == "both" else (args.mode,)),
             "l2": "flushed between timed steps (256 MiB write); the 4 MB matrix is L2-resident within a step",
-            "threads_per_cta": args.threads, "kernel": args.kernel}
+            "threads_per_cta": args.threads, "kernel": args.kernel, "distances": args.distances,
+            "first_restart": args.first_restart}
 
   if args.impl == "reference":
     if rank != 0:
