@@ -50,7 +50,7 @@ L2_FLUSH_BYTES = 256 << 20
 #: DRAM bytes (read + write) of one launch of the default workload's scan kernels, from one
 #: ncu capture of this command (profiles/two_opt_scan_c2.md); only the default 1024-tour,
 #: 128-thread scan configuration has a captured figure.
-NCU_DRAM_BYTES_PER_LAUNCH = {"best": 8_746_240, "first": 9_101_056}
+NCU_DRAM_BYTES_PER_LAUNCH = {"best": 8_833_536, "first": 8_825_856}
 
 
 def _peaks() -> dict:
