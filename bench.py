@@ -441,7 +441,9 @@ def run_ga_bench(args) -> dict:
 
   def run_once():
     # replicas per rank: the same instance, each run's generator seeded per rank and repetition
-    ctxs = [ProblemContext(Problem.from_coordinates(coords), seed=42 + r + reps * rank) for r in range(reps)]
+    # like the reference's runner: one problem, one candidate cache, a context per repetition
+    problem, cache = Problem.from_coordinates(coords), {}
+    ctxs = [ProblemContext(problem, seed=42 + r + reps * rank, candidate_cache=cache) for r in range(reps)]
     ls = LocalSearchConfig("best", 10, 20)
     t0 = time.perf_counter()
     if args.engine == "batch":
@@ -613,6 +615,8 @@ def run_uneven_bench(args) -> dict:
                                   "two_opt_threads": b.two_opt_threads, "offspring_threads": b.offspring_threads}
                                  for b in solver.buckets],
                      "setup_s": solver.last_timing["setup_s"], "tune_s_total": tune_s,
+                     "last_run": {k: round(v, 4) for k, v in solver.last_timing.items() if isinstance(v, (int, float))},
+                     "walls_s": [round(w, 4) for w in walls],
                      "setup_parts_s": {k: round(solver.last_timing[k], 3)
                                        for k in ("setup_operands_s", "setup_tape_s", "setup_nn_init_s")}}}
 

@@ -71,9 +71,16 @@ def auto_threads(num_tours: int) -> int:
 
 
 def check_free(required_bytes: int, what: str) -> None:
+  """Raise VRAMInsufficientError before an allocation that cannot succeed. Memory that
+  torch's caching allocator already holds unused is counted first (host-side counters);
+  the driver is asked for free memory only when that does not cover the request."""
+  cached = torch.cuda.memory_reserved() - torch.cuda.memory_allocated()
+  if required_bytes <= cached:
+    return
   free, _ = torch.cuda.mem_get_info()
-  if required_bytes > free:
-    raise VRAMInsufficientError(f"Insufficient VRAM for {what}", required_bytes=required_bytes, available_bytes=free)
+  if required_bytes > free + cached:
+    raise VRAMInsufficientError(f"Insufficient VRAM for {what}", required_bytes=required_bytes,
+                                available_bytes=free + cached)
 
 
 class PinnedStager:
@@ -147,13 +154,26 @@ class DeviceOperands:
   """
 
   def __init__(self, context):
-    self.context = context
+    # weak: the operands live in a WeakKeyDictionary keyed by the context, so a strong
+    # reference here would keep every context (and its device matrices) alive for good
+    self._context_ref = weakref.ref(context)
     self.h2d_bytes = 0
     self._dist = None
     self._coords = None
-    self._cand: dict[int, tuple] = {}
+    # contexts of one Problem object (repetitions of a run) share its device data
+    self._shared = _problem_cache(context)
+    self._cand: dict[int, tuple] = self._shared.setdefault("cand", {}) if self._shared is not None else {}
+
+  @property
+  def context(self):
+    ctx = self._context_ref()
+    if ctx is None:
+      raise RuntimeError("the problem context of these device operands no longer exists")
+    return ctx
 
   def coords(self):
+    if self._coords is None and self._shared is not None:
+      self._coords = self._shared.get("coords")
     if self._coords is None:
       c = self.context.get_cpu_coordinates()
       if c is None:
@@ -166,9 +186,20 @@ class DeviceOperands:
         raise ValueError("coordinates too large for exact int32 gains")
       self._coords = device_tensor(c, torch.float64)
       self.h2d_bytes += self._coords.numel() * 8
+      if self._shared is not None:
+        self._shared["coords"] = self._coords
     return self._coords
 
   def dist(self):
+    if self._dist is None and self._shared is not None:
+      self._dist = self._shared.get("dist")
+    if self._dist is None:
+      self._dist = self._build_dist()
+      if self._shared is not None:
+        self._shared["dist"] = self._dist
+    return self._dist
+
+  def _build_dist(self):
     if self._dist is None and self._euc2d_on_device():
       # The matrix of an EUC_2D coordinate problem is built in HBM from the coordinates with
       # the reference's rounding (compute_distance_matrix, matrix.py:214-273): only the
@@ -332,6 +363,19 @@ def candidate_list(context, k: int) -> np.ndarray:
 
 
 _operands: "weakref.WeakKeyDictionary[Any, DeviceOperands]" = weakref.WeakKeyDictionary()
+_problems: "weakref.WeakKeyDictionary[Any, dict]" = weakref.WeakKeyDictionary()
+
+
+def _problem_cache(context) -> dict | None:
+  """Device data shared by the contexts of one Problem object, or None when the problem
+  cannot be weakly referenced."""
+  prob = getattr(context, "problem", None)
+  if prob is None:
+    return None
+  try:
+    return _problems.setdefault(prob, {})
+  except TypeError:
+    return None
 
 
 def operands_for(context) -> DeviceOperands:
