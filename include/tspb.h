@@ -257,6 +257,11 @@ typedef struct tspb_nn_job {
 } tspb_nn_job;
 int tspb_nn_init_jobs(const tspb_nn_job* jobs, int32_t num_jobs, int32_t max_rows, int32_t* workspace,
                       const int64_t* ws_offsets, void* stream);
+/* The same tours with every row's working arrays in shared memory (no workspace): max_n
+ * and max_k bound every job's n and k; TSPB_ERR_UNSUPPORTED when 4 max_n + 2 max_k bytes
+ * exceed 200 KB or max_n > 65535 (use tspb_nn_init_jobs then). */
+int tspb_nn_init_jobs_smem(const tspb_nn_job* jobs, int32_t num_jobs, int32_t max_rows, int32_t max_n, int32_t max_k,
+                           void* stream);
 
 /*
  * Exhaustive steepest-descent 3-opt of open (cyclic TSP) tours in place, up to

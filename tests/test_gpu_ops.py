@@ -148,3 +148,50 @@ def test_nn_init_matches_reference(torch_mod, golden):
   ctx3 = _ctx(g["c3_coords"], 42)
   pop3 = InitializationB200TourNearestNeighbor(k=5, seed=42, return_gpu=True).initialize(list(range(2000)), 512, ctx3)
   assert hashlib.sha256(pop3.cpu().numpy().astype(np.int32).tobytes()).hexdigest() == str(g["c3_init_digest"])
+
+
+def test_nn_init_jobs_shared_memory_matches_workspace_kernel(torch_mod):
+  """Nearest-neighbour rows built with the working arrays in shared memory equal the
+  workspace kernel's, for jobs of different sizes and k (k = 0: uniform choices only)."""
+  import ctypes
+
+  from tsp_gpu_clean_b200 import native
+  from tsp_gpu_clean_b200.device import ptr, stream_handle
+
+  torch = torch_mod
+  specs = [(4, 3), (7, 0), (500, 5), (5000, 5), (1200, 12)]
+  rows = 9
+  rng = np.random.default_rng(3)
+  tabs = [odist.candidate_list(k, coords=instances.uniform_instance(n, n)) if k else np.zeros((n, 0), np.int32)
+          for n, k in specs]
+  d_cand = [torch.from_numpy(np.ascontiguousarray(t).reshape(-1).copy() if t.size else np.zeros(1, np.int32)).cuda()
+            for t in tabs]
+  seeds = rng.integers(0, 2**62, (len(specs), rows), dtype=np.int64)
+  d_seeds = torch.from_numpy(seeds).cuda()
+  outs = [[torch.full((rows, n), -1, dtype=torch.int32, device="cuda") for n, _ in specs] for _ in range(2)]
+
+  def jobs_for(which):
+    h = (native.NNJob * len(specs))()
+    for i, ((n, k), c) in enumerate(zip(specs, d_cand)):
+      h[i].n, h[i].k, h[i].rows = n, k, rows
+      h[i].cand = c.data_ptr()
+      h[i].seeds = d_seeds.data_ptr() + i * rows * 8
+      h[i].out = outs[which][i].data_ptr()
+    return torch.frombuffer(bytearray(h), dtype=torch.uint8).cuda()
+
+  j0, j1 = jobs_for(0), jobs_for(1)
+  per = [rows * (2 * n + k) for n, k in specs]
+  off = np.concatenate([[0], np.cumsum(per)[:-1]]).astype(np.int64)
+  ws = torch.empty(int(sum(per)), dtype=torch.int32, device="cuda")
+  d_off = torch.from_numpy(off).cuda()
+  native.call("tspb_nn_init_jobs", ptr(j0), len(specs), rows, ptr(ws), ptr(d_off), stream_handle())
+  native.call("tspb_nn_init_jobs_smem", ptr(j1), len(specs), rows, max(n for n, _ in specs),
+              max(k for _, k in specs), stream_handle())
+  for (n, _), a, b in zip(specs, outs[0], outs[1]):
+    a, b = a.cpu().numpy(), b.cpu().numpy()
+    assert np.array_equal(a, b), n
+    assert (np.sort(a, axis=1) == np.arange(n)).all()
+  lib = native.load_library()
+  assert lib.tspb_nn_init_jobs_smem(ptr(j1), 1, 1, 70000, 5, None) == native.TSPB_ERR_UNSUPPORTED
+  assert lib.tspb_nn_init_jobs_smem(None, 1, 1, 100, 5, None) == native.TSPB_ERR_ARG
+  del ctypes

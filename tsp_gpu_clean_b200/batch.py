@@ -468,7 +468,8 @@ class FusedBatchSolver:
 
   def _nn_init(self, h_jobs, seeds_all: np.ndarray, tables: list, ns: list[int]) -> None:
     """GRASP nearest-neighbour populations of every instance in one launch
-    (`tspb_nn_init_jobs`, each row as `InitializationCPUTourNearestNeighbor` builds it)."""
+    (`tspb_nn_init_jobs_smem`, or `tspb_nn_init_jobs` for rows too large for shared memory;
+    each row as `InitializationCPUTourNearestNeighbor` builds it)."""
     P = self.P
     ks = [int(t.shape[1]) if t.ndim == 2 else 0 for t in tables]
     cand_off = np.zeros(self.I + 1, dtype=np.int64)
@@ -478,10 +479,6 @@ class FusedBatchSolver:
       flat[cand_off[i]: cand_off[i + 1]] = t.reshape(-1)
     d_cand = torch.from_numpy(flat).cuda()
     d_seeds = torch.from_numpy(seeds_all.view(np.int64)).cuda()
-    ws_off = np.zeros(self.I + 1, dtype=np.int64)
-    ws_off[1:] = np.cumsum([P * (2 * n + k) for n, k in zip(ns, ks)])
-    d_ws = torch.empty(max(int(ws_off[-1]), 1), dtype=torch.int32, device="cuda")
-    d_ws_off = torch.from_numpy(ws_off[:-1].copy()).cuda()
     for i, (n, k) in enumerate(zip(ns, ks)):
       job = h_jobs[i]
       job.n, job.k, job.rows = n, k, P
@@ -489,7 +486,16 @@ class FusedBatchSolver:
       job.seeds = d_seeds.data_ptr() + i * P * 8
       job.out = self.pop[0].data_ptr() + self.pop_offsets[i] * 4
     d_jobs = torch.frombuffer(bytearray(h_jobs), dtype=torch.uint8).cuda()
-    native.call("tspb_nn_init_jobs", ptr(d_jobs), self.I, P, ptr(d_ws), ptr(d_ws_off), stream_handle())
+    # every row's working arrays in shared memory when they fit, else a global workspace
+    rc = native.load_library().tspb_nn_init_jobs_smem(ptr(d_jobs), self.I, P, max(ns), max(ks), stream_handle())
+    if rc == native.TSPB_ERR_UNSUPPORTED:
+      ws_off = np.zeros(self.I + 1, dtype=np.int64)
+      ws_off[1:] = np.cumsum([P * (2 * n + k) for n, k in zip(ns, ks)])
+      d_ws = torch.empty(max(int(ws_off[-1]), 1), dtype=torch.int32, device="cuda")
+      d_ws_off = torch.from_numpy(ws_off[:-1].copy()).cuda()
+      native.call("tspb_nn_init_jobs", ptr(d_jobs), self.I, P, ptr(d_ws), ptr(d_ws_off), stream_handle())
+    else:
+      native.check("tspb_nn_init_jobs_smem", rc)
     torch.cuda.current_stream().synchronize()  # the host buffers above are released on return
     self.kernel_launches += 1
 

@@ -149,6 +149,73 @@ __global__ void nn_init_jobs_kernel(const tspb_nn_job* __restrict__ jobs, int nu
   }
 }
 
+// The jobs kernel with each row's unvisited list, position map and rank order in shared
+// memory (16-bit entries: 4 n + 2 k bytes per row): the walk's dependent accesses become
+// shared-memory accesses instead of L2/HBM round trips. One warp per (job, row): the warp
+// fills the arrays, lane 0 walks exactly as nn_init_jobs_kernel does.
+__global__ void __launch_bounds__(32) nn_init_jobs_smem_kernel(const tspb_nn_job* __restrict__ jobs, int num_jobs,
+                                                               int stride_u16) {
+  extern __shared__ __align__(16) uint16_t smu[];
+  const int j = blockIdx.y;
+  if (j >= num_jobs) return;
+  const tspb_nn_job J = jobs[j];
+  const int row = blockIdx.x;
+  if (row >= J.rows) return;
+  const int n = J.n, k = J.k;
+  if (n <= 0) return;
+  uint16_t* unv = smu;
+  uint16_t* pmap = smu + stride_u16;
+  uint16_t* order = pmap + stride_u16;
+  for (int q = threadIdx.x; q < n; q += 32) {
+    unv[q] = (uint16_t)q;
+    pmap[q] = (uint16_t)q;
+  }
+  __syncwarp();
+  if (threadIdx.x != 0) return;
+  int32_t* dst = J.out + (long long)row * n;
+  unsigned long long st = J.seeds[row];
+  int rem = n;
+  int s = (int)splitmix64_bounded(st, (unsigned)rem);
+  int cur = unv[s];
+  dst[0] = cur;
+  int last = rem - 1;
+  int ln = unv[last];
+  unv[s] = (uint16_t)ln;
+  unv[last] = (uint16_t)cur;
+  pmap[ln] = (uint16_t)s;
+  pmap[cur] = (uint16_t)last;
+  rem = last;
+  for (int step = 1; step < n; ++step) {
+    int chosen = -1;
+    if (k > 0) {
+      for (int i = 0; i < k; ++i) order[i] = (uint16_t)i;
+      const int32_t* crow = J.cand + (long long)cur * k;
+      for (int i = 0; i < k; ++i) {
+        const int jj = i + (int)splitmix64_bounded(st, (unsigned)(k - i));
+        const uint16_t tmp = order[i];
+        order[i] = order[jj];
+        order[jj] = tmp;
+        const int nb = __ldg(crow + order[i]);
+        if (nb >= 0 && nb < n && (int)pmap[nb] < rem) {
+          chosen = nb;
+          break;
+        }
+      }
+    }
+    if (chosen < 0) chosen = unv[(int)splitmix64_bounded(st, (unsigned)rem)];
+    dst[step] = chosen;
+    const int p = pmap[chosen];
+    last = rem - 1;
+    ln = unv[last];
+    unv[p] = (uint16_t)ln;
+    unv[last] = (uint16_t)chosen;
+    pmap[ln] = (uint16_t)p;
+    pmap[chosen] = (uint16_t)last;
+    rem = last;
+    cur = chosen;
+  }
+}
+
 }  // namespace tspb
 
 using namespace tspb;
@@ -163,6 +230,22 @@ extern "C" int tspb_nn_init_jobs(const tspb_nn_job* jobs, int32_t num_jobs, int3
   const dim3 grid((max_rows + threads - 1) / threads, num_jobs);
   nn_init_jobs_kernel<<<grid, threads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
       jobs, num_jobs, workspace, reinterpret_cast<const long long*>(ws_offsets));
+  return tspb_launch_status();
+}
+
+extern "C" int tspb_nn_init_jobs_smem(const tspb_nn_job* jobs, int32_t num_jobs, int32_t max_rows, int32_t max_n,
+                                      int32_t max_k, void* stream) {
+  if (num_jobs < 0 || max_rows < 0 || max_n < 0 || max_k < 0) return TSPB_ERR_ARG;
+  if (num_jobs == 0 || max_rows == 0 || max_n == 0) return TSPB_OK;
+  if (!jobs) return TSPB_ERR_ARG;
+  if (num_jobs > 65535 || max_n > 65535) return TSPB_ERR_UNSUPPORTED;
+  const int stride = (max_n + 7) & ~7;  // 16-byte aligned sub-arrays
+  const size_t smem = (size_t)2 * (2 * (size_t)stride + (size_t)((max_k + 7) & ~7));
+  if (smem > 200 * 1024) return TSPB_ERR_UNSUPPORTED;
+  if (smem > 48 * 1024)
+    TSPB_CUDA_CHECK(cudaFuncSetAttribute(nn_init_jobs_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  nn_init_jobs_smem_kernel<<<dim3(max_rows, num_jobs), 32, smem, reinterpret_cast<cudaStream_t>(stream)>>>(
+      jobs, num_jobs, stride);
   return tspb_launch_status();
 }
 

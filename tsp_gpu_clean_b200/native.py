@@ -72,6 +72,7 @@ SIGNATURES: dict[str, tuple] = {
   "tspb_select_topk": (ctypes.c_int, [_p, _p, _i32, _i32, _i32, _p, _p]),
   "tspb_nn_init": (ctypes.c_int, [_p, _i32, _p, _i32, _i32, _p, _i32, _i32, _p, _sz, _p, _p]),
   "tspb_nn_init_jobs": (ctypes.c_int, [_p, _i32, _i32, _p, _p, _p]),
+  "tspb_nn_init_jobs_smem": (ctypes.c_int, [_p, _i32, _i32, _i32, _i32, _p]),
   "tspb_random_init": (ctypes.c_int, [_p, _i32, _i32, _p, _p, _p]),
   "tspb_distance_matrix": (ctypes.c_int, [_p, _i32, _i32, _i32, _p, _i64, _p]),
   "tspb_three_opt": (ctypes.c_int, [_p, _i32, _i32, _p, _i64, _p, _i64, _i32, _p, _sz, _p, _p, _p]),
