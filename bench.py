@@ -485,7 +485,7 @@ def run_ga_bench(args) -> dict:
           "e2e": {"value": e2e_units / wall_s, "unit": "generations/s", "h2d_bytes_per_step": int(reps * coords.nbytes),
                   "d2h_bytes_per_step": int(reps * (n * 4 + (G + 1) * 8 + P * n * 4))},
           "gpu_launches": launches, "desc": desc, "best": stats["best_fitness"],
-          "loop_ms_steps": [round(v, 3) for v in loop_ms],
+          "loop_ms_steps": [round(v, 3) for v in loop_ms], "walls_s": [round(w, 4) for w in walls],
           "timing": {k: round(v, 4) for k, v in solver.last_timing.items() if isinstance(v, (int, float))}}
 
 
@@ -895,7 +895,7 @@ def main_ga(args) -> int:
           "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)", "config": config, "clocks": res["clocks"],
           "e2e": res["e2e"], "gpu_launches": res["gpu_launches"],
           "detail": {"best_fitness": res["best"], "engine": args.engine, "last_run": res["timing"],
-                     "loop_ms_steps": res["loop_ms_steps"]}}
+                     "loop_ms_steps": res["loop_ms_steps"], "walls_s": res["walls_s"]}}
   if res["world"] > 1:
     config["parallelism"] = f"{res['world']} independent replicas (one GA run per GPU, generator seeded per rank)"
   if not args.no_cpu_baseline and res["world"] == 1:

@@ -306,16 +306,19 @@ class DeviceOperands:
     return tables
 
 
-def _host_knn_rows(context, rows: np.ndarray, k_eff: int) -> np.ndarray:
+def _host_knn_rows(context, rows: np.ndarray, k_eff: int, dist=None) -> np.ndarray:
   """Rows of the reference's k-NN table computed by its own procedure (`matrix.py:177-211`:
   self masked with the largest int64, argpartition, then lexsort by (distance, id)).
   NumPy partitions every row of a block independently, so a row's result does not depend
-  on the other rows of the block it is computed with."""
+  on the other rows of the block it is computed with. The rows' distances come from the
+  device matrix `dist` when given (the same values), else from the host formula."""
   from .problem import distance_block
 
   prob = context.problem
   if getattr(prob, "distances", None) is not None:
     block = np.asarray(prob.distances[rows], dtype=np.int64)
+  elif dist is not None:
+    block = dist[torch.from_numpy(rows).to(dist.device)].cpu().numpy().astype(np.int64)
   else:
     c = np.asarray(prob.coordinates, dtype=np.float64)
     block = distance_block(c[rows], c, getattr(prob, "edge_type", "EUC_2D")).astype(np.int64)
@@ -357,7 +360,9 @@ def candidate_list(context, k: int) -> np.ndarray:
   table = out.cpu().numpy()
   tied = np.nonzero(ties.cpu().numpy())[0]
   if tied.size:
-    table[tied] = _host_knn_rows(context, tied, k_eff)
+    # the device matrix holds the reference's values bit for bit except for GEO (device cos/acos)
+    rows_from = dist if dist is not None and getattr(prob, "edge_type", "EUC_2D") != "GEO" else None
+    table[tied] = _host_knn_rows(context, tied, k_eff, rows_from)
   cache[k] = table
   return table
 
