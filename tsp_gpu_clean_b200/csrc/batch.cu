@@ -117,9 +117,14 @@ __global__ void __launch_bounds__(256) batch_offspring_kernel(const tspb_batch B
         (origin.same[0] && clean[origin.parent[0]]) || (origin.same[1] && clean[origin.parent[1]]) ? 1 : 0;
 }
 
-// CTA per instance: stable rank of the 2P combined fitness (old population first), keep P.
-__global__ void batch_survival_rank_kernel(const tspb_batch B) {
-  extern __shared__ double f2[];
+// CTA per instance: the stable order of the 2P combined fitness values (old population
+// first), i.e. (fitness, index) ascending, as the reference's lexsort keeps it; the first P
+// indices go to order[]. A bitonic sort of (fitness, index) pairs in shared memory, padded
+// with +inf to the next power of two n2.
+__global__ void batch_survival_rank_kernel(const tspb_batch B, int n2) {
+  extern __shared__ __align__(16) unsigned char rank_sm[];
+  double* key = reinterpret_cast<double*>(rank_sm);
+  int* idx = reinterpret_cast<int*>(key + n2);
   const int i = blockIdx.x, P = B.P;
   const int* c = B.ctl + 4 * i;
   if (c[1] != TSPB_BATCH_RUN) return;
@@ -127,17 +132,31 @@ __global__ void batch_survival_rank_kernel(const tspb_batch B) {
   const double* fa = fit_buf(B, parity) + (long long)i * P;
   const double* fb = B.off_fit + (long long)i * P;
   const int count = 2 * P;
-  for (int j = threadIdx.x; j < count; j += blockDim.x) f2[j] = j < P ? fa[j] : fb[j - P];
-  __syncthreads();
-  for (int j = threadIdx.x; j < count; j += blockDim.x) {
-    const double fj = f2[j];
-    int rank = 0;
-    for (int t = 0; t < count; ++t) {
-      const double ft = f2[t];
-      rank += (ft < fj) || (ft == fj && t < j);
-    }
-    if (rank < P) B.order[(long long)i * P + rank] = j;
+  for (int j = threadIdx.x; j < n2; j += blockDim.x) {
+    key[j] = j < P ? fa[j] : (j < count ? fb[j - P] : __longlong_as_double(0x7ff0000000000000LL));
+    idx[j] = j;
   }
+  __syncthreads();
+  for (int kk = 2; kk <= n2; kk <<= 1) {
+    for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+      for (int t = threadIdx.x; t < n2; t += blockDim.x) {
+        const int u = t ^ jj;
+        if (u > t) {
+          const double kt = key[t], ku = key[u];
+          const int it = idx[t], iu = idx[u];
+          const bool t_after_u = kt > ku || (kt == ku && it > iu);
+          if (t_after_u == ((t & kk) == 0)) {
+            key[t] = ku;
+            key[u] = kt;
+            idx[t] = iu;
+            idx[u] = it;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int r = threadIdx.x; r < P; r += blockDim.x) B.order[(long long)i * P + r] = idx[r];
 }
 
 // CTA per (instance, survivor): new_pop[r] = combined[order[r]] with its fitness and
@@ -180,26 +199,26 @@ __global__ void __launch_bounds__(128) batch_survival_gather_kernel(const tspb_b
   }
 }
 
-// Thread per RUN instance, after the gather: an elite-edge tie pauses the run unless every
-// row of the tied group (contiguous: survivors are sorted by (fitness, index)) is converged.
+// Warp per RUN instance, after the gather: an elite-edge tie pauses the run unless every
+// row of the tied group is converged. Survivors are sorted by (fitness, index), so the
+// tied group is every row whose fitness equals the elite edge's.
 __global__ void batch_pause_kernel(const tspb_batch B) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
   if (i >= B.num_instances) return;
   int* c = B.ctl + 4 * i;
-  if (c[1] != TSPB_BATCH_RUN || B.ties[(long long)i * B.G + c[0]] == 0) return;
+  if (c[1] != TSPB_BATCH_RUN || B.ties[(long long)i * B.G + c[0]] == 0) return;  // warp-uniform
   bool settled = false;
   if (B.clean[0]) {
     const int P = B.P, e = B.elite, parity = (c[0] + 1) & 1;
     const double* f = fit_buf(B, parity) + (long long)i * P;
     const uint8_t* cl = clean_buf(B, parity) + (long long)i * P;
     const double fe = f[e - 1];
-    int lo = e - 1, hi = e;
-    while (lo > 0 && f[lo - 1] == fe) --lo;
-    while (hi < P && f[hi] == fe) ++hi;
-    settled = true;
-    for (int r = lo; r < hi; ++r) settled = settled && cl[r] != 0;
+    bool ok = true;
+    for (int r = lane; r < P; r += 32) ok = ok && (f[r] != fe || cl[r] != 0);
+    settled = __all_sync(FULL, ok);
   }
-  if (!settled) c[1] = TSPB_BATCH_PAUSED;
+  if (!settled && lane == 0) c[1] = TSPB_BATCH_PAUSED;
 }
 
 // Persistent 2-opt over the (item, row) units of one phase. COORDS: the bucket's
@@ -267,23 +286,29 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value)
   }
 }
 
-// Warp per (instance, refined row) of a phase: fitness after the 2-opt (of the offspring
-// rows into off_fit in the OFFSPRING phase).
-__global__ void batch_elite_cost_kernel(const tspb_batch B, int phase) {
-  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+// CTA per (instance, refined row) of a phase: fitness after the 2-opt (of the offspring
+// rows into off_fit in the OFFSPRING phase), an exact int64 sum over the CTA.
+__global__ void __launch_bounds__(128) batch_elite_cost_kernel(const tspb_batch B, int phase) {
+  __shared__ long long red[32];
+  const long long w = blockIdx.x;
   const bool offspring = phase == TSPB_BATCH_PHASE_OFFSPRING;
   const int e_count = offspring ? B.P : B.elite;
   if (w >= (long long)B.num_instances * e_count) return;
   const int i = (int)(w / e_count), e = (int)(w - (long long)i * e_count);
   const int* c = B.ctl + 4 * i;
-  if (c[1] != phase_state(phase)) return;
+  if (c[1] != phase_state(phase)) return;  // uniform per CTA
   const int parity = (c[0] + 1) & 1;
   const int row = phase == TSPB_BATCH_PHASE_RESUME ? B.host_elites[(long long)i * e_count + e] : e;
   if ((unsigned)row >= (unsigned)B.P) return;
   const tspb_batch_instance I = B.inst[i];
   const int32_t* tour = (offspring ? B.off : pop_buf(B, parity)) + I.pop_offset + (long long)row * I.n;
-  const double f = warp_tour_length(tour, I.n, inst_ds(I));
-  if ((threadIdx.x & 31) == 0) (offspring ? B.off_fit : fit_buf(B, parity))[(long long)i * B.P + row] = f;
+  const DistSrc ds = inst_ds(I);
+  const int n = I.n;
+  long long acc = 0;
+  for (int p = threadIdx.x; p < n; p += blockDim.x) acc += ds(tour[p], tour[p + 1 == n ? 0 : p + 1]);
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0)
+    (offspring ? B.off_fit : fit_buf(B, parity))[(long long)i * B.P + row] = n <= 1 ? 0.0 : (double)acc;
 }
 
 // CTA per instance of a phase: argmin of fitness (first minimum), strict improvement by
@@ -492,11 +517,16 @@ extern "C" int tspb_batch_survival(const tspb_batch* b, void* stream) {
   if (b->num_instances == 0 || b->G == 0) return TSPB_OK;
   if ((long long)b->num_instances * b->P > 0x7fffffffLL || b->P > 3072) return TSPB_ERR_UNSUPPORTED;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  int rank_threads = ((2 * b->P + 31) / 32) * 32;
-  if (rank_threads > 512) rank_threads = 512;
-  batch_survival_rank_kernel<<<b->num_instances, rank_threads, (size_t)16 * b->P, st>>>(*b);
+  int n2 = 1;
+  while (n2 < 2 * b->P) n2 <<= 1;
+  const int rank_threads = n2 >= 1024 ? 512 : (n2 / 2 > 32 ? n2 / 2 : 32);
+  const size_t rank_smem = (size_t)12 * n2;
+  if (rank_smem > 48 * 1024)
+    TSPB_CUDA_CHECK(cudaFuncSetAttribute(batch_survival_rank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)rank_smem));
+  batch_survival_rank_kernel<<<b->num_instances, rank_threads, rank_smem, st>>>(*b, n2);
   batch_survival_gather_kernel<<<b->num_instances * b->P, 128, 0, st>>>(*b);
-  batch_pause_kernel<<<(b->num_instances + 127) / 128, 128, 0, st>>>(*b);
+  batch_pause_kernel<<<(b->num_instances * 32 + 127) / 128, 128, 0, st>>>(*b);
   return tspb_launch_status();
 }
 
@@ -537,9 +567,9 @@ extern "C" int tspb_batch_elite_cost(const tspb_batch* b, int32_t phase, void* s
   const int rows = phase == TSPB_BATCH_PHASE_OFFSPRING ? b->P : b->elite;
   if (b->num_instances == 0 || rows == 0 || b->G == 0) return TSPB_OK;
   if (phase == TSPB_BATCH_PHASE_RESUME && !b->host_elites) return TSPB_ERR_ARG;
-  const long long threads = (long long)b->num_instances * rows * 32;
-  if ((threads + 255) / 256 > 0x7fffffffLL) return TSPB_ERR_UNSUPPORTED;
-  batch_elite_cost_kernel<<<(int)((threads + 255) / 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(*b, phase);
+  const long long ctas = (long long)b->num_instances * rows;
+  if (ctas > 0x7fffffffLL) return TSPB_ERR_UNSUPPORTED;
+  batch_elite_cost_kernel<<<(unsigned)ctas, 128, 0, reinterpret_cast<cudaStream_t>(stream)>>>(*b, phase);
   return tspb_launch_status();
 }
 
