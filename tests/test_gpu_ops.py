@@ -153,8 +153,6 @@ def test_nn_init_matches_reference(torch_mod, golden):
 def test_nn_init_jobs_shared_memory_matches_workspace_kernel(torch_mod):
   """Nearest-neighbour rows built with the working arrays in shared memory equal the
   workspace kernel's, for jobs of different sizes and k (k = 0: uniform choices only)."""
-  import ctypes
-
   from tsp_gpu_clean_b200 import native
   from tsp_gpu_clean_b200.device import ptr, stream_handle
 
@@ -194,4 +192,3 @@ def test_nn_init_jobs_shared_memory_matches_workspace_kernel(torch_mod):
   lib = native.load_library()
   assert lib.tspb_nn_init_jobs_smem(ptr(j1), 1, 1, 70000, 5, None) == native.TSPB_ERR_UNSUPPORTED
   assert lib.tspb_nn_init_jobs_smem(None, 1, 1, 100, 5, None) == native.TSPB_ERR_ARG
-  del ctypes
