@@ -452,7 +452,8 @@ def run_ga_bench(args) -> dict:
       solver = FusedBatchSolver(population_size=P, mutation_rate=o["rate"], tournament_k=5, nn_k=5, local_search=ls,
                                 elite_count=elite, post_init=post_init, max_matrix_dimension=None, tuner=tuner,
                                 chunk=args.chunk, use_graph=not args.no_graph, crossover=o["crossover"],
-                                mutation=o["mutation"], init=o["init"], local_search_stage=o["stage"])
+                                mutation=o["mutation"], init=o["init"], local_search_stage=o["stage"],
+                                incremental=args.batch_incremental)
       results = solver.evolve(ctxs, G, patience=10**9)
       stats = {"generations_completed": sum(st["generations_completed"] for _, st in results),
                "best_fitness": min(st["best_fitness"] for _, st in results)}
@@ -488,6 +489,9 @@ def run_ga_bench(args) -> dict:
                   "d2h_bytes_per_step": int(reps * (n * 4 + (G + 1) * 8 + P * n * 4))},
           "gpu_launches": launches, "desc": desc, "best": stats["best_fitness"],
           "loop_ms_steps": [round(v, 3) for v in loop_ms], "walls_s": [round(w, 4) for w in walls],
+          "buckets": [{"n": [b.lo, b.hi], "two_opt_threads": b.two_opt_threads, "incremental": b.incremental,
+                       "offspring_threads": b.offspring_threads} for b in getattr(solver, "buckets", [])],
+          "two_opt_totals": getattr(solver, "two_opt_totals", None),
           "timing": {k: round(v, 4) for k, v in solver.last_timing.items() if isinstance(v, (int, float))}}
 
 
@@ -572,7 +576,7 @@ def run_uneven_bench(args) -> dict:
     solver = FusedBatchSolver(population_size=64, mutation_rate=0.05, tournament_k=5, nn_k=5,
                               local_search=LocalSearchConfig("best", 10, 20), elite_count=8, post_init=True,
                               max_matrix_dimension=4096, tuner=tuner, chunk=args.chunk,
-                              use_graph=not args.no_graph)
+                              use_graph=not args.no_graph, incremental=args.batch_incremental)
     gc.collect()  # the previous runs' garbage, outside the timed call
     t0 = time.perf_counter()
     res = solver.evolve(ctxs, G, patience=10**9)
@@ -615,7 +619,8 @@ def run_uneven_bench(args) -> dict:
                      "generations_per_step": gens // args.steps,
                      "elite_edge_ties_per_step": ties // args.steps, "host_pauses_per_step": pauses // args.steps,
                      "buckets": [{"n": [b.lo, b.hi], "coords": b.coords, "instances": len(b.items),
-                                  "two_opt_threads": b.two_opt_threads, "offspring_threads": b.offspring_threads}
+                                  "two_opt_threads": b.two_opt_threads, "incremental": b.incremental,
+                                  "offspring_threads": b.offspring_threads}
                                  for b in solver.buckets],
                      "setup_s": solver.last_timing["setup_s"], "tune_s_total": tune_s,
                      "last_run": {k: round(v, 4) for k, v in solver.last_timing.items() if isinstance(v, (int, float))},
@@ -777,6 +782,9 @@ def main(argv=None) -> int:
                   help="two_opt: read the int32 matrix, or rebuild each distance from FP64 coordinates")
   ap.add_argument("--first-restart", default="incremental", choices=["incremental", "full"],
                   help="first mode: restart each pass from the affected entries and row bi, or rescan from entry 0")
+  ap.add_argument("--batch-incremental", default="auto", choices=["auto", "on", "off"],
+                  help="GA/uneven: 2-opt with the reverse k-NN index (best: only the rows a move can change are "
+                       "recomputed; first: incremental restart); auto lets the tuner measure both")
   ap.add_argument("--cpu-workers", type=int, default=0, help="0: all host cores, capped at 64")
   ap.add_argument("--no-cpu-baseline", action="store_true")
   ap.add_argument("--workload", default="two_opt", choices=["two_opt", "learned", "uneven", *GA_WORKLOADS])
@@ -898,7 +906,8 @@ def main_ga(args) -> int:
           "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)", "config": config, "clocks": res["clocks"],
           "e2e": res["e2e"], "gpu_launches": res["gpu_launches"],
           "detail": {"best_fitness": res["best"], "engine": args.engine, "last_run": res["timing"],
-                     "loop_ms_steps": res["loop_ms_steps"], "walls_s": res["walls_s"]}}
+                     "loop_ms_steps": res["loop_ms_steps"], "walls_s": res["walls_s"], "buckets": res["buckets"],
+                     "two_opt_totals": res["two_opt_totals"]}}
   if res["world"] > 1:
     config["parallelism"] = f"{res['world']} independent replicas (one GA run per GPU, generator seeded per rank)"
   if not args.no_cpu_baseline and res["world"] == 1:

@@ -434,6 +434,8 @@ typedef struct tspb_batch_instance {
   int64_t patience;             /* generations without a strict improvement before STOPPED */
   double optimal;               /* known optimal cost (> 0) for the early stops of
                                    genetic_algorithm.py:894-905, else 0 */
+  const int32_t* rev_off;       /* reverse k-NN index (tspb_candidate_reverse_index), or NULL; */
+  const int32_t* rev_idx;       /* required by TSPB_BATCH_INCREMENTAL */
 } tspb_batch_instance;
 
 typedef struct tspb_batch {
@@ -484,6 +486,12 @@ int tspb_batch_offspring(const tspb_batch* b, const int32_t* items, int32_t num_
 int tspb_batch_survival(const tspb_batch* b, void* stream);
 #define TSPB_BATCH_COORDS 1  /* every item has dist == NULL: distances rebuilt from coordinates */
 #define TSPB_BATCH_GROUPED 2 /* every item's k is a multiple of 4 and its packed table 16-byte aligned */
+/* with GROUPED: every item has rev_off/rev_idx. Best mode keeps the minimum improving key
+ * of every row and, after a move with window [bi, bj], recomputes only the rows of the
+ * window and the earlier rows with a candidate in it (30 n bytes of shared memory per
+ * CTA instead of 16 n); first mode restarts from the move's row after checking the
+ * affected entries (as tspb_two_opt with the reverse index). Same results either way. */
+#define TSPB_BATCH_INCREMENTAL 4
 /* 2-opt over the (item, row) units of one phase: persistent CTAs (ctas <= 0: every CTA
  * that fits) take units from the device counter `queue` (zeroed by this call) in item
  * order; put the largest instances first. `flags` (TSPB_BATCH_*) state what holds for
@@ -494,8 +502,8 @@ int tspb_batch_survival(const tspb_batch* b, void* stream);
 int tspb_batch_two_opt(const tspb_batch* b, const int32_t* items, int32_t num_items, int32_t max_n,
                        int32_t flags, int32_t phase, int32_t mode, int64_t max_iterations, int32_t threads,
                        int32_t ctas, uint32_t* queue, void* stream);
-/* Resident CTAs per SM of tspb_batch_two_opt for this shape (0: does not fit). */
-int tspb_batch_two_opt_occupancy(int32_t max_n, int32_t mode, int32_t threads);
+/* Resident CTAs per SM of tspb_batch_two_opt for this shape and flags (0: does not fit). */
+int tspb_batch_two_opt_occupancy(int32_t max_n, int32_t mode, int32_t threads, int32_t flags);
 /* Fitness of the refined rows of a phase (RESUME, RUN, or OFFSPRING into off_fit). */
 int tspb_batch_elite_cost(const tspb_batch* b, int32_t phase, void* stream);
 /* Best tracking, history, early stops and the generation counter of a phase's instances:

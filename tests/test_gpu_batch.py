@@ -117,7 +117,10 @@ def test_batch_elite_boundary_ties_match_oracle(batch_mod, iters):
     _check_run(solver, res, ctxs, idx, _oracle_run(coords, seed, 40, 0.3, 6, False, "best", iters, 8, 40, 10**9))
 
 
-def test_batch_first_mode_and_early_stop_match_oracle(batch_mod):
+@pytest.mark.parametrize("incremental", ["on", "off"])
+def test_batch_first_mode_and_early_stop_match_oracle(batch_mod, incremental):
+  """First mode, with (on) or without (off) the incremental restart through the reverse
+  k-NN index (k = 12 for the grouped layout that it needs), and patience stops."""
   from tsp_gpu_clean_b200.fused import LocalSearchConfig
   from tsp_gpu_clean_b200.instances import uniform_instance
   from tsp_gpu_clean_b200.problem import Problem, ProblemContext
@@ -125,11 +128,13 @@ def test_batch_first_mode_and_early_stop_match_oracle(batch_mod):
   insts = [(uniform_instance(n, 100 + n), 200 + n) for n in (9, 40, 77, 130)]
   ctxs = [ProblemContext(Problem.from_coordinates(c), seed=s) for c, s in insts]
   solver = batch_mod.FusedBatchSolver(population_size=24, mutation_rate=0.2, elite_count=5, post_init=True,
-                                      local_search=LocalSearchConfig("first", 4, 10), max_matrix_dimension=100)
+                                      local_search=LocalSearchConfig("first", 4, 12), max_matrix_dimension=100,
+                                      incremental=incremental)
   res = solver.evolve(ctxs, 30, patience=3)
   assert any(st["stopped_early"] for _, st in res)
   for idx, (coords, seed) in enumerate(insts):
-    _check_run(solver, res, ctxs, idx, _oracle_run(coords, seed, 24, 0.2, 5, True, "first", 4, 10, 30, 3))
+    _check_run(solver, res, ctxs, idx, _oracle_run(coords, seed, 24, 0.2, 5, True, "first", 4, 12, 30, 3))
+  assert any(b.incremental for b in solver.buckets) == (incremental == "on")
 
 
 def test_converged_row_skipping_changes_nothing(batch_mod):

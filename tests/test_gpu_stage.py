@@ -149,10 +149,12 @@ def test_fused_ga_with_post_mutation_stage_matches_reference(torch_mod, golden, 
   _check(g, tag, best, stats, ctx)
 
 
-@pytest.mark.parametrize("skip_converged", [True, False])
-def test_batch_chapter4_runs_of_mixed_sizes_match_oracle(torch_mod, skip_converged):
+@pytest.mark.parametrize("skip_converged,incremental", [(True, "on"), (False, "on"), (True, "off")])
+def test_batch_chapter4_runs_of_mixed_sizes_match_oracle(torch_mod, skip_converged, incremental):
   """Instances of sizes across several buckets, Chapter-4 configuration, each run equal to
-  the oracle GA (random init, OX, swap, 2-opt on every child) with its own seed."""
+  the oracle GA (random init, OX, swap, 2-opt on every child) with its own seed. With the
+  reverse k-NN index (incremental "on") best mode recomputes only the rows a move can
+  change: fewer gains evaluated than the pairs the reference scans, the same runs."""
   from tsp_gpu_clean_b200 import instances
   from tsp_gpu_clean_b200.batch import FusedBatchSolver
   from tsp_gpu_clean_b200.fused import LocalSearchConfig
@@ -164,8 +166,14 @@ def test_batch_chapter4_runs_of_mixed_sizes_match_oracle(torch_mod, skip_converg
   solver = FusedBatchSolver(population_size=P, mutation_rate=rate, tournament_k=5, nn_k=5,
                             local_search=LocalSearchConfig("best", 10, 8), elite_count=0, post_init=False,
                             chunk=5, skip_converged=skip_converged, crossover="ox", mutation="swap", init="random",
-                            local_search_stage="post_mutation")
+                            local_search_stage="post_mutation", incremental=incremental)
   results = solver.evolve(ctxs, G, patience=10**9)
+  assert all(b.incremental == (incremental == "on") for b in solver.buckets)
+  tot = solver.two_opt_totals
+  if incremental == "on":
+    assert tot["evaluated"] < tot["pairs"]
+  else:
+    assert tot["evaluated"] == tot["pairs"]
   for j, ((best, stats), c) in enumerate(zip(results, coords)):
     cache = {}
 
@@ -194,6 +202,8 @@ def test_invalid_stage_options():
     FusedBatchSolver(local_search_stage="post_crossover")
   with pytest.raises(ValueError):
     FusedBatchSolver(init="greedy")
+  with pytest.raises(ValueError):
+    FusedBatchSolver(incremental="yes")
   with pytest.raises(ValueError):
     FusedMemeticSolver(engine="single", local_search_stage="post_mutation")
   with pytest.raises(ValueError):

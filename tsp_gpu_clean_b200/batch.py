@@ -102,6 +102,7 @@ class Bucket:
   max_n: int = 0
   grouped: bool = False  # every item's k % 4 == 0 and its packed table 16-byte aligned
   can_rebuild: bool = False  # every item has coordinates: the tuner may pick them over the matrix
+  incremental: bool = False  # the 2-opt runs with the reverse k-NN index (TSPB_BATCH_INCREMENTAL)
   two_opt_threads: int = 128
   offspring_threads: int = 128
   d_items: Any = None
@@ -138,7 +139,7 @@ class FusedBatchSolver:
                tuner: BatchAutotuner | None = None, bucket_bounds: Sequence[int] = DEFAULT_BUCKET_BOUNDS,
                chunk: int = 16, skip_converged: bool = True, concurrent_buckets: bool = True,
                crossover: str = "pmx", mutation: str = "inversion", init: str = "nn",
-               local_search_stage: str = "none") -> None:
+               local_search_stage: str = "none", incremental: str = "auto") -> None:
     if population_size < 2:
       raise ValueError("population_size must be >= 2")
     if init not in ("nn", "random"):
@@ -146,6 +147,11 @@ class FusedBatchSolver:
     if local_search_stage not in ("none", "post_mutation"):
       raise ValueError("local_search_stage must be 'none' or 'post_mutation'")
     self.init, self.stage = init, local_search_stage
+    # 2-opt with the reverse k-NN index: best mode recomputes only the rows a move can
+    # change, first mode restarts from the move's row; "auto" lets the tuner measure both
+    if incremental not in ("auto", "on", "off"):
+      raise ValueError("incremental must be 'auto', 'on' or 'off'")
+    self.incremental = incremental
     if crossover not in CROSSOVER_CODES:
       raise ValueError(f"crossover must be one of {sorted(CROSSOVER_CODES)}")
     if mutation not in MUTATION_CODES:
@@ -236,7 +242,8 @@ class FusedBatchSolver:
 
   @staticmethod
   def _flags(bucket: Bucket) -> int:
-    return (native.TSPB_BATCH_COORDS if bucket.coords else 0) | (native.TSPB_BATCH_GROUPED if bucket.grouped else 0)
+    return ((native.TSPB_BATCH_COORDS if bucket.coords else 0) | (native.TSPB_BATCH_GROUPED if bucket.grouped else 0)
+            | (native.TSPB_BATCH_INCREMENTAL if bucket.incremental else 0))
 
   def _two_opt(self, st_ref, bucket: Bucket, phase: int, threads: int | None = None) -> None:
     rc = native.load_library().tspb_batch_two_opt(
@@ -325,15 +332,20 @@ class FusedBatchSolver:
       if self._ls_rows:
         units = len(b.items) * self._ls_rows
         key = self.tuner.key(name, "two_opt", mode=self.ls.mode, k=self.k, iters=int(self.ls.max_iterations),
-                             lo=b.lo, hi=b.hi, coords=b.coords, rebuild=b.can_rebuild, units=units)
-        threads = [t for t in TWO_OPT_THREADS if lib.tspb_batch_two_opt_occupancy(b.max_n, self._mode, t) > 0]
-        if not threads:
-          raise ValueError(f"instances of n={b.max_n} do not fit the batch 2-opt's shared memory")
-        # candidate = 2 * threads + source (1: distances rebuilt from coordinates)
+                             lo=b.lo, hi=b.hi, coords=b.coords, rebuild=b.can_rebuild, units=units,
+                             inc=self.incremental if b.grouped else "off")
+        # candidate = 4 * threads + 2 * incremental + source (1: distances rebuilt from coordinates)
+        incs = {"auto": (0, 1), "on": (1,), "off": (0,)}[self.incremental] if b.grouped else (0,)
         sources = (0, 1) if (b.can_rebuild and not b.coords) else ((1,) if b.coords else (0,))
-        cands = [2 * t + src for t in threads for src in sources]
-        choice = self.tuner.choose(key, cands, lambda c, b=b: self._probe_two_opt(b, c // 2, bool(c & 1)))
-        b.two_opt_threads = choice // 2
+        cands = [4 * t + 2 * inc + src for t in TWO_OPT_THREADS for inc in incs for src in sources
+                 if lib.tspb_batch_two_opt_occupancy(
+                   b.max_n, self._mode, t, native.TSPB_BATCH_GROUPED | native.TSPB_BATCH_INCREMENTAL if inc else 0) > 0]
+        if not cands:
+          raise ValueError(f"instances of n={b.max_n} do not fit the batch 2-opt's shared memory")
+        choice = self.tuner.choose(key, cands,
+                                   lambda c, b=b: self._probe_two_opt(b, c // 4, bool(c & 1), bool(c & 2)))
+        b.two_opt_threads = choice // 4
+        b.incremental = bool(choice & 2)
         if choice & 1 and not b.coords:
           self._rebuild_from_coordinates(b)
       if self.G:
@@ -363,11 +375,12 @@ class FusedBatchSolver:
     self.d_inst.copy_(torch.frombuffer(bytearray(self.h_inst), dtype=torch.uint8))
     b.coords = True
 
-  def _probe_two_opt(self, b: Bucket, threads: int, rebuild: bool = False) -> float:
+  def _probe_two_opt(self, b: Bucket, threads: int, rebuild: bool = False, incremental: bool = False) -> float:
     """The generation's 2-opt work shape for one bucket on scratch copies of the initial
     tours: the first `elite` rows of every instance (every row with the post_mutation
     stage), refined for up to max_iterations passes, with the bucket's matrices or
-    (rebuild) distances rebuilt from coordinates."""
+    (rebuild) distances rebuilt from coordinates, and with or without the reverse k-NN
+    index (incremental)."""
     e = max(self._ls_rows, 2)  # the probe batch needs P >= 2
     ns = self.ns
     offs = np.zeros(self.I, dtype=np.int64)
@@ -381,7 +394,8 @@ class FusedBatchSolver:
         inst[i].dist = None
         inst[i].dist_stride = 0
     d_inst = torch.frombuffer(bytearray(inst), dtype=torch.uint8).cuda()
-    flags = self._flags(b) | (native.TSPB_BATCH_COORDS if rebuild else 0)
+    flags = ((native.TSPB_BATCH_COORDS if (b.coords or rebuild) else 0)
+             | (native.TSPB_BATCH_GROUPED if b.grouped else 0) | (native.TSPB_BATCH_INCREMENTAL if incremental else 0))
     status = torch.zeros((self.I, e), dtype=torch.int32, device="cuda")
     st = self._state()
     st.P = e
@@ -594,6 +608,8 @@ class FusedBatchSolver:
       rebuildable.append(xy is not None)
       self._keep.append(xy)
       inst.cand_packed = tabs.packed.data_ptr()
+      inst.rev_off = tabs.rev_off.data_ptr()
+      inst.rev_idx = tabs.rev_idx.data_ptr()
       pat = patience[i] if isinstance(patience, (list, tuple, np.ndarray)) else patience
       inst.patience = int(pat) if pat is not None else int(2 * math.sqrt(n))
       opt = optimal_cost[i] if isinstance(optimal_cost, (list, tuple, np.ndarray)) else optimal_cost

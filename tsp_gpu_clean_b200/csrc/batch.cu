@@ -224,8 +224,10 @@ __global__ void batch_pause_kernel(const tspb_batch B) {
 // Persistent 2-opt over the (item, row) units of one phase. COORDS: the bucket's
 // instances rebuild distances from coordinates (no matrix); otherwise they all have one.
 // LAYOUT: SCAN_GROUPED when every item's k is a multiple of U and its packed table is
-// U*4-byte aligned, else SCAN_PACKED.
-template <int MODE, int THREADS, int U, bool COORDS, int LAYOUT>
+// U*4-byte aligned, else SCAN_PACKED. REV (TSPB_BATCH_INCREMENTAL): the items carry their
+// reverse k-NN index; best mode then keeps incremental row keys (INC, grouped layout only)
+// and first mode restarts incrementally.
+template <int MODE, int THREADS, int U, bool COORDS, int LAYOUT, bool REV = false>
 __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value)
     batch_two_opt_kernel(const tspb_batch B, const int32_t* __restrict__ items, int num_items, int rows, int phase,
                          long long max_iter, int max_n, unsigned* __restrict__ queue) {
@@ -261,7 +263,8 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value)
     const tspb_batch_instance I = B.inst[i];
     const bool layout_ok = LAYOUT != SCAN_GROUPED ||
                            (I.k % U == 0 && (reinterpret_cast<uintptr_t>(I.cand_packed) % (U * sizeof(uint32_t))) == 0);
-    if ((I.dist == nullptr) != COORDS || I.n > max_n || I.n < 4 || I.k < 1 || !layout_ok) {
+    const bool rev_ok = !REV || (I.rev_off != nullptr && I.rev_idx != nullptr);
+    if ((I.dist == nullptr) != COORDS || I.n > max_n || I.n < 4 || I.k < 1 || !layout_ok || !rev_ok) {
       if (threadIdx.x == 0) B.ls_status[(long long)i * B.rows_max + e] = TSPB_ERR_UNSUPPORTED;
       continue;
     }
@@ -282,7 +285,9 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value)
     T.accumulate = 1;
     T.moved = nullptr;
     T.converged = clean;
-    scan_tour<MODE, THREADS, U, LAYOUT>(T, S);
+    T.rev_off = REV ? I.rev_off : nullptr;
+    T.rev_idx = REV ? I.rev_idx : nullptr;
+    scan_tour<MODE, THREADS, U, LAYOUT, REV && MODE == TSPB_MODE_BEST>(T, S);
   }
 }
 
@@ -393,10 +398,21 @@ static int batch_two_opt_launch(const tspb_batch& b, const int32_t* items, int n
                                 long long max_iter, int max_n, size_t smem, int ctas, int flags, unsigned* queue,
                                 cudaStream_t st) {
   const bool coords = flags & TSPB_BATCH_COORDS, grouped = flags & TSPB_BATCH_GROUPED;
-  auto kern = coords ? (grouped ? batch_two_opt_kernel<MODE, THREADS, U, true, SCAN_GROUPED>
+  const bool rev = flags & TSPB_BATCH_INCREMENTAL;
+  using Kern = void (*)(const tspb_batch, const int32_t*, int, int, int, long long, int, unsigned*);
+  Kern kern = coords ? (grouped ? batch_two_opt_kernel<MODE, THREADS, U, true, SCAN_GROUPED>
                                 : batch_two_opt_kernel<MODE, THREADS, U, true, SCAN_PACKED>)
                      : (grouped ? batch_two_opt_kernel<MODE, THREADS, U, false, SCAN_GROUPED>
                                 : batch_two_opt_kernel<MODE, THREADS, U, false, SCAN_PACKED>);
+  if (rev) {
+    // the reverse-index variants exist for the grouped layout (the caller checked GROUPED),
+    // which every CTA size launches with four words per thread
+    if constexpr (U == 4)
+      kern = coords ? batch_two_opt_kernel<MODE, THREADS, U, true, SCAN_GROUPED, true>
+                    : batch_two_opt_kernel<MODE, THREADS, U, false, SCAN_GROUPED, true>;
+    else
+      return TSPB_ERR_ARG;
+  }
   TSPB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   TSPB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem));
@@ -417,8 +433,9 @@ static int batch_two_opt_launch(const tspb_batch& b, const int32_t* items, int n
 }
 
 template <int MODE, int THREADS, int U>
-static int batch_two_opt_occ(size_t smem) {
-  auto kern = batch_two_opt_kernel<MODE, THREADS, U, false, SCAN_GROUPED>;
+static int batch_two_opt_occ(size_t smem, bool rev) {
+  auto kern = rev ? batch_two_opt_kernel<MODE, THREADS, U, false, SCAN_GROUPED, true>
+                  : batch_two_opt_kernel<MODE, THREADS, U, false, SCAN_GROUPED>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem) != cudaSuccess) return 0;
@@ -458,13 +475,13 @@ static int batch_two_opt_mode(const tspb_batch& b, const int32_t* items, int num
 }
 
 template <int MODE>
-static int batch_two_opt_occ_mode(int threads, size_t smem) {
+static int batch_two_opt_occ_mode(int threads, size_t smem, bool rev) {
   switch (threads) {
-    case 64: return batch_two_opt_occ<MODE, 64, 4>(smem);
-    case 128: return batch_two_opt_occ<MODE, 128, 4>(smem);
-    case 256: return batch_two_opt_occ<MODE, 256, 4>(smem);
-    case 512: return batch_two_opt_occ<MODE, 512, 2>(smem);
-    case 1024: return batch_two_opt_occ<MODE, 1024, 2>(smem);
+    case 64: return batch_two_opt_occ<MODE, 64, 4>(smem, rev);
+    case 128: return batch_two_opt_occ<MODE, 128, 4>(smem, rev);
+    case 256: return batch_two_opt_occ<MODE, 256, 4>(smem, rev);
+    case 512: return batch_two_opt_occ<MODE, 512, 4>(smem, rev);
+    case 1024: return batch_two_opt_occ<MODE, 1024, 4>(smem, rev);
     default: return 0;
   }
 }
@@ -530,19 +547,22 @@ extern "C" int tspb_batch_survival(const tspb_batch* b, void* stream) {
   return tspb_launch_status();
 }
 
-extern "C" int tspb_batch_two_opt_occupancy(int32_t max_n, int32_t mode, int32_t threads) {
+extern "C" int tspb_batch_two_opt_occupancy(int32_t max_n, int32_t mode, int32_t threads, int32_t flags) {
   if (max_n < 4 || (mode != TSPB_MODE_BEST && mode != TSPB_MODE_FIRST)) return 0;
-  const size_t smem = scan_tour_state_bytes(max_n, mode);
+  const bool rev = flags & TSPB_BATCH_INCREMENTAL;
+  const size_t smem = scan_tour_state_bytes(max_n, mode, rev);
   if (smem > (size_t)smem_optin() - 2048) return 0;
-  return mode == TSPB_MODE_BEST ? batch_two_opt_occ_mode<TSPB_MODE_BEST>(threads, smem)
-                                : batch_two_opt_occ_mode<TSPB_MODE_FIRST>(threads, smem);
+  return mode == TSPB_MODE_BEST ? batch_two_opt_occ_mode<TSPB_MODE_BEST>(threads, smem, rev)
+                                : batch_two_opt_occ_mode<TSPB_MODE_FIRST>(threads, smem, rev);
 }
 
 extern "C" int tspb_batch_two_opt(const tspb_batch* b, const int32_t* items, int32_t num_items, int32_t max_n,
                                   int32_t flags, int32_t phase, int32_t mode, int64_t max_iterations, int32_t threads,
                                   int32_t ctas, uint32_t* queue, void* stream) {
   if (!batch_ok(b) || num_items < 0 || max_n < 4 || !queue) return TSPB_ERR_ARG;
-  if (flags & ~(TSPB_BATCH_COORDS | TSPB_BATCH_GROUPED)) return TSPB_ERR_ARG;
+  if (flags & ~(TSPB_BATCH_COORDS | TSPB_BATCH_GROUPED | TSPB_BATCH_INCREMENTAL)) return TSPB_ERR_ARG;
+  const bool rev = flags & TSPB_BATCH_INCREMENTAL;
+  if (rev && !(flags & TSPB_BATCH_GROUPED)) return TSPB_ERR_ARG;
   if (phase < TSPB_BATCH_PHASE_POSTINIT || phase > TSPB_BATCH_PHASE_OFFSPRING) return TSPB_ERR_ARG;
   if (mode != TSPB_MODE_BEST && mode != TSPB_MODE_FIRST) return TSPB_ERR_ARG;
   const int rows = (phase == TSPB_BATCH_PHASE_POSTINIT || phase == TSPB_BATCH_PHASE_OFFSPRING) ? b->P : b->elite;
@@ -550,7 +570,7 @@ extern "C" int tspb_batch_two_opt(const tspb_batch* b, const int32_t* items, int
   if (!items) return TSPB_ERR_ARG;
   if (phase == TSPB_BATCH_PHASE_RESUME && !b->host_elites) return TSPB_ERR_ARG;
   if ((long long)num_items * rows > 0x7fffffffLL || max_n > 65535) return TSPB_ERR_UNSUPPORTED;
-  const size_t smem = scan_tour_state_bytes(max_n, mode);
+  const size_t smem = scan_tour_state_bytes(max_n, mode, rev);
   if (smem > (size_t)smem_optin() - 2048) return TSPB_ERR_UNSUPPORTED;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   if (mode == TSPB_MODE_BEST)

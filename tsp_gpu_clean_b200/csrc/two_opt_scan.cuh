@@ -18,6 +18,14 @@
 // publishes the smallest improving index of a round with a shared atomicMin; once set,
 // later rounds only count the pairs the reference still evaluates (validity, no gains).
 //
+// best with incremental row keys (INC, grouped layout, reverse k-NN index): every row keeps
+// the minimum key of its improving entries. After a move with window [bi, bj] only the rows
+// in the window and the earlier rows with a candidate in the window can change (rows after
+// bj see the window's candidates at invalid positions), so a pass recomputes those rows
+// and reduces the row keys; long windows take a full recomputation. It pays where few CTAs
+// share an SM (the 30n bytes of tour state leave L1 to the k-NN table) and tours need few
+// passes, as for the children of locally optimal parents.
+//
 // first with the reverse k-NN index (incremental restart): the reference restarts every
 // pass at entry 0. After a move with window [bi, bj] (the first improving entry was in row
 // bi, so every entry before it was non-improving), an entry (i, r) of a row i < bi keeps
@@ -34,8 +42,9 @@ namespace tspb {
 struct ScanSmem {
   unsigned long long red64[32];
   long long redll[32];
-  long long total;  // first: valid entries of the current tour (kept exact across passes)
+  long long total;  // first (and incremental best): valid entries of the current tour, kept exact
   unsigned first;
+  int nlist;        // incremental best: rows to recompute in this pass
   int bad;
   int stop;
 };
@@ -45,9 +54,11 @@ struct ScanMinBlocks {
   static constexpr int value = THREADS == 64 ? 16 : THREADS == 128 ? 8 : THREADS == 256 ? 4 : THREADS == 512 ? 2 : 1;
 };
 
-// Bytes of tour state per tour: tour, pos, succ, eout (+ per-row valid counts for first).
-__host__ __device__ inline size_t scan_tour_state_bytes(int n, int mode) {
-  return (size_t)(mode == TSPB_MODE_FIRST ? 20 : 16) * (size_t)n;
+// Bytes of tour state per tour: tour, pos, succ, eout (+ per-row valid counts for first;
+// best with incremental row keys adds the keys, valid counts and a row list).
+__host__ __device__ inline size_t scan_tour_state_bytes(int n, int mode, bool incremental = false) {
+  if (mode == TSPB_MODE_FIRST) return (size_t)20 * (size_t)n;
+  return (size_t)(incremental ? 30 : 16) * (size_t)n;
 }
 
 struct ScanTour {
@@ -95,7 +106,7 @@ __device__ __forceinline__ void load_words(const uint32_t* p, uint32_t (&w)[U]) 
 }
 
 // Refines one tour with the whole CTA. Every thread of the CTA must call it.
-template <int MODE, int THREADS, int U, int LAYOUT>
+template <int MODE, int THREADS, int U, int LAYOUT, bool INC = false>
 __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
   constexpr bool PACKED = LAYOUT != SCAN_PLAIN;
   constexpr bool GROUPED = LAYOUT == SCAN_GROUPED;
@@ -106,7 +117,13 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
   int* pos = tour + n;
   int* succ = pos + n;
   int* eout = succ + n;
-  int* rcnt = eout + n;  // first: valid entries per row (position), n ints
+  // INC: the caller gives the reverse index; per-row minimum keys (8-byte aligned at 16n),
+  // valid counts and the row list follow the tour state
+  constexpr bool inc_best = MODE == TSPB_MODE_BEST && GROUPED && INC;
+  unsigned long long* rkey = reinterpret_cast<unsigned long long*>(eout + n);
+  int* rcnt = inc_best ? reinterpret_cast<int*>(rkey + n) : eout + n;  // valid entries per row (position)
+  uint16_t* rlist = reinterpret_cast<uint16_t*>(rcnt + n);
+  constexpr bool track_rows = MODE == TSPB_MODE_FIRST || inc_best;
   const DistSrc ds = T.ds;
   const uint32_t* __restrict__ packed = T.packed;
   const int32_t* __restrict__ cand = T.cand;
@@ -172,7 +189,7 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
     }
     return c;
   };
-  if (MODE == TSPB_MODE_FIRST) {
+  if (track_rows) {
     long long sum = 0;
     for (int i = tid; i < n; i += THREADS) {
       const int v = i < rows ? row_count(i) : 0;
@@ -206,7 +223,7 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
       break;
     }
     ++passes;
-    if (MODE == TSPB_MODE_FIRST && tid == 0) my_pairs += S.total;
+    if (track_rows && tid == 0) my_pairs += S.total;
     int bgain = 0;            // best: smallest gain of this thread (strictly below 0 to count)
     unsigned bidx = NO_IDX;   // and its scan index (first in thread order wins ties)
     int cnt = 0, evals = 0;
@@ -237,8 +254,102 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
       found = S.first != NO_IDX;
       start_row = win_lo;
     }
+    if constexpr (inc_best) {
+      // minimum improving key of the U entries of row gi starting at column gr
+      auto group_key = [&](int gi, int gr) -> unsigned long long {
+        const int a = tour[gi];
+        uint32_t w[U];
+        load_words<U>(packed + ((unsigned)a * (unsigned)k + (unsigned)gr), w);
+        const int sa = succ[a], ea = eout[a];
+        const int lo = gi + 2;
+        const unsigned span = (unsigned)(n - (gi == 0) - lo);
+        bool ok[U];
+        int c[U], sc[U], dbd[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          c[u] = (int)(w[u] & 0xffffu);
+          ok[u] = (unsigned)c[u] < (unsigned)n && (unsigned)(pos[c[u]] - lo) < span;
+          if (ok[u]) sc[u] = succ[c[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (ok[u]) dbd[u] = dist ? __ldcg(dist + ((unsigned)sa * stride + (unsigned)sc[u])) : ds(sa, sc[u]);
+        unsigned long long key = NO_KEY;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          if (!ok[u]) continue;
+          ++evals;
+          const int gain = ((int)(w[u] >> 16) - ea) + (dbd[u] - eout[c[u]]);
+          if (gain < 0) {
+            const unsigned long long kk = gain_key(gain, (unsigned)(gi * k + gr + u));
+            key = kk < key ? kk : key;
+          }
+        }
+        return key;
+      };
+      constexpr unsigned long long DIRTY = NO_KEY - 1;  // never a key: keys hold negative gains
+      const int G = k / U;
+      const bool full = win_lo < 0 || 2LL * (win_hi - win_lo + 1) * (k + 1) > (long long)rows;
+      if (full) {
+        for (int i = tid; i < rows; i += THREADS) rkey[i] = NO_KEY;
+        __syncthreads();
+        for (int it = tid; it < rows * G; it += THREADS) {
+          const int gi = it / G, gr = (it - gi * G) * U;
+          const unsigned long long key = group_key(gi, gr);
+          if (key != NO_KEY) atomicMin(&rkey[gi], key);
+        }
+      } else {
+        if (tid == 0) S.nlist = 0;
+        const int r_hi = win_hi < rows - 1 ? win_hi : rows - 1;
+        for (int i = win_lo + tid; i <= r_hi; i += THREADS) rkey[i] = DIRTY;
+        const int lane = tid & 31, wid = tid >> 5;
+        constexpr int NW = THREADS / 32;
+        for (int q = win_lo + wid; q <= win_hi; q += NW) {
+          const int c = tour[q];
+          const int s0 = __ldg(T.rev_off + c), s1 = __ldg(T.rev_off + c + 1);
+          for (int sx = s0 + lane; sx < s1; sx += 32) {
+            const int i = pos[__ldg(T.rev_idx + sx) / k];
+            if (i < win_lo) rkey[i] = DIRTY;
+          }
+        }
+        __syncthreads();
+        // compaction with one shared atomic per warp (every lane takes every round)
+        for (int i0 = 0; i0 < rows; i0 += THREADS) {
+          const int i = i0 + tid;
+          const bool d = i < rows && rkey[i] == DIRTY;
+          const unsigned m = __ballot_sync(0xffffffffu, d);
+          int base = 0;
+          if (lane == 0 && m) base = atomicAdd(&S.nlist, __popc(m));
+          base = __shfl_sync(0xffffffffu, base, 0);
+          if (d) {
+            rkey[i] = NO_KEY;
+            rlist[base + __popc(m & ((1u << lane) - 1u))] = (uint16_t)i;
+          }
+        }
+        __syncthreads();
+        const int items = S.nlist * G;
+        for (int it = tid; it < items; it += THREADS) {
+          const int q = it / G;
+          const int gi = rlist[q], gr = (it - q * G) * U;
+          const unsigned long long key = group_key(gi, gr);
+          if (key != NO_KEY) atomicMin(&rkey[gi], key);
+        }
+      }
+      __syncthreads();
+      unsigned long long key = NO_KEY;
+      for (int i = tid; i < rows; i += THREADS) {
+        const unsigned long long v = rkey[i];
+        key = v < key ? v : key;
+      }
+      if (key != NO_KEY) {
+        bgain = key_gain(key);
+        bidx = (unsigned)key;
+      }
+      found = true;  // skip the per-pass scan below
+    }
     if (found) {
-      // nothing to scan: the smallest improving affected entry is the first of the pass
+      // nothing to scan: first mode's smallest improving affected entry is the first of the
+      // pass; incremental best already holds this thread's share of the row keys
     } else if constexpr (GROUPED) {
       // entries [e0 + tid*U, e0 + tid*U + U) of round e0 lie in row gi, columns gr..gr+U-1
       int gi = g_row0 + start_row, gr = g_col0;
@@ -415,7 +526,7 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
     ++moves;
     win_lo = bi;
     win_hi = bj;
-    if (MODE == TSPB_MODE_FIRST) {
+    if (track_rows) {
       // Only rows [bi, bj] (and row 0 when bj == n-1) can change their valid count.
       const int r_hi = bj < rows - 1 ? bj : rows - 1;
       const bool row0 = bj == n - 1 && bi > 0;

@@ -84,7 +84,7 @@ SIGNATURES: dict[str, tuple] = {
   "tspb_batch_offspring": (ctypes.c_int, [_p, _p, _i32, _i32, _i32, _p]),
   "tspb_batch_survival": (ctypes.c_int, [_p, _p]),
   "tspb_batch_two_opt": (ctypes.c_int, [_p, _p, _i32, _i32, _i32, _i32, _i32, _i64, _i32, _i32, _p, _p]),
-  "tspb_batch_two_opt_occupancy": (ctypes.c_int, [_i32, _i32, _i32]),
+  "tspb_batch_two_opt_occupancy": (ctypes.c_int, [_i32, _i32, _i32, _i32]),
   "tspb_batch_elite_cost": (ctypes.c_int, [_p, _i32, _p]),
   "tspb_batch_track": (ctypes.c_int, [_p, _i32, _p]),
 }
@@ -109,6 +109,7 @@ TSPB_MUT_INVERSION = 0
 TSPB_MUT_SWAP = 1
 TSPB_BATCH_COORDS = 1
 TSPB_BATCH_GROUPED = 2
+TSPB_BATCH_INCREMENTAL = 4
 
 
 class Pcg64(ctypes.Structure):
@@ -143,7 +144,8 @@ class BatchInstance(ctypes.Structure):
   """`tspb_batch_instance` of include/tspb.h."""
 
   _fields_ = [("n", _i32), ("k", _i32), ("pop_offset", _i64), ("node_offset", _i64), ("dist", _p),
-              ("dist_stride", _i64), ("coords", _p), ("cand_packed", _p), ("patience", _i64), ("optimal", _f64)]
+              ("dist_stride", _i64), ("coords", _p), ("cand_packed", _p), ("patience", _i64), ("optimal", _f64),
+              ("rev_off", _p), ("rev_idx", _p)]
 
 
 class BatchState(ctypes.Structure):
