@@ -496,7 +496,10 @@ int tspb_batch_survival(const tspb_batch* b, void* stream);
  * that fits) take units from the device counter `queue` (zeroed by this call) in item
  * order; put the largest instances first. `flags` (TSPB_BATCH_*) state what holds for
  * every item; an item that disagrees gets TSPB_ERR_UNSUPPORTED in ls_status and is left
- * unchanged. mode BEST or FIRST, candidate mode only, threads 64/128/256/512/1024.
+ * unchanged. mode BEST or FIRST, candidate mode only, threads 64/128/256/512/1024. In the
+ * RESUME, RUN and OFFSPRING phases every refined row's fitness (fit or off_fit) is
+ * rewritten from the final tour, the exact int64 sum of its edges; converged rows that are
+ * skipped keep theirs.
  * Replaces the post-init and elite refinement calls of LocalSearchCPUTourTwoOpt
  * (pipeline_steps.py:103-125, 153-195) for every run. */
 int tspb_batch_two_opt(const tspb_batch* b, const int32_t* items, int32_t num_items, int32_t max_n,
@@ -504,7 +507,9 @@ int tspb_batch_two_opt(const tspb_batch* b, const int32_t* items, int32_t num_it
                        int32_t ctas, uint32_t* queue, void* stream);
 /* Resident CTAs per SM of tspb_batch_two_opt for this shape and flags (0: does not fit). */
 int tspb_batch_two_opt_occupancy(int32_t max_n, int32_t mode, int32_t threads, int32_t flags);
-/* Fitness of the refined rows of a phase (RESUME, RUN, or OFFSPRING into off_fit). */
+/* Fitness of the refined rows of a phase (RESUME, RUN, or OFFSPRING into off_fit).
+ * tspb_batch_two_opt already stores the fitness of every row it refines in those phases;
+ * this kernel serves rows changed by other means. */
 int tspb_batch_elite_cost(const tspb_batch* b, int32_t phase, void* stream);
 /* Best tracking, history, early stops and the generation counter of a phase's instances:
  * RUN/RESUME -> HIT_OPTIMAL, NEAR_OPTIMAL, STOPPED (patience), DONE or RUN, checked in

@@ -290,11 +290,11 @@ class FusedBatchSolver:
     st = ctypes.byref(self.state)
     sh = stream_handle()
     R, U, O = native.TSPB_BATCH_PHASE_RESUME, native.TSPB_BATCH_PHASE_RUN, native.TSPB_BATCH_PHASE_OFFSPRING
+    # the 2-opt kernel stores each refined row's fitness itself (no separate cost pass)
     if self.elite:
       self._per_bucket(lambda b: self._two_opt(st, b, R))
-      native.check("tspb_batch_elite_cost", lib.tspb_batch_elite_cost(st, R, sh))
       native.check("tspb_batch_track", lib.tspb_batch_track(st, R, sh))
-      self.kernel_launches += 2
+      self.kernel_launches += 1
 
     def children(b: Bucket) -> None:
       self._offspring(st, b)
@@ -302,15 +302,10 @@ class FusedBatchSolver:
         self._two_opt(st, b, O)
 
     self._per_bucket(children)
-    if self._post_mutation:
-      native.check("tspb_batch_elite_cost", lib.tspb_batch_elite_cost(st, O, sh))
-      self.kernel_launches += 1
     native.check("tspb_batch_survival", lib.tspb_batch_survival(st, sh))
     self.kernel_launches += 3
     if self.elite:
       self._per_bucket(lambda b: self._two_opt(st, b, U))
-      native.check("tspb_batch_elite_cost", lib.tspb_batch_elite_cost(st, U, sh))
-      self.kernel_launches += 1
     native.check("tspb_batch_track", lib.tspb_batch_track(st, U, sh))
     self.kernel_launches += 1
 
@@ -318,9 +313,9 @@ class FusedBatchSolver:
     nb = len(self.buckets)
     per = nb + 3 + 1  # offspring per bucket, survival (3 kernels), track
     if self.elite:
-      per += 2 * nb + 3  # two 2-opt phases per bucket, resume cost + track, run cost
+      per += 2 * nb + 1  # two 2-opt phases per bucket, resume track
     if self._post_mutation:
-      per += nb + 1  # offspring 2-opt per bucket, offspring cost
+      per += nb  # offspring 2-opt per bucket
     return per
 
   # ------------------------------------------------------------------------ autotuning

@@ -287,6 +287,11 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value)
     T.converged = clean;
     T.rev_off = REV ? I.rev_off : nullptr;
     T.rev_idx = REV ? I.rev_idx : nullptr;
+    // the refined row's fitness (as tspb_batch_elite_cost would compute it); POSTINIT
+    // leaves fitness to tspb_batch_init (the tuner's probes refine scratch rows there)
+    T.cost = phase == TSPB_BATCH_PHASE_POSTINIT
+                 ? nullptr
+                 : (offspring ? B.off_fit : fit_buf(B, parity)) + (long long)i * B.P + row;
     scan_tour<MODE, THREADS, U, LAYOUT, REV && MODE == TSPB_MODE_BEST>(T, S);
   }
 }

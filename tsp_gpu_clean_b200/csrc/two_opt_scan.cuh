@@ -22,9 +22,9 @@
 // the minimum key of its improving entries. After a move with window [bi, bj] only the rows
 // in the window and the earlier rows with a candidate in the window can change (rows after
 // bj see the window's candidates at invalid positions), so a pass recomputes those rows
-// and reduces the row keys; long windows take a full recomputation. It pays where few CTAs
-// share an SM (the 30n bytes of tour state leave L1 to the k-NN table) and tours need few
-// passes, as for the children of locally optimal parents.
+// and reduces the row keys; long windows take a full recomputation. It computes fewer
+// gains but adds barriers and a row-key reduction to every pass, so the batch engine's
+// tuner selects it only where it measures faster.
 //
 // first with the reverse k-NN index (incremental restart): the reference restarts every
 // pass at entry 0. After a move with window [bi, bj] (the first improving entry was in row
@@ -79,6 +79,7 @@ struct ScanTour {
                        // move (the tour is then a fixed point of any further refinement)
   const int32_t* rev_off = nullptr;  // optional (first mode): CSR reverse k-NN index, n + 1 offsets
   const int32_t* rev_idx = nullptr;  // flat entries a * k + r grouped by candidate node
+  double* cost = nullptr;  // optional: the refined tour's length (exact int64 sum of eout, as float64)
 };
 
 // k-NN table layouts of scan_tour: plain int32 candidates (+ optional distances), packed
@@ -547,6 +548,12 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
   for (int p = tid; p < n; p += THREADS) g_tour[p] = tour[p];
   const long long tp = block_sum(my_pairs, S.redll);
   const long long te = block_sum(my_eval, S.redll);
+  if (T.cost != nullptr) {  // eout[x] = d(x, succ[x]) of the final tour: its edges, each once
+    long long len = 0;
+    for (int p = tid; p < n; p += THREADS) len += eout[p];
+    len = block_sum(len, S.redll);
+    if (tid == 0) *T.cost = (double)len;
+  }
   if (tid == 0) {
     if (T.moved) *T.moved = moves > 0 ? 1 : 0;
     if (T.converged) *T.converged = converged && err == TSPB_OK ? 1 : 0;
