@@ -766,6 +766,142 @@ def run_learned_bench(args) -> dict:
                     "final_loss": float(np.mean(lc.train_log[-20:]))}}
 
 
+# ------------------------------------------------------------------------ Or-opt
+OR_OPT_PASSES = 50
+OR_OPT_SEGMENT = 3
+OR_OPT_BYTES_PER_ENTRY = 12  # candidate id + d(x, c) from the k-NN tables, one gathered d(y, e)
+OR_OPT_CPU_TOURS = 6
+
+
+def _or_opt_cpu_sample(coords, cand, tours_np) -> dict:
+  """Oracle Or-opt (NumPy, one core) on the first tours of the workload, same passes."""
+  from oracle import distances as odist
+  from oracle import or_opt as oo
+
+  D = odist.euc2d_matrix(coords)
+  t0 = time.perf_counter()
+  evaluated = 0
+  outs = []
+  for t in tours_np[:OR_OPT_CPU_TOURS]:
+    out, _, _, ev = oo.refine(t, D, cand, OR_OPT_PASSES, OR_OPT_SEGMENT)
+    evaluated += ev
+    outs.append(out)
+  dt = time.perf_counter() - t0
+  return {"value": evaluated / dt, "unit": "entries/s", "cores": 1, "kind": "port", "outs": outs,
+          "sample": f"{OR_OPT_CPU_TOURS} of the tours, {OR_OPT_PASSES} passes each ({dt:.1f} s)"}
+
+
+def main_or_opt(args) -> int:
+  """Candidate Or-opt on the C2 instance: 1024 random tours, k=20, segments of up to 3
+  cities, 50 best-improvement passes per tour; metric = valid entries evaluated per second."""
+  import torch
+
+  from tsp_gpu_clean_b200 import native
+  from tsp_gpu_clean_b200.build import build_library
+  from tsp_gpu_clean_b200.device import operands_for, ptr, stream_handle
+  from tsp_gpu_clean_b200.problem import Problem, ProblemContext
+  from tsp_gpu_clean_b200.strategies.or_opt import LocalSearchB200OrOpt
+
+  world, rank, _ = _dist_env()
+  n = instances.C2_N
+  coords, _ = instances.c2_workload(tours=1)
+  tours_np = instances.random_tours(n, args.tours, instances.C2_TOUR_SEED + 1000 * rank)
+  ctx = ProblemContext(Problem.from_coordinates(coords, "c2"), seed=0)
+  cand_np = ctx.get_cpu_candidate_list(K_CAND)
+  config = {"workload": f"Or-opt (best improvement, candidate_k={K_CAND}, segments <= {OR_OPT_SEGMENT}, "
+                        f"{OR_OPT_PASSES} passes) on random tours of the 1000-city 20-cluster EUC_2D instance",
+            "tours": args.tours, "n": n, "k": K_CAND, "passes": OR_OPT_PASSES,
+            "l2": "flushed between timed steps (256 MiB write)"}
+  metric = "Or-opt entries evaluated/s"
+  if args.impl == "reference":
+    if rank != 0:
+      return 0
+    cpu = _or_opt_cpu_sample(coords, cand_np, tours_np)
+    print(json.dumps({"metric": metric, "value": cpu["value"], "unit": "entries/s", "n_gpus": args.gpus,
+                      "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                      "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)", "impl": "reference",
+                      "config": config,
+                      "cpu_baseline": {k: v for k, v in cpu.items() if k != "outs"},
+                      "e2e": {"value": cpu["value"], "unit": "entries/s", "h2d_bytes_per_step": 0,
+                              "d2h_bytes_per_step": 0}}))
+    return 0
+  torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+  build_library()
+  lib = native.load_library()
+  ops = operands_for(ctx)
+  dist_t, stride, _ = ops.distance_args(n)
+  tabs = ops.candidates(K_CAND, cand_np, n)
+  pristine = torch.from_numpy(tours_np).cuda()
+  work = torch.empty_like(pristine)
+  stats = torch.zeros((args.tours, 3), dtype=torch.int64, device="cuda")
+  status = torch.zeros(args.tours, dtype=torch.int32, device="cuda")
+  flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+  def launch():
+    native.check("tspb_or_opt", lib.tspb_or_opt(ptr(work), args.tours, n, ptr(dist_t), stride, None, ptr(tabs.cand),
+                                                 ptr(tabs.cand_dist), tabs.k, OR_OPT_SEGMENT, OR_OPT_PASSES, 256,
+                                                 ptr(status), ptr(stats), stream_handle()))
+
+  for _ in range(args.warmup):
+    work.copy_(pristine)
+    launch()
+  torch.cuda.synchronize()
+  _barrier(world)
+  ms, evaluated, launches = [], 0, 0
+  with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+    for _ in range(args.steps):
+      work.copy_(pristine)
+      flush.fill_(1)
+      e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+      e0.record()
+      launch()
+      e1.record()
+      torch.cuda.synchronize()
+      ms.append(e0.elapsed_time(e1))
+      evaluated += int(stats[:, 2].sum().item())
+      launches += 1
+  if int(status.max().item()) != 0:
+    raise RuntimeError(f"Or-opt kernel reported {native.status_text(int(status.max().item()))}")
+  device_out = work.cpu().numpy()
+  _barrier(world)
+  units, secs = aggregate(evaluated, sum(ms) / 1e3, world)
+  # end to end through the strategy: host tours in, host tours out
+  ls = LocalSearchB200OrOpt(max_iterations=OR_OPT_PASSES, candidate_k=K_CAND, max_segment=OR_OPT_SEGMENT)
+  ls.improve_batch(tours_np[:2], ctx)
+  walls, e2e_eval = [], 0
+  for _ in range(args.steps):
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    out = ls.improve_batch(tours_np, ctx)
+    walls.append(time.perf_counter() - t0)
+    e2e_eval += int(ls.last_stats[:, 2].sum())
+  assert np.array_equal(out, device_out)
+  e2e_units, e2e_s = aggregate(e2e_eval, sum(walls), world)
+  _finish_ranks(world)
+  if rank != 0:
+    return 0
+  line = {"metric": metric, "value": units / secs, "unit": "entries/s", "n_gpus": world, "steps": args.steps,
+          "warmup": args.warmup, "ms_per_step": sum(ms) / len(ms), "higher_is_better": True, "scaling": "weak",
+          "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)", "config": config,
+          "clocks": clocks.summary(),
+          "e2e": {"value": e2e_units / e2e_s, "unit": "entries/s", "h2d_bytes_per_step": int(tours_np.nbytes),
+                  "d2h_bytes_per_step": int(tours_np.nbytes)},
+          "gpu_launches": launches}
+  per_launch = evaluated / len(ms) * OR_OPT_BYTES_PER_ENTRY
+  peaks = _peaks()
+  achieved = per_launch / (sum(ms) / len(ms) / 1e3) / 1e9
+  line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                      "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                      "note": f"{OR_OPT_BYTES_PER_ENTRY} B per valid entry; peak {peaks['source']}"}
+  if world == 1 and not args.no_cpu_baseline:
+    cpu = _or_opt_cpu_sample(coords, cand_np, tours_np)
+    for t, o in enumerate(cpu["outs"]):
+      assert np.array_equal(o, device_out[t]), t
+    line["cpu_baseline"] = {k: v for k, v in cpu.items() if k != "outs"}
+  print(json.dumps(line))
+  return 0
+
+
 def main(argv=None) -> int:
   ap = argparse.ArgumentParser()
   ap.add_argument("--gpus", type=int, default=1)
@@ -787,7 +923,7 @@ def main(argv=None) -> int:
                        "recomputed; first: incremental restart); auto lets the tuner measure both")
   ap.add_argument("--cpu-workers", type=int, default=0, help="0: all host cores, capped at 64")
   ap.add_argument("--no-cpu-baseline", action="store_true")
-  ap.add_argument("--workload", default="two_opt", choices=["two_opt", "learned", "uneven", *GA_WORKLOADS])
+  ap.add_argument("--workload", default="two_opt", choices=["two_opt", "learned", "uneven", "or_opt", *GA_WORKLOADS])
   ap.add_argument("--instances", type=int, default=256, help="uneven: instances in the batch")
   ap.add_argument("--generations", type=int, default=100, help="uneven: generations")
   ap.add_argument("--train-instances", type=int, default=2000)
@@ -815,6 +951,8 @@ def main(argv=None) -> int:
     return 0
   if args.workload == "uneven":
     return main_uneven(args)
+  if args.workload == "or_opt":
+    return main_or_opt(args)
   if args.workload != "two_opt":
     return main_ga(args)
   world, rank, _ = _dist_env()

@@ -280,6 +280,26 @@ int tspb_three_opt(int32_t* tours, int32_t num_tours, int32_t n, const int32_t* 
                    size_t workspace_bytes, int32_t* status, int64_t* stats, void* stream);
 int tspb_three_opt_workspace_bytes(int32_t n, int32_t ctas, size_t* bytes);
 
+/*
+ * Candidate-list Or-opt of open (cyclic TSP) tours in place, best improvement, up to
+ * max_iterations passes each. No reference counterpart (the reference's local search has
+ * 2-opt and an experimental 3-opt); it widens the family with the reference's candidate
+ * 2-opt conventions (src/algorithms/strategies/local_search/two_opt.py:347-367: k-NN
+ * candidates, position 0 fixed, exact integer deltas, first move in scan order on ties).
+ * A move relocates t[i .. i+L-1] (1 <= L <= max_segment <= 8, i >= 1) after a candidate c
+ * of its first city (forward) or of its last city (reversed, L >= 2); the move applied is
+ * the smallest negative delta, then the smallest key (((i-1)*max_segment + L-1)*k + r)*2 + o.
+ * cand / cand_dist: n x k k-NN ids and d(a, cand) (1 <= k <= n-1, symmetric distances);
+ * distances from `dist` (n x dist_stride) or rebuilt from EUC_2D `coords`. One CTA per
+ * tour (persistent), `threads` 128, 256 or 512, 16 n bytes of shared memory
+ * (n <= tspb_or_opt_max_n()). n < 3: nothing to do. stats (optional): [tours][3] passes,
+ * moves, valid entries evaluated.
+ */
+int tspb_or_opt(int32_t* tours, int32_t num_tours, int32_t n, const int32_t* dist, int64_t dist_stride,
+                const double* coords, const int32_t* cand, const int32_t* cand_dist, int32_t k, int32_t max_segment,
+                int64_t max_iterations, int32_t threads, int32_t* status, int64_t* stats, void* stream);
+int tspb_or_opt_max_n(void);
+
 /* Coordinate-based TSPLIB edge weight types (src/distances/matrix.py:39-41). */
 #define TSPB_EDGE_EUC_2D 0
 #define TSPB_EDGE_EUC_3D 1

@@ -28,6 +28,7 @@ from tsp_gpu_clean_b200.strategies import (  # noqa: E402
   EvaluationB200Cost,
   InitializationB200PermRandom,
   InitializationB200TourNearestNeighbor,
+  LocalSearchB200OrOpt,
   LocalSearchB200ThreeOpt,
   LocalSearchB200TourTwoOpt,
   MutationB200PermInversion,
@@ -43,6 +44,7 @@ __all__ = [
   "FusedGeneticAlgorithm",
   "InitializationB200PermRandom",
   "InitializationB200TourNearestNeighbor",
+  "LocalSearchB200OrOpt",
   "LocalSearchB200ThreeOpt",
   "LocalSearchB200TourTwoOpt",
   "MutationB200PermInversion",

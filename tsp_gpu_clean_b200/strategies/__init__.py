@@ -4,6 +4,7 @@ from __future__ import annotations
 
 from .initialization import InitializationB200PermRandom, InitializationB200TourNearestNeighbor
 from .local_search import LocalSearchB200TourTwoOpt
+from .or_opt import LocalSearchB200OrOpt
 from .three_opt import LocalSearchB200ThreeOpt
 from .operators import (
   CrossoverB200PermOrder,
@@ -20,6 +21,7 @@ STRATEGY_REGISTRY: dict[str, type] = {
   "EvaluationB200Cost": EvaluationB200Cost,
   "InitializationB200PermRandom": InitializationB200PermRandom,
   "InitializationB200TourNearestNeighbor": InitializationB200TourNearestNeighbor,
+  "LocalSearchB200OrOpt": LocalSearchB200OrOpt,
   "LocalSearchB200ThreeOpt": LocalSearchB200ThreeOpt,
   "LocalSearchB200TourTwoOpt": LocalSearchB200TourTwoOpt,
   "MutationB200PermInversion": MutationB200PermInversion,
@@ -58,6 +60,7 @@ __all__ = [
   "EvaluationB200Cost",
   "InitializationB200PermRandom",
   "InitializationB200TourNearestNeighbor",
+  "LocalSearchB200OrOpt",
   "LocalSearchB200ThreeOpt",
   "LocalSearchB200TourTwoOpt",
   "MutationB200PermInversion",
