@@ -527,10 +527,6 @@ int tspb_batch_two_opt(const tspb_batch* b, const int32_t* items, int32_t num_it
                        int32_t ctas, uint32_t* queue, void* stream);
 /* Resident CTAs per SM of tspb_batch_two_opt for this shape and flags (0: does not fit). */
 int tspb_batch_two_opt_occupancy(int32_t max_n, int32_t mode, int32_t threads, int32_t flags);
-/* Fitness of the refined rows of a phase (RESUME, RUN, or OFFSPRING into off_fit).
- * tspb_batch_two_opt already stores the fitness of every row it refines in those phases;
- * this kernel serves rows changed by other means. */
-int tspb_batch_elite_cost(const tspb_batch* b, int32_t phase, void* stream);
 /* Best tracking, history, early stops and the generation counter of a phase's instances:
  * RUN/RESUME -> HIT_OPTIMAL, NEAR_OPTIMAL, STOPPED (patience), DONE or RUN, checked in
  * that order (genetic_algorithm.py:876-910). */

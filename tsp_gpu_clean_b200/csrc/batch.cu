@@ -287,38 +287,13 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value)
     T.converged = clean;
     T.rev_off = REV ? I.rev_off : nullptr;
     T.rev_idx = REV ? I.rev_idx : nullptr;
-    // the refined row's fitness (as tspb_batch_elite_cost would compute it); POSTINIT
-    // leaves fitness to tspb_batch_init (the tuner's probes refine scratch rows there)
+    // the refined row's fitness (fit, or off_fit for children); POSTINIT leaves fitness
+    // to tspb_batch_init (the tuner's probes refine scratch rows there)
     T.cost = phase == TSPB_BATCH_PHASE_POSTINIT
                  ? nullptr
                  : (offspring ? B.off_fit : fit_buf(B, parity)) + (long long)i * B.P + row;
     scan_tour<MODE, THREADS, U, LAYOUT, REV && MODE == TSPB_MODE_BEST>(T, S);
   }
-}
-
-// CTA per (instance, refined row) of a phase: fitness after the 2-opt (of the offspring
-// rows into off_fit in the OFFSPRING phase), an exact int64 sum over the CTA.
-__global__ void __launch_bounds__(128) batch_elite_cost_kernel(const tspb_batch B, int phase) {
-  __shared__ long long red[32];
-  const long long w = blockIdx.x;
-  const bool offspring = phase == TSPB_BATCH_PHASE_OFFSPRING;
-  const int e_count = offspring ? B.P : B.elite;
-  if (w >= (long long)B.num_instances * e_count) return;
-  const int i = (int)(w / e_count), e = (int)(w - (long long)i * e_count);
-  const int* c = B.ctl + 4 * i;
-  if (c[1] != phase_state(phase)) return;  // uniform per CTA
-  const int parity = (c[0] + 1) & 1;
-  const int row = phase == TSPB_BATCH_PHASE_RESUME ? B.host_elites[(long long)i * e_count + e] : e;
-  if ((unsigned)row >= (unsigned)B.P) return;
-  const tspb_batch_instance I = B.inst[i];
-  const int32_t* tour = (offspring ? B.off : pop_buf(B, parity)) + I.pop_offset + (long long)row * I.n;
-  const DistSrc ds = inst_ds(I);
-  const int n = I.n;
-  long long acc = 0;
-  for (int p = threadIdx.x; p < n; p += blockDim.x) acc += ds(tour[p], tour[p + 1 == n ? 0 : p + 1]);
-  acc = block_sum(acc, red);
-  if (threadIdx.x == 0)
-    (offspring ? B.off_fit : fit_buf(B, parity))[(long long)i * B.P + row] = n <= 1 ? 0.0 : (double)acc;
 }
 
 // CTA per instance of a phase: argmin of fitness (first minimum), strict improvement by
@@ -583,19 +558,6 @@ extern "C" int tspb_batch_two_opt(const tspb_batch* b, const int32_t* items, int
                                               ctas, flags, queue, st);
   return batch_two_opt_mode<TSPB_MODE_FIRST>(*b, items, num_items, rows, phase, max_iterations, max_n, threads, smem,
                                              ctas, flags, queue, st);
-}
-
-extern "C" int tspb_batch_elite_cost(const tspb_batch* b, int32_t phase, void* stream) {
-  if (!batch_ok(b) || (phase != TSPB_BATCH_PHASE_RESUME && phase != TSPB_BATCH_PHASE_RUN &&
-                       phase != TSPB_BATCH_PHASE_OFFSPRING))
-    return TSPB_ERR_ARG;
-  const int rows = phase == TSPB_BATCH_PHASE_OFFSPRING ? b->P : b->elite;
-  if (b->num_instances == 0 || rows == 0 || b->G == 0) return TSPB_OK;
-  if (phase == TSPB_BATCH_PHASE_RESUME && !b->host_elites) return TSPB_ERR_ARG;
-  const long long ctas = (long long)b->num_instances * rows;
-  if (ctas > 0x7fffffffLL) return TSPB_ERR_UNSUPPORTED;
-  batch_elite_cost_kernel<<<(unsigned)ctas, 128, 0, reinterpret_cast<cudaStream_t>(stream)>>>(*b, phase);
-  return tspb_launch_status();
 }
 
 extern "C" int tspb_batch_track(const tspb_batch* b, int32_t phase, void* stream) {

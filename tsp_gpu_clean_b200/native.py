@@ -87,7 +87,6 @@ SIGNATURES: dict[str, tuple] = {
   "tspb_batch_survival": (ctypes.c_int, [_p, _p]),
   "tspb_batch_two_opt": (ctypes.c_int, [_p, _p, _i32, _i32, _i32, _i32, _i32, _i64, _i32, _i32, _p, _p]),
   "tspb_batch_two_opt_occupancy": (ctypes.c_int, [_i32, _i32, _i32, _i32]),
-  "tspb_batch_elite_cost": (ctypes.c_int, [_p, _i32, _p]),
   "tspb_batch_track": (ctypes.c_int, [_p, _i32, _p]),
 }
 
