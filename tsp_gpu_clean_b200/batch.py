@@ -48,7 +48,7 @@ import numpy as np
 
 from . import native
 from .autotune import BatchAutotuner
-from .device import candidate_list, operands_for, ptr, require_gpu, stream_handle, torch
+from .device import candidate_list, check_packed, operands_for, ptr, require_gpu, stream_handle, torch
 from .fused import LocalSearchConfig, draw_generation_tape
 from .problem import resolve_rng
 from .strategies.initialization import draw_row_seeds
@@ -578,6 +578,7 @@ class FusedBatchSolver:
     coords_flags = []
     rebuildable = []
     t_ops = t_tape = 0.0
+    all_tabs = []
     for i, (ctx, n, rng) in enumerate(zip(contexts, ns, rngs)):
       seeds_all[i] = draw_row_seeds(rng, P)  # nearest_neighbor_init.py:118-121, random_init.py:42
       if self.init == "nn":
@@ -586,8 +587,9 @@ class FusedBatchSolver:
       ops = operands_for(ctx)
       dist, stride, coords = ops.distance_args(n, self.max_matrix_dimension)
       tabs = ops.candidates(k, candidate_list(ctx, k), n, self.max_matrix_dimension)
-      if tabs.packed is None:
+      if tabs.packed_words is None:
         raise ValueError(f"instance {i}: k-NN table does not pack into 16-bit ids and distances")
+      all_tabs.append(tabs)
       t_ops += time.perf_counter() - t0
       self._keep.append((dist, coords, tabs))
       inst = h_inst[i]
@@ -602,7 +604,7 @@ class FusedBatchSolver:
       inst.coords = xy.data_ptr() if xy is not None else None
       rebuildable.append(xy is not None)
       self._keep.append(xy)
-      inst.cand_packed = tabs.packed.data_ptr()
+      inst.cand_packed = tabs.packed_words.data_ptr()
       inst.rev_off = tabs.rev_off.data_ptr()
       inst.rev_idx = tabs.rev_idx.data_ptr()
       pat = patience[i] if isinstance(patience, (list, tuple, np.ndarray)) else patience
@@ -610,6 +612,12 @@ class FusedBatchSolver:
       opt = optimal_cost[i] if isinstance(optimal_cost, (list, tuple, np.ndarray)) else optimal_cost
       inst.optimal = float(opt) if opt is not None and opt > 0 else 0.0
       coords_flags.append(dist is None)
+    t0 = time.perf_counter()
+    check_packed(all_tabs)  # every instance's pack-overflow flag in one sync
+    bad = [i for i, t in enumerate(all_tabs) if t.packed is None]
+    if bad:
+      raise ValueError(f"instance {bad[0]}: k-NN table does not pack into 16-bit ids and distances")
+    t_ops += time.perf_counter() - t0
     t0 = time.perf_counter()
     if self.init == "nn":
       self._nn_init(h_jobs, seeds_all, nn_tables, ns)

@@ -48,10 +48,24 @@ def ptr(t) -> ctypes.c_void_p | None:
   return ctypes.c_void_p(t.data_ptr())
 
 
+#: Arrays up to this size are staged through pinned memory (see device_tensor).
+_PINNED_COPY_MAX = 64 << 20
+
+
 def device_tensor(a: np.ndarray, dtype) -> "torch.Tensor":
-  """H2D copy of a host array (C-contiguous) to the current device."""
+  """H2D copy of a host array to the current device, stream-ordered.
+
+  The array is first copied into pinned memory (torch's caching host allocator keeps that
+  block until the copy has run), so the call does not wait for the device; a blocking copy
+  from pageable memory would synchronise the stream every time."""
   t = torch.from_numpy(np.ascontiguousarray(a))
-  return t.to(device="cuda", dtype=dtype)
+  if t.dtype != dtype:
+    t = t.to(dtype)
+  if t.numel() == 0:
+    return torch.empty(t.shape, dtype=dtype, device="cuda")
+  if t.numel() * t.element_size() > _PINNED_COPY_MAX:
+    return t.to(device="cuda")  # large one-off arrays: not worth a cached pinned block
+  return t.pin_memory().to(device="cuda", non_blocking=True)
 
 
 _SM_COUNT: int | None = None
@@ -132,14 +146,46 @@ MAX_DISTANCE = (1 << 30) - 1
 
 
 class CandidateTables:
-  """Device k-NN table, its distances and its reverse index (CSR)."""
+  """Device k-NN table, its distances, its reverse index (CSR) and the packed words.
 
-  def __init__(self, cand, cand_dist, rev_off, rev_idx, packed=None):
+  The packing kernel flags entries that do not fit 16 bits on the device; the flag is read
+  on the first use of `packed` (None when an entry overflowed), or for many tables at once
+  with `check_packed`, so building the tables does not wait for the device."""
+
+  def __init__(self, cand, cand_dist, rev_off, rev_idx, packed=None, overflow=None):
     self.cand = cand
     self.cand_dist = cand_dist
     self.rev_off = rev_off
     self.rev_idx = rev_idx
-    self.packed = packed
+    self._packed = packed
+    self._overflow = overflow if packed is not None else None
+
+  @property
+  def packed(self):
+    if self._overflow is not None:
+      check_packed([self])
+    return self._packed
+
+  @property
+  def packed_words(self):
+    """The packed table before its overflow flag is read (callers then use check_packed)."""
+    return self._packed
+
+  @property
+  def k(self) -> int:
+    return int(self.cand.shape[1])
+
+
+def check_packed(tables) -> None:
+  """Read the pack-overflow flags of many CandidateTables with one device sync."""
+  pending = [t for t in tables if t._overflow is not None]
+  if not pending:
+    return
+  flags = torch.cat([t._overflow for t in pending]).cpu().numpy()
+  for t, f in zip(pending, flags):
+    if int(f) != 0:
+      t._packed = None
+    t._overflow = None
 
   @property
   def k(self) -> int:
@@ -294,14 +340,12 @@ class DeviceOperands:
     if rows and kk:
       call("tspb_candidate_distances", ptr(d_cand), rows, kk, ptr(dist), stride, ptr(coords), ptr(d_cd), stream_handle())
       call("tspb_candidate_reverse_index", ptr(d_cand), rows, kk, ptr(rev_off), ptr(rev_idx), ptr(scratch), stream_handle())
-    packed = None
+    packed = overflow = None
     if rows and kk and rows <= 0xFFFF:
       packed = torch.empty((rows, kk), dtype=torch.int32, device="cuda")
-      overflow = torch.zeros(1, dtype=torch.int32, device="cuda")
+      overflow = torch.empty(1, dtype=torch.int32, device="cuda")  # zeroed by tspb_candidate_pack
       call("tspb_candidate_pack", ptr(d_cand), ptr(d_cd), rows, kk, ptr(packed), ptr(overflow), stream_handle())
-      if int(overflow.item()) != 0:
-        packed = None
-    tables = CandidateTables(d_cand, d_cd, rev_off, rev_idx, packed)
+    tables = CandidateTables(d_cand, d_cd, rev_off, rev_idx, packed, overflow)
     self._cand[key] = (table, tables)
     return tables
 
