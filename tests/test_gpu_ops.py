@@ -192,3 +192,21 @@ def test_nn_init_jobs_shared_memory_matches_workspace_kernel(torch_mod):
   lib = native.load_library()
   assert lib.tspb_nn_init_jobs_smem(ptr(j1), 1, 1, 70000, 5, None) == native.TSPB_ERR_UNSUPPORTED
   assert lib.tspb_nn_init_jobs_smem(None, 1, 1, 100, 5, None) == native.TSPB_ERR_ARG
+
+
+def test_check_free_counts_cached_memory_and_rejects_impossible_requests(torch_mod, monkeypatch):
+  """check_free reads torch's allocator counters first (no driver call when its cached
+  memory covers the request) and raises VRAMInsufficientError for more than the device has."""
+  from tsp_gpu_clean_b200.device import check_free
+  from tsp_gpu_clean_b200.errors import VRAMInsufficientError
+
+  block = torch_mod.empty(64 << 20, dtype=torch_mod.uint8, device="cuda")
+  del block  # the 64 MiB stay reserved by the caching allocator
+  calls = []
+  real = torch_mod.cuda.mem_get_info
+  monkeypatch.setattr(torch_mod.cuda, "mem_get_info", lambda *a: calls.append(1) or real(*a))
+  check_free(32 << 20, "a request the cache covers")
+  assert calls == []
+  with pytest.raises(VRAMInsufficientError):
+    check_free(1 << 50, "a petabyte")
+  assert calls == [1]
