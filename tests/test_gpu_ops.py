@@ -210,3 +210,30 @@ def test_check_free_counts_cached_memory_and_rejects_impossible_requests(torch_m
   with pytest.raises(VRAMInsufficientError):
     check_free(1 << 50, "a petabyte")
   assert calls == [1]
+
+
+def test_euc2d_rounding_boundaries_match_the_reference_formula(torch_mod):
+  """Distances on and around half-integers (where a float root alone could round the other
+  way), at several scales, equal NumPy's `int64(sqrt(dx*dx + dy*dy) + 0.5)`."""
+  from tsp_gpu_clean_b200 import native
+  from tsp_gpu_clean_b200.device import ptr, stream_handle
+
+  torch = torch_mod
+  rng = np.random.default_rng(77)
+  pts = [(0.0, 0.0)]
+  for m in (0, 1, 2, 7, 100, 1414, 4095, 30000, 65534, 200000, 1 << 20):
+    for eps in (0.0, 1e-12, -1e-12, 1e-9, -1e-9, 1e-6, -1e-6, 1e-4, -1e-4, 3e-3, -3e-3):
+      pts.append((0.0, m + 0.5 + eps))
+      a = rng.uniform(0, np.pi / 2)
+      r = m + 0.5 + eps
+      pts.append((r * np.cos(a), r * np.sin(a)))
+  # Pythagorean-style exact half-integers: (1.5, 2) -> 2.5, scaled
+  for k in (1, 3, 101, 1001, 20001):
+    pts.append((1.5 * k, 2.0 * k))
+  pts += [tuple(p) for p in rng.uniform(0, 1000, (200, 2))]
+  coords = np.asarray(pts, dtype=np.float64)
+  n = len(coords)
+  d = torch.empty((n, n), dtype=torch.int32, device="cuda")
+  dc = torch.from_numpy(np.ascontiguousarray(coords)).cuda()
+  native.call("tspb_euc2d_matrix", ptr(dc), n, ptr(d), n, stream_handle())
+  assert np.array_equal(d.cpu().numpy(), odist.euc2d_matrix(coords))
