@@ -127,3 +127,54 @@ def test_or_opt_errors(torch_mod):
   assert lib.tspb_or_opt(p(t), 1, 30, None, 0, None, p(c), p(c), 4, 3, 10, 256, p(st), None, None) == native.TSPB_ERR_ARG
   assert lib.tspb_or_opt(p(t), 1, 2, p(d), 30, None, p(c), p(c), 1, 3, 10, 256, p(st), None, None) == native.TSPB_OK
   assert lib.tspb_or_opt_max_n() > 10000
+
+
+class _OracleOrOpt:
+  """Test-only LocalSearchStrategy: the oracle's Or-opt on host arrays."""
+
+  def __init__(self, coords, table, iters, S):
+    self.D = odist.euc2d_matrix(coords)
+    self.table, self.iters, self.S = table, iters, S
+
+  def improve(self, route, context):
+    return self.improve_batch(np.asarray(route)[None, :], context)[0]
+
+  def improve_batch(self, routes, context):
+    routes = np.asarray(routes, dtype=np.int32)
+    return np.stack([oo.refine(r, self.D, self.table, self.iters, self.S)[0] for r in routes]).astype(np.int32)
+
+
+def test_or_opt_drops_into_the_ga_pipeline(torch_mod):
+  """The reference-shaped GA (post-init and elite local-search steps) with
+  LocalSearchB200OrOpt equals the same pipeline whose local search is the oracle."""
+  from tsp_gpu_clean_b200.device import candidate_list
+  from tsp_gpu_clean_b200.ga import GeneticAlgorithm
+  from tsp_gpu_clean_b200.pipeline_steps import EliteOnlyLocalSearchStep, PostInitLocalSearchStep
+  from tsp_gpu_clean_b200.strategies import (
+    CrossoverB200PermPartiallyMapped,
+    EvaluationB200Cost,
+    InitializationB200TourNearestNeighbor,
+    LocalSearchB200OrOpt,
+    MutationB200PermInversion,
+    SelectionB200Tournament,
+  )
+
+  coords = instances.uniform_instance(90, 31)
+  runs = []
+  for which in ("b200", "oracle"):
+    ctx = _ctx(coords)
+    ls = (LocalSearchB200OrOpt(max_iterations=6, candidate_k=10) if which == "b200"
+          else _OracleOrOpt(coords, candidate_list(ctx, 10), 6, 3))
+    ev = EvaluationB200Cost()
+    steps = [PostInitLocalSearchStep(local_search=ls, evaluation=ev),
+             EliteOnlyLocalSearchStep(local_search=ls, evaluation=ev, elite_count=6)]
+    ga = GeneticAlgorithm(population_size=32, mutation_rate=0.1, seed=42,
+                          initialization=InitializationB200TourNearestNeighbor(k=5, seed=42),
+                          selection=SelectionB200Tournament(k=5, seed=42),
+                          crossover=CrossoverB200PermPartiallyMapped(seed=42),
+                          mutation=MutationB200PermInversion(seed=42), local_search=ls, evaluation=ev,
+                          pipeline=steps)
+    best, stats = ga.evolve(context=ctx, customers=list(range(90)), max_generations=12, patience=10**9)
+    runs.append((np.asarray(best), list(stats["convergence_history"])))
+  assert np.array_equal(runs[0][0], runs[1][0])
+  assert runs[0][1] == runs[1][1]
