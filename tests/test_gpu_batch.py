@@ -264,3 +264,27 @@ def test_many_small_runs_device_tape_match_oracle(batch_mod):
   assert solver._dev_states is not None
   for idx, (coords, seed) in enumerate(insts):
     _check_run(solver, res, ctxs, idx, _oracle_run(coords, seed, 10, 0.2, 3, True, "best", 5, 6, 6, 10**9))
+
+
+def test_sharded_solver_on_one_rank_equals_the_batch_solver(batch_mod):
+  """Without a process group the sharded solver runs every instance on one batch solver:
+  the same best tours and costs as FusedBatchSolver.evolve."""
+  from tsp_gpu_clean_b200.fused import LocalSearchConfig
+  from tsp_gpu_clean_b200.instances import uneven_batch
+  from tsp_gpu_clean_b200.problem import Problem, ProblemContext
+  from tsp_gpu_clean_b200.sharding import ShardedBatchSolver
+
+  coords = uneven_batch(5, 33, n_min=20, n_max=300)
+
+  def make():
+    return batch_mod.FusedBatchSolver(population_size=24, elite_count=4,
+                                      local_search=LocalSearchConfig("best", 10, 20))
+
+  ref = make().evolve([ProblemContext(Problem.from_coordinates(c), seed=60 + i) for i, c in enumerate(coords)], 8,
+                      patience=10**9)
+  sharded = ShardedBatchSolver(make, population_size=24)
+  got = sharded.evolve([ProblemContext(Problem.from_coordinates(c), seed=60 + i) for i, c in enumerate(coords)], 8,
+                       patience=10**9)
+  assert sharded.plan == [list(range(5))]
+  for (best, stats), (tour, cost) in zip(ref, got):
+    assert np.array_equal(best, tour) and cost == stats["best_fitness"]
