@@ -771,6 +771,7 @@ OR_OPT_PASSES = 50
 OR_OPT_SEGMENT = 3
 OR_OPT_BYTES_PER_ENTRY = 12  # candidate id + d(x, c) from the k-NN tables, one gathered d(y, e)
 OR_OPT_CPU_TOURS = 6
+OR_OPT_THREADS = 128  # fastest of 128 / 256 / 512 threads per CTA here
 
 
 def _or_opt_cpu_sample(coords, cand, tours_np) -> dict:
@@ -811,7 +812,7 @@ def main_or_opt(args) -> int:
   config = {"workload": f"Or-opt (best improvement, candidate_k={K_CAND}, segments <= {OR_OPT_SEGMENT}, "
                         f"{OR_OPT_PASSES} passes) on random tours of the 1000-city 20-cluster EUC_2D instance",
             "tours": args.tours, "n": n, "k": K_CAND, "passes": OR_OPT_PASSES,
-            "l2": "flushed between timed steps (256 MiB write)"}
+            "threads_per_cta": OR_OPT_THREADS, "l2": "flushed between timed steps (256 MiB write)"}
   metric = "Or-opt entries evaluated/s"
   if args.impl == "reference":
     if rank != 0:
@@ -839,7 +840,7 @@ def main_or_opt(args) -> int:
 
   def launch():
     native.check("tspb_or_opt", lib.tspb_or_opt(ptr(work), args.tours, n, ptr(dist_t), stride, None, ptr(tabs.cand),
-                                                 ptr(tabs.cand_dist), tabs.k, OR_OPT_SEGMENT, OR_OPT_PASSES, 256,
+                                                 ptr(tabs.cand_dist), tabs.k, OR_OPT_SEGMENT, OR_OPT_PASSES, OR_OPT_THREADS,
                                                  ptr(status), ptr(stats), stream_handle()))
 
   for _ in range(args.warmup):

@@ -33,7 +33,7 @@ class LocalSearchB200OrOpt(StrategyBase):
   """Candidate-list Or-opt (segments of 1..max_segment cities), one CTA per tour."""
 
   def __init__(self, max_iterations: int = 10, candidate_k: int = 20, max_segment: int = 3,
-               threads_per_block: int = 256, max_matrix_dimension: int | None = None) -> None:
+               threads_per_block: int = 128, max_matrix_dimension: int | None = None) -> None:
     super().__init__()
     if max_iterations < 0:
       raise ValueError(f"max_iterations must be >= 0, got {max_iterations}")
@@ -87,6 +87,7 @@ class LocalSearchB200OrOpt(StrategyBase):
       host = np.ascontiguousarray(batch, dtype=np.int32)
       d_tours = self._stager.upload(host, torch.int32)
       self.h2d_bytes += host.nbytes
+    # 128 is fastest on the 1024-tour, n = 1000 workload (27.9 ms vs 32.3 ms at 256, 30.3 at 512)
     threads = 512 if self.threads_per_block >= 512 else (256 if self.threads_per_block >= 256 else 128)
     stats = torch.empty((num, 3), dtype=torch.int64, device="cuda")
     status = torch.empty(num, dtype=torch.int32, device="cuda")
