@@ -840,7 +840,8 @@ def main_or_opt(args) -> int:
 
   def launch():
     native.check("tspb_or_opt", lib.tspb_or_opt(ptr(work), args.tours, n, ptr(dist_t), stride, None, ptr(tabs.cand),
-                                                 ptr(tabs.cand_dist), tabs.k, OR_OPT_SEGMENT, OR_OPT_PASSES, OR_OPT_THREADS,
+                                                 ptr(tabs.cand_dist), ptr(tabs.packed), tabs.k, OR_OPT_SEGMENT,
+                                                 OR_OPT_PASSES, OR_OPT_THREADS,
                                                  ptr(status), ptr(stats), stream_handle()))
 
   for _ in range(args.warmup):

@@ -290,14 +290,17 @@ int tspb_three_opt_workspace_bytes(int32_t n, int32_t ctas, size_t* bytes);
  * of its first city (forward) or of its last city (reversed, L >= 2); the move applied is
  * the smallest negative delta, then the smallest key (((i-1)*max_segment + L-1)*k + r)*2 + o.
  * cand / cand_dist: n x k k-NN ids and d(a, cand) (1 <= k <= n-1, symmetric distances);
+ * cand_packed (optional): the same as c | d << 16 words (tspb_candidate_pack, no overflow),
+ * read four at a time when k % 4 == 0 and the table is 16-byte aligned;
  * distances from `dist` (n x dist_stride) or rebuilt from EUC_2D `coords`. One CTA per
  * tour (persistent), `threads` 128, 256 or 512, 16 n bytes of shared memory
  * (n <= tspb_or_opt_max_n()). n < 3: nothing to do. stats (optional): [tours][3] passes,
  * moves, valid entries evaluated.
  */
 int tspb_or_opt(int32_t* tours, int32_t num_tours, int32_t n, const int32_t* dist, int64_t dist_stride,
-                const double* coords, const int32_t* cand, const int32_t* cand_dist, int32_t k, int32_t max_segment,
-                int64_t max_iterations, int32_t threads, int32_t* status, int64_t* stats, void* stream);
+                const double* coords, const int32_t* cand, const int32_t* cand_dist, const uint32_t* cand_packed,
+                int32_t k, int32_t max_segment, int64_t max_iterations, int32_t threads, int32_t* status,
+                int64_t* stats, void* stream);
 int tspb_or_opt_max_n(void);
 
 /* Coordinate-based TSPLIB edge weight types (src/distances/matrix.py:39-41). */

@@ -122,10 +122,10 @@ def test_or_opt_errors(torch_mod):
   c = torch_mod.zeros((30, 4), dtype=torch_mod.int32, device="cuda")
   d = torch_mod.zeros((30, 30), dtype=torch_mod.int32, device="cuda")
   p = lambda x: x.data_ptr()  # noqa: E731
-  assert lib.tspb_or_opt(p(t), 1, 30, p(d), 30, None, p(c), p(c), 4, 3, 10, 200, p(st), None, None) == native.TSPB_ERR_ARG
-  assert lib.tspb_or_opt(p(t), 1, 30, p(d), 30, None, p(c), p(c), 30, 3, 10, 256, p(st), None, None) == native.TSPB_ERR_ARG
-  assert lib.tspb_or_opt(p(t), 1, 30, None, 0, None, p(c), p(c), 4, 3, 10, 256, p(st), None, None) == native.TSPB_ERR_ARG
-  assert lib.tspb_or_opt(p(t), 1, 2, p(d), 30, None, p(c), p(c), 1, 3, 10, 256, p(st), None, None) == native.TSPB_OK
+  assert lib.tspb_or_opt(p(t), 1, 30, p(d), 30, None, p(c), p(c), None, 4, 3, 10, 200, p(st), None, None) == native.TSPB_ERR_ARG
+  assert lib.tspb_or_opt(p(t), 1, 30, p(d), 30, None, p(c), p(c), None, 30, 3, 10, 256, p(st), None, None) == native.TSPB_ERR_ARG
+  assert lib.tspb_or_opt(p(t), 1, 30, None, 0, None, p(c), p(c), None, 4, 3, 10, 256, p(st), None, None) == native.TSPB_ERR_ARG
+  assert lib.tspb_or_opt(p(t), 1, 2, p(d), 30, None, p(c), p(c), None, 1, 3, 10, 256, p(st), None, None) == native.TSPB_OK
   assert lib.tspb_or_opt_max_n() > 10000
 
 
@@ -178,3 +178,35 @@ def test_or_opt_drops_into_the_ga_pipeline(torch_mod):
     runs.append((np.asarray(best), list(stats["convergence_history"])))
   assert np.array_equal(runs[0][0], runs[1][0])
   assert runs[0][1] == runs[1][1]
+
+
+def test_or_opt_packed_and_plain_tables_agree(torch_mod):
+  """k % 4 == 0: the packed words (four per 16-byte load) and the plain id / distance
+  tables give the same tours and counts, both equal to the oracle."""
+  from tsp_gpu_clean_b200 import native
+  from tsp_gpu_clean_b200.device import candidate_list, operands_for, ptr, stream_handle
+
+  coords = instances.clustered_instance(300, 6, 25.0, 4)
+  ctx = _ctx(coords)
+  ops = operands_for(ctx)
+  dist, stride, _ = ops.distance_args(300)
+  tabs = ops.candidates(12, candidate_list(ctx, 12), 300)
+  assert tabs.packed is not None and tabs.k == 12
+  tours = _tours(np.random.default_rng(8), 300, 6)
+  lib = native.load_library()
+  outs = []
+  for packed in (tabs.packed, None):
+    t = torch_mod.from_numpy(tours.copy()).cuda()
+    st = torch_mod.zeros(6, dtype=torch_mod.int32, device="cuda")
+    stats = torch_mod.zeros((6, 3), dtype=torch_mod.int64, device="cuda")
+    native.check("tspb_or_opt", lib.tspb_or_opt(ptr(t), 6, 300, ptr(dist), stride, None, ptr(tabs.cand),
+                                                ptr(tabs.cand_dist), ptr(packed), 12, 3, 1000, 128, ptr(st), ptr(stats),
+                                                stream_handle()))
+    assert int(st.max().item()) == 0
+    outs.append((t.cpu().numpy(), stats.cpu().numpy()))
+  assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+  D = odist.euc2d_matrix(coords)
+  cand = candidate_list(ctx, 12)
+  for r in range(6):
+    want, passes, moves, evaluated = oo.refine(tours[r], D, cand, 1000, 3)
+    assert np.array_equal(outs[0][0][r], want) and outs[0][1][r].tolist() == [passes, moves, evaluated]

@@ -14,9 +14,10 @@
 //
 // Layout: tour[p], pos[a], eout[a] = d(a, succ a) and a rebuild buffer in shared memory
 // (16 n bytes). A thread evaluates four consecutive candidates of one (i, L, o): the
-// candidate ids and d(x, c) come from the k-NN table and its distance table, pos, the
-// successor and eout from shared memory, and d(y, e) is the only gather per entry. The move
-// rewrites only the positions between the segment and the insertion point.
+// candidate ids and d(x, c) come from the k-NN table and its distance table (PACKED: one
+// 16-byte load of four c | d << 16 words), pos, the successor and eout from shared memory,
+// and d(y, e) is the only gather per entry. The move rewrites only the positions between the
+// segment and the insertion point.
 #include "common.cuh"
 #include "two_opt.cuh"
 
@@ -60,10 +61,11 @@ __device__ __forceinline__ OrMove block_min_or(OrMove m, OrMove* sh) {
   return r;
 }
 
-template <int THREADS>
+template <int THREADS, bool PACKED>
 __global__ void __launch_bounds__(THREADS) or_opt_kernel(int32_t* __restrict__ tours, int num, int n, DistSrc ds,
                                                          const int32_t* __restrict__ cand,
-                                                         const int32_t* __restrict__ cdist, int k, int S,
+                                                         const int32_t* __restrict__ cdist,
+                                                         const uint32_t* __restrict__ packed, int k, int S,
                                                          long long max_iter, int32_t* __restrict__ status,
                                                          long long* __restrict__ stats) {
   extern __shared__ __align__(16) int sm[];
@@ -126,13 +128,24 @@ __global__ void __launch_bounds__(THREADS) or_opt_kernel(int32_t* __restrict__ t
         const int r0 = ch * 4;
         int c[4], dxc[4], e[4], dye[4];
         bool ok[4];
+        if constexpr (PACKED) {  // k % 4 == 0: the four entries exist and are 16-byte aligned
+          const uint4 w = __ldg(reinterpret_cast<const uint4*>(packed + (long long)x * k + r0));
+          const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          ok[u] = r0 + u < k;
-          if (ok[u]) {
-            const long long at = (long long)x * k + r0 + u;
-            c[u] = __ldg(cand + at);
-            dxc[u] = __ldg(cdist + at);
+          for (int u = 0; u < 4; ++u) {
+            ok[u] = true;
+            c[u] = (int)(ws[u] & 0xffffu);
+            dxc[u] = (int)(ws[u] >> 16);
+          }
+        } else {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            ok[u] = r0 + u < k;
+            if (ok[u]) {
+              const long long at = (long long)x * k + r0 + u;
+              c[u] = __ldg(cand + at);
+              dxc[u] = __ldg(cdist + at);
+            }
           }
         }
 #pragma unroll
@@ -230,9 +243,9 @@ __global__ void __launch_bounds__(THREADS) or_opt_kernel(int32_t* __restrict__ t
 
 template <int THREADS>
 static int launch_or_opt(int32_t* tours, int num, int n, const DistSrc& ds, const int32_t* cand,
-                         const int32_t* cdist, int k, int S, long long max_iter, int32_t* status, long long* stats,
-                         size_t smem, cudaStream_t st) {
-  auto kern = or_opt_kernel<THREADS>;
+                         const int32_t* cdist, const uint32_t* packed, int k, int S, long long max_iter,
+                         int32_t* status, long long* stats, size_t smem, cudaStream_t st) {
+  auto kern = packed ? or_opt_kernel<THREADS, true> : or_opt_kernel<THREADS, false>;
   if (smem > 48 * 1024) TSPB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0, dev = 0, sms = 0;
   TSPB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem));
@@ -240,7 +253,7 @@ static int launch_or_opt(int32_t* tours, int num, int n, const DistSrc& ds, cons
   TSPB_CUDA_CHECK(cudaGetDevice(&dev));
   TSPB_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const long long grid = (long long)per_sm * sms < num ? (long long)per_sm * sms : num;
-  kern<<<(int)grid, THREADS, smem, st>>>(tours, num, n, ds, cand, cdist, k, S, max_iter, status, stats);
+  kern<<<(int)grid, THREADS, smem, st>>>(tours, num, n, ds, cand, cdist, packed, k, S, max_iter, status, stats);
   return tspb_launch_status();
 }
 
@@ -254,9 +267,9 @@ extern "C" int tspb_or_opt_max_n(void) {
 }
 
 extern "C" int tspb_or_opt(int32_t* tours, int32_t num_tours, int32_t n, const int32_t* dist, int64_t dist_stride,
-                           const double* coords, const int32_t* cand, const int32_t* cand_dist, int32_t k,
-                           int32_t max_segment, int64_t max_iterations, int32_t threads, int32_t* status,
-                           int64_t* stats, void* stream) {
+                           const double* coords, const int32_t* cand, const int32_t* cand_dist,
+                           const uint32_t* cand_packed, int32_t k, int32_t max_segment, int64_t max_iterations,
+                           int32_t threads, int32_t* status, int64_t* stats, void* stream) {
   if (num_tours < 0 || n < 0 || max_iterations < 0 || max_segment < 1 || max_segment > 8) return TSPB_ERR_ARG;
   if (threads != 128 && threads != 256 && threads != 512) return TSPB_ERR_ARG;
   if (num_tours == 0 || n < 3) return TSPB_OK;
@@ -272,9 +285,18 @@ extern "C" int tspb_or_opt(int32_t* tours, int32_t num_tours, int32_t n, const i
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   const size_t smem = (size_t)16 * n;
   long long* s = reinterpret_cast<long long*>(stats);
+  // the packed words serve only whole, aligned groups of four
+  const uint32_t* pk =
+      cand_packed && k % 4 == 0 && reinterpret_cast<uintptr_t>(cand_packed) % 16 == 0 ? cand_packed : nullptr;
   switch (threads) {
-    case 128: return launch_or_opt<128>(tours, num_tours, n, ds, cand, cand_dist, k, max_segment, max_iterations, status, s, smem, st);
-    case 512: return launch_or_opt<512>(tours, num_tours, n, ds, cand, cand_dist, k, max_segment, max_iterations, status, s, smem, st);
-    default: return launch_or_opt<256>(tours, num_tours, n, ds, cand, cand_dist, k, max_segment, max_iterations, status, s, smem, st);
+    case 128:
+      return launch_or_opt<128>(tours, num_tours, n, ds, cand, cand_dist, pk, k, max_segment, max_iterations, status, s,
+                                smem, st);
+    case 512:
+      return launch_or_opt<512>(tours, num_tours, n, ds, cand, cand_dist, pk, k, max_segment, max_iterations, status, s,
+                                smem, st);
+    default:
+      return launch_or_opt<256>(tours, num_tours, n, ds, cand, cand_dist, pk, k, max_segment, max_iterations, status, s,
+                                smem, st);
   }
 }

@@ -77,7 +77,7 @@ SIGNATURES: dict[str, tuple] = {
   "tspb_distance_matrix": (ctypes.c_int, [_p, _i32, _i32, _i32, _p, _i64, _p]),
   "tspb_three_opt": (ctypes.c_int, [_p, _i32, _i32, _p, _i64, _p, _i64, _i32, _p, _sz, _p, _p, _p]),
   "tspb_three_opt_workspace_bytes": (ctypes.c_int, [_i32, _i32, ctypes.POINTER(ctypes.c_size_t)]),
-  "tspb_or_opt": (ctypes.c_int, [_p, _i32, _i32, _p, _i64, _p, _p, _p, _i32, _i32, _i64, _i32, _p, _p, _p]),
+  "tspb_or_opt": (ctypes.c_int, [_p, _i32, _i32, _p, _i64, _p, _p, _p, _p, _i32, _i32, _i64, _i32, _p, _p, _p]),
   "tspb_or_opt_max_n": (ctypes.c_int, []),
   "tspb_random_init_jobs": (ctypes.c_int, [_p, _i32, _i32, _i32, _p]),
   "tspb_tape_draw_host": (ctypes.c_int, [_p, _i32, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _p]),

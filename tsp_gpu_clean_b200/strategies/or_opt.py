@@ -92,8 +92,8 @@ class LocalSearchB200OrOpt(StrategyBase):
     stats = torch.empty((num, 3), dtype=torch.int64, device="cuda")
     status = torch.empty(num, dtype=torch.int32, device="cuda")
     native.call("tspb_or_opt", ptr(d_tours), num, n, ptr(dist), stride, ptr(coords), ptr(tabs.cand),
-                ptr(tabs.cand_dist), int(tabs.k), int(self.max_segment), int(self.max_iterations), threads,
-                ptr(status), ptr(stats), stream_handle())
+                ptr(tabs.cand_dist), ptr(tabs.packed), int(tabs.k), int(self.max_segment), int(self.max_iterations),
+                threads, ptr(status), ptr(stats), stream_handle())
     self.kernel_launches += 1
     code = int(status.max().item())
     if code == native.TSPB_ERR_NOT_PERMUTATION:
