@@ -920,9 +920,10 @@ def main(argv=None) -> int:
                   help="two_opt: read the int32 matrix, or rebuild each distance from FP64 coordinates")
   ap.add_argument("--first-restart", default="incremental", choices=["incremental", "full"],
                   help="first mode: restart each pass from the affected entries and row bi, or rescan from entry 0")
-  ap.add_argument("--batch-incremental", default="auto", choices=["auto", "on", "off"],
+  ap.add_argument("--batch-incremental", default="off", choices=["auto", "on", "off"],
                   help="GA/uneven: 2-opt with the reverse k-NN index (best: only the rows a move can change are "
-                       "recomputed; first: incremental restart); auto lets the tuner measure both")
+                       "recomputed; first: incremental restart); auto lets the tuner measure both; off (the "
+                       "solver's default) uses the plain kernel")
   ap.add_argument("--cpu-workers", type=int, default=0, help="0: all host cores, capped at 64")
   ap.add_argument("--no-cpu-baseline", action="store_true")
   ap.add_argument("--workload", default="two_opt", choices=["two_opt", "learned", "uneven", "or_opt", *GA_WORKLOADS])

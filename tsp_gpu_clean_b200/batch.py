@@ -139,7 +139,7 @@ class FusedBatchSolver:
                tuner: BatchAutotuner | None = None, bucket_bounds: Sequence[int] = DEFAULT_BUCKET_BOUNDS,
                chunk: int = 16, skip_converged: bool = True, concurrent_buckets: bool = True,
                crossover: str = "pmx", mutation: str = "inversion", init: str = "nn",
-               local_search_stage: str = "none", incremental: str = "auto") -> None:
+               local_search_stage: str = "none", incremental: str = "off") -> None:
     if population_size < 2:
       raise ValueError("population_size must be >= 2")
     if init not in ("nn", "random"):
@@ -148,7 +148,9 @@ class FusedBatchSolver:
       raise ValueError("local_search_stage must be 'none' or 'post_mutation'")
     self.init, self.stage = init, local_search_stage
     # 2-opt with the reverse k-NN index: best mode recomputes only the rows a move can
-    # change, first mode restarts from the move's row; "auto" lets the tuner measure both
+    # change, first mode restarts from the move's row; "auto" lets the tuner measure both.
+    # Off by default: it lost on every workload measured (C3, Chapter 4), and trying it
+    # doubles the tuner's 2-opt probes.
     if incremental not in ("auto", "on", "off"):
       raise ValueError("incremental must be 'auto', 'on' or 'off'")
     self.incremental = incremental
