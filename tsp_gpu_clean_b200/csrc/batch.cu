@@ -159,6 +159,74 @@ __global__ void batch_survival_rank_kernel(const tspb_batch B, int n2) {
   for (int r = threadIdx.x; r < P; r += blockDim.x) B.order[(long long)i * P + r] = idx[r];
 }
 
+// The same order with n2 / 2 threads (64 <= n2 <= 2048): thread t holds positions t and
+// t + n2/2 in registers. A compare-exchange at distance j pairs positions e and e ^ j: for
+// j < 32 the partner sits in the same warp (lane ^ j, same slot), for j = n2/2 it is the
+// thread's other slot, otherwise the pair meets in shared memory. Each position keeps the
+// smaller (fitness, index) when it is the lower one of an ascending pair ((e & k) == 0) or
+// the higher one of a descending pair, as in the shared-memory sort above.
+__device__ __forceinline__ bool rank_after(double ka, int ia, double kb, int ib) {
+  return ka > kb || (ka == kb && ia > ib);
+}
+
+__device__ __forceinline__ void rank_keep(double& k, int& id, double pk, int pid, int e, int p, int kk) {
+  const bool asc = (e & kk) == 0;
+  const bool want_small = (e < p) == asc;
+  if (rank_after(k, id, pk, pid) == want_small) {  // the partner is the one this position keeps
+    k = pk;
+    id = pid;
+  }
+}
+
+__global__ void batch_survival_rank_reg_kernel(const tspb_batch B, int n2) {
+  extern __shared__ __align__(16) unsigned char rank_sm[];
+  double* skey = reinterpret_cast<double*>(rank_sm);
+  int* sidx = reinterpret_cast<int*>(skey + n2);
+  const int i = blockIdx.x, P = B.P;
+  const int* c = B.ctl + 4 * i;
+  if (c[1] != TSPB_BATCH_RUN) return;  // uniform per CTA
+  const int parity = c[0] & 1;
+  const double* fa = fit_buf(B, parity) + (long long)i * P;
+  const double* fb = B.off_fit + (long long)i * P;
+  const int half = n2 >> 1, t = threadIdx.x, count = 2 * P;
+  const double inf = __longlong_as_double(0x7ff0000000000000LL);
+  auto load = [&](int e) { return e < P ? fa[e] : (e < count ? fb[e - P] : inf); };
+  const int e0 = t, e1 = t + half;
+  double k0 = load(e0), k1 = load(e1);
+  int i0 = e0, i1 = e1;
+  for (int kk = 2; kk <= n2; kk <<= 1) {
+    for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+      if (jj == half) {  // e1 = e0 ^ half: both in this thread (kk == n2, ascending)
+        if (rank_after(k0, i0, k1, i1)) {
+          const double tk = k0;
+          const int ti = i0;
+          k0 = k1;
+          i0 = i1;
+          k1 = tk;
+          i1 = ti;
+        }
+      } else if (jj < 32) {
+        const double p0 = __shfl_xor_sync(FULL, k0, jj), p1 = __shfl_xor_sync(FULL, k1, jj);
+        const int q0 = __shfl_xor_sync(FULL, i0, jj), q1 = __shfl_xor_sync(FULL, i1, jj);
+        rank_keep(k0, i0, p0, q0, e0, e0 ^ jj, kk);
+        rank_keep(k1, i1, p1, q1, e1, e1 ^ jj, kk);
+      } else {
+        skey[e0] = k0;
+        sidx[e0] = i0;
+        skey[e1] = k1;
+        sidx[e1] = i1;
+        __syncthreads();
+        const double p0 = skey[e0 ^ jj], p1 = skey[e1 ^ jj];
+        const int q0 = sidx[e0 ^ jj], q1 = sidx[e1 ^ jj];
+        __syncthreads();  // every partner read before the next stage writes
+        rank_keep(k0, i0, p0, q0, e0, e0 ^ jj, kk);
+        rank_keep(k1, i1, p1, q1, e1, e1 ^ jj, kk);
+      }
+    }
+  }
+  if (e0 < P) B.order[(long long)i * P + e0] = i0;  // half >= P: slot 1 is never a survivor
+}
+
 // CTA per (instance, survivor): new_pop[r] = combined[order[r]] with its fitness and
 // converged bit; the elite-edge tie flag.
 __global__ void __launch_bounds__(128) batch_survival_gather_kernel(const tspb_batch B) {
@@ -516,12 +584,16 @@ extern "C" int tspb_batch_survival(const tspb_batch* b, void* stream) {
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   int n2 = 1;
   while (n2 < 2 * b->P) n2 <<= 1;
-  const int rank_threads = n2 >= 1024 ? 512 : (n2 / 2 > 32 ? n2 / 2 : 32);
   const size_t rank_smem = (size_t)12 * n2;
-  if (rank_smem > 48 * 1024)
-    TSPB_CUDA_CHECK(cudaFuncSetAttribute(batch_survival_rank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)rank_smem));
-  batch_survival_rank_kernel<<<b->num_instances, rank_threads, rank_smem, st>>>(*b, n2);
+  if (n2 >= 64 && n2 <= 2048) {  // n2 / 2 threads, pairs in registers
+    batch_survival_rank_reg_kernel<<<b->num_instances, n2 / 2, rank_smem, st>>>(*b, n2);
+  } else {
+    const int rank_threads = n2 >= 1024 ? 512 : (n2 / 2 > 32 ? n2 / 2 : 32);
+    if (rank_smem > 48 * 1024)
+      TSPB_CUDA_CHECK(cudaFuncSetAttribute(batch_survival_rank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)rank_smem));
+    batch_survival_rank_kernel<<<b->num_instances, rank_threads, rank_smem, st>>>(*b, n2);
+  }
   batch_survival_gather_kernel<<<b->num_instances * b->P, 128, 0, st>>>(*b);
   batch_pause_kernel<<<(b->num_instances * 32 + 127) / 128, 128, 0, st>>>(*b);
   return tspb_launch_status();
