@@ -26,3 +26,27 @@ def test_operand_cache_does_not_keep_contexts_alive():
   gc.collect()
   assert ref() is None
   assert len(device._operands) == before - 1
+
+
+def test_pack_overflow_flags_are_read_lazily_and_in_one_batch():
+  """CandidateTables keeps the packing kernel's overflow flag until the packed table is
+  first used; check_packed reads many flags at once. (CPU tensors stand in for device ones.)"""
+  import torch
+
+  from tsp_gpu_clean_b200.device import CandidateTables, check_packed
+
+  def tables(flag):
+    z = torch.zeros((3, 2), dtype=torch.int32)
+    return CandidateTables(z, z, torch.zeros(4, dtype=torch.int32), torch.zeros(6, dtype=torch.int32),
+                           packed=z.clone(), overflow=torch.tensor([flag], dtype=torch.int32))
+
+  ok, bad = tables(0), tables(1)
+  assert ok.packed_words is not None and bad.packed_words is not None  # unchecked views
+  check_packed([ok, bad])
+  assert ok.packed is not None and bad.packed is None
+  assert ok._overflow is None and bad._overflow is None  # read once
+  lazy = tables(1)
+  assert lazy.packed is None  # first use reads the flag
+  none = CandidateTables(torch.zeros((3, 2)), None, None, None)
+  check_packed([none])
+  assert none.packed is None
