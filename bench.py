@@ -81,8 +81,8 @@ def _cpu_worker(args):
 
 def cpu_sample(pool, workers: int, seed_offset: int = 0) -> dict:
   """Oracle deltas/s on `workers` tours in parallel (one tour per process)."""
-  coords, _ = instances.c2_workload(tours=1)
-  tours = instances.random_tours(instances.C2_N, workers, 777 + seed_offset)
+  coords, _ = instances.two_opt_workload(tours=1)
+  tours = instances.random_tours(instances.TWO_OPT_N, workers, 777 + seed_offset)
   t0 = time.perf_counter()
   res = pool.map(_cpu_worker, [(coords, tours[i]) for i in range(workers)])
   wall = time.perf_counter() - t0
@@ -216,9 +216,9 @@ def run_gpu(args, pool) -> dict | None:
   build_library()
   lib = native.load_library()
 
-  coords, _ = instances.c2_workload(tours=1)
-  tours_np = instances.random_tours(instances.C2_N, args.tours, instances.C2_TOUR_SEED + 1000 * rank)
-  n = instances.C2_N
+  coords, _ = instances.two_opt_workload(tours=1)
+  tours_np = instances.random_tours(instances.TWO_OPT_N, args.tours, instances.TWO_OPT_TOUR_SEED + 1000 * rank)
+  n = instances.TWO_OPT_N
   ctx = ProblemContext(Problem.from_coordinates(coords, "c2"), seed=0)
   ops = operands_for(ctx)
   dist_t, stride, _ = ops.distance_args(n)
@@ -329,7 +329,7 @@ def run_gpu(args, pool) -> dict | None:
                  "frac": achieved_gbs / peaks["hbm_gbs"],
                  "traffic": (NCU_DRAM_BYTES_PER_LAUNCH[dominant]
                              if (args.tours, args.threads, args.kernel, args.max_iter)
-                             == (instances.C2_TOURS, 128, "scan", 10**9) else None),
+                             == (instances.TWO_OPT_TOURS, 128, "scan", 10**9) else None),
                  "kernel": f"two_opt_{args.kernel}_kernel<{dominant}>",
                  "peak_source": peaks["source"],
                  "basis": f"{BYTES_PER_DELTA} B per gain the kernel computed"},
@@ -793,8 +793,9 @@ def _or_opt_cpu_sample(coords, cand, tours_np) -> dict:
 
 
 def main_or_opt(args) -> int:
-  """Candidate Or-opt on the C2 instance: 1024 random tours, k=20, segments of up to 3
-  cities, 50 best-improvement passes per tour; metric = valid entries evaluated per second."""
+  """Candidate Or-opt on the 1000-city 20-cluster instance: 1024 random tours, k=20,
+  segments of up to 3 cities, 50 best-improvement passes per tour; metric = valid entries
+  evaluated per second."""
   import torch
 
   from tsp_gpu_clean_b200 import native
@@ -804,9 +805,9 @@ def main_or_opt(args) -> int:
   from tsp_gpu_clean_b200.strategies.or_opt import LocalSearchB200OrOpt
 
   world, rank, _ = _dist_env()
-  n = instances.C2_N
-  coords, _ = instances.c2_workload(tours=1)
-  tours_np = instances.random_tours(n, args.tours, instances.C2_TOUR_SEED + 1000 * rank)
+  n = instances.TWO_OPT_N
+  coords, _ = instances.two_opt_workload(tours=1)
+  tours_np = instances.random_tours(n, args.tours, instances.TWO_OPT_TOUR_SEED + 1000 * rank)
   ctx = ProblemContext(Problem.from_coordinates(coords, "c2"), seed=0)
   cand_np = ctx.get_cpu_candidate_list(K_CAND)
   config = {"workload": f"Or-opt (best improvement, candidate_k={K_CAND}, segments <= {OR_OPT_SEGMENT}, "
@@ -910,7 +911,7 @@ def main(argv=None) -> int:
   ap.add_argument("--steps", type=int, default=3)
   ap.add_argument("--warmup", type=int, default=3)
   ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-  ap.add_argument("--tours", type=int, default=instances.C2_TOURS)
+  ap.add_argument("--tours", type=int, default=instances.TWO_OPT_TOURS)
   ap.add_argument("--max-iter", type=int, default=10**9,
                   help="2-opt: passes per tour (default: to a local optimum; fewer only for short profiling runs)")
   ap.add_argument("--mode", default="both", choices=["both", "best", "first"])
@@ -962,7 +963,7 @@ def main(argv=None) -> int:
   workers = args.cpu_workers or min(os.cpu_count() or 1, 64)
   config = {"workload": "2-opt to local optimum (best and first modes, candidate_k=20) on random tours of a "
                         "1000-city 20-cluster EUC_2D instance",
-            "tours": args.tours, "n": instances.C2_N, "k": K_CAND, "modes": list(MODES if args.mode == "both" else (args.mode,)),
+            "tours": args.tours, "n": instances.TWO_OPT_N, "k": K_CAND, "modes": list(MODES if args.mode == "both" else (args.mode,)),
             "l2": "flushed between timed steps (256 MiB write); the 4 MB matrix is L2-resident within a step",
             "threads_per_cta": args.threads, "kernel": args.kernel, "distances": args.distances,
             "first_restart": args.first_restart}

@@ -165,7 +165,7 @@ def main(ref_root: str) -> None:
   np.savez_compressed(os.path.join(HERE, "two_opt_small.npz"), **out)
   print(f"two_opt_small: {case} cases in {time.time() - t0:.1f}s")
 
-  # ------------------------------------------------------------------ 2-opt C2 subset
+  # ------------------------------------------------ 2-opt subset of the 1024-tour, 1000-city workload
   t0 = time.time()
   counts = {"pairs": 0, "passes": 0}
   orig_blocks = LocalSearchCPUTourTwoOpt._pair_blocks
@@ -177,7 +177,7 @@ def main(ref_root: str) -> None:
       yield i_idx, j_idx
 
   LocalSearchCPUTourTwoOpt._pair_blocks = counting_blocks
-  coords, tours = instances.c2_workload(tours=4)
+  coords, tours = instances.two_opt_workload(tours=4)
   prob = coord_problem(coords, "c2")
   c2: dict[str, np.ndarray] = {"coords": coords, "tours_in": tours}
   for mode in ("best", "first"):

@@ -70,6 +70,6 @@ def test_weak_scaling_shards_differ_per_rank():
   a = instances.uneven_batch(8, bench.UNEVEN_SEED)
   b = instances.uneven_batch(8, bench.UNEVEN_SEED + 7919)
   assert [len(x) for x in a] != [len(x) for x in b] or any(not np.array_equal(x, y) for x, y in zip(a, b))
-  t0 = instances.random_tours(50, 4, instances.C2_TOUR_SEED)
-  t1 = instances.random_tours(50, 4, instances.C2_TOUR_SEED + 1000)
+  t0 = instances.random_tours(50, 4, instances.TWO_OPT_TOUR_SEED)
+  t1 = instances.random_tours(50, 4, instances.TWO_OPT_TOUR_SEED + 1000)
   assert not np.array_equal(t0, t1)

@@ -52,7 +52,7 @@ def test_two_opt_c2_subset_matches_reference_with_counts(golden, mode):
 
 def test_c2_workload_generator_is_stable(golden):
   data = golden("two_opt_c2.npz")
-  coords, tours = instances.c2_workload(tours=4)
+  coords, tours = instances.two_opt_workload(tours=4)
   assert np.array_equal(coords, data["coords"])
   assert np.array_equal(tours, data["tours_in"])
 

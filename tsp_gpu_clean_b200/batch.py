@@ -149,8 +149,9 @@ class FusedBatchSolver:
     self.init, self.stage = init, local_search_stage
     # 2-opt with the reverse k-NN index: best mode recomputes only the rows a move can
     # change, first mode restarts from the move's row; "auto" lets the tuner measure both.
-    # Off by default: it lost on every workload measured (C3, Chapter 4), and trying it
-    # doubles the tuner's 2-opt probes.
+    # Off by default: it lost on every workload measured (a 2000-city GA refining 64
+    # elites, a 1002-city GA refining every child), and trying it doubles the tuner's
+    # 2-opt probes.
     if incremental not in ("auto", "on", "off"):
       raise ValueError("incremental must be 'auto', 'on' or 'off'")
     self.incremental = incremental

@@ -53,12 +53,12 @@ def uneven_batch(count: int, seed: int, n_min: int = 50, n_max: int = 5000) -> l
 
 
 #: The 2-opt batch workload: 1024 random tours of a 1000-city, 20-cluster instance.
-C2_N = 1000
-C2_TOURS = 1024
-C2_INSTANCE_SEED = 20260
-C2_TOUR_SEED = 20261
+TWO_OPT_N = 1000
+TWO_OPT_TOURS = 1024
+TWO_OPT_INSTANCE_SEED = 20260
+TWO_OPT_TOUR_SEED = 20261
 
 
-def c2_workload(tours: int = C2_TOURS) -> tuple[np.ndarray, np.ndarray]:
-  coords = clustered_instance(C2_N, 20, 30.0, C2_INSTANCE_SEED)
-  return coords, random_tours(C2_N, tours, C2_TOUR_SEED)
+def two_opt_workload(tours: int = TWO_OPT_TOURS) -> tuple[np.ndarray, np.ndarray]:
+  coords = clustered_instance(TWO_OPT_N, 20, 30.0, TWO_OPT_INSTANCE_SEED)
+  return coords, random_tours(TWO_OPT_N, tours, TWO_OPT_TOUR_SEED)
