@@ -8,8 +8,10 @@ segment of one to three consecutive cities elsewhere in the tour, optionally rev
 with the same k-NN candidate and fixed-start conventions as the reference's candidate
 2-opt (`src/algorithms/strategies/local_search/two_opt.py:347-367`). Two independent
 restatements are kept: `best_move` (NumPy arrays over a pass) and `best_move_loops`
-(plain loops); the tests pin each against the other and the applied delta against the
-tour-length change.
+(plain loops); the tests pin each against the other, the applied delta against the
+tour-length change, and the neighbourhood against the 3-opt oracle (pinned to the
+reference's CPU 3-opt): every Or-opt move is a 3-opt reconnection, so 3-opt local optima
+admit no improving Or-opt move.
 
 Definition, for an open cyclic tour `t` (a permutation of 0..n-1 whose position 0 never
 moves), a k-NN table `N` of shape (n, k) and symmetric distances `D`:

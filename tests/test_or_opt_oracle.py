@@ -83,3 +83,24 @@ def test_refine_is_monotone_and_counts_passes():
   part, p5, m5, _ = oo.refine(t, D, cand, 5)
   assert (p5, m5) == (5, 5)
   assert np.array_equal(oo.refine(part, D, cand, 10**6)[0], out)  # passes compose
+
+
+def test_three_opt_local_optima_admit_no_improving_or_opt_move():
+  """Every Or-opt move removes three edges and reconnects them without a reversal or with
+  the segment reversed, i.e. it is one of the seven 3-opt reconnections. A tour refined to a
+  local optimum by the 3-opt oracle (pinned to the reference's CPU 3-opt) therefore admits
+  no improving Or-opt move, even with full candidate lists."""
+  from oracle import three_opt as o3
+
+  rng = np.random.default_rng(21)
+  for n in (8, 13, 21, 28):
+    coords = rng.uniform(0, 500, (n, 2))
+    D = odist.euc2d_matrix(coords)
+    full = odist.candidate_list(n - 1, coords=coords)
+    t = _tour(rng, n)
+    opt, _ = o3.refine(t, D, 10**6)
+    assert o3.best_move(opt, D)[0] == 0  # a 3-opt local optimum
+    for S in (1, 2, 3):
+      assert oo.best_move(opt, D, full, S)[0][1] == -1, (n, S)
+    # while a random tour does have improving Or-opt moves
+    assert oo.best_move(t, D, full, 3)[0][1] >= 0
