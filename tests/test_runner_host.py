@@ -34,6 +34,10 @@ def test_config_instantiates_every_variant():
   assert isinstance(fused, runner.FusedGeneticAlgorithm)
   assert (fused.population_size, fused.mutation_rate, fused.seed, fused.two_opt_iterations) == (256, 0.02, 7, 3)
   assert (fused.crossover, fused.mutation, fused.initialization) == ("ox", "swap", "random")
+  or_opt = runner.instantiate(algos["B200ModularOrOpt"], defaults)
+  from tsp_gpu_clean_b200.strategies import LocalSearchB200OrOpt
+
+  assert isinstance(or_opt.local_search, LocalSearchB200OrOpt) and or_opt.local_search.max_segment == 3
   memetic = runner.instantiate(algos["B200MemeticFused"], defaults)
   assert (memetic.population_size, memetic.elite_count, memetic.post_init, memetic.crossover) == (128, 16, True, "pmx")
 
@@ -112,5 +116,6 @@ def test_reference_config_models_instantiate_the_b200_config():
   assert lines["B200Modular"] == ["GeneticAlgorithm", "256", "InitializationB200PermRandom", "SelectionB200Tournament",
                                   "CrossoverB200PermOrder", "MutationB200PermSwap", "LocalSearchB200TourTwoOpt",
                                   "EvaluationB200Cost"]
+  assert lines["B200ModularOrOpt"][6] == "LocalSearchB200OrOpt"
   assert lines["B200Fused"][:2] == ["FusedGeneticAlgorithm", "256"]
   assert lines["B200MemeticFused"][:2] == ["FusedGeneticAlgorithm", "128"]
