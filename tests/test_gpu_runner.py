@@ -119,3 +119,19 @@ def test_early_stops_match_the_strategy_pipeline(algos, golden, kind):
     stop = next(t for t in range(1, len(hist)) if hist[t] <= optimal + 1e-6
                 or (hist[t] - optimal) / optimal * 100.0 < 1.0)
     assert out[1][1] == stop and out[1][4] == hist[: stop + 1].tolist()
+
+
+def test_or_opt_variant_runs_through_the_runner(algos, golden):
+  """B200ModularOrOpt: the modular pipeline with Or-opt as its local search runs seeded
+  repetitions end to end; every best tour is a permutation and histories never rise."""
+  from tsp_gpu_clean_b200 import runner
+
+  g = golden("stage.npz")
+  problem = _problem(g)
+  algo = _make(algos, "B200ModularOrOpt", population_size=32)
+  r = runner.run_repetitions(algo, problem, 8, 2, seed_base=42, patience=10**9)
+  n = len(g["ga_s1_coords"])
+  for tour, final, initial in zip(r["best_tours"], r["final_costs"], r["initial_costs"]):
+    assert sorted(tour) == list(range(n))
+    assert final <= initial
+  assert r["generations"] == [8, 8]
