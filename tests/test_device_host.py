@@ -50,3 +50,34 @@ def test_pack_overflow_flags_are_read_lazily_and_in_one_batch():
   none = CandidateTables(torch.zeros((3, 2)), None, None, None)
   check_packed([none])
   assert none.packed is None
+
+
+def test_check_free_logic_against_fake_allocator_counters(monkeypatch):
+  """check_free on the CPU with fakes of the two torch calls it makes: cached memory covers
+  a request without asking the driver; otherwise free + cached decides; an uninitialised
+  allocator counts as nothing cached."""
+  import pytest
+  import torch
+
+  from tsp_gpu_clean_b200 import device
+  from tsp_gpu_clean_b200.errors import VRAMInsufficientError
+
+  state = {"stats": {"reserved_bytes": {"all": {"current": 100}}, "allocated_bytes": {"all": {"current": 40}}},
+           "free": 1000, "driver_calls": 0}
+
+  def fake_mem_get_info(*a):
+    state["driver_calls"] += 1
+    return state["free"], 10**6
+
+  monkeypatch.setattr(torch.cuda, "memory_stats_as_nested_dict", lambda *a: state["stats"])
+  monkeypatch.setattr(torch.cuda, "mem_get_info", fake_mem_get_info)
+  device.check_free(60, "fits the cache")
+  assert state["driver_calls"] == 0
+  device.check_free(1000 + 60, "fits free + cached")
+  assert state["driver_calls"] == 1
+  with pytest.raises(VRAMInsufficientError):
+    device.check_free(1000 + 61, "one byte too many")
+  state["stats"] = {}
+  device.check_free(1000, "no allocator yet")
+  with pytest.raises(VRAMInsufficientError):
+    device.check_free(1001, "no allocator yet, too large")
