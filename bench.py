@@ -219,7 +219,7 @@ def run_gpu(args, pool) -> dict | None:
   coords, _ = instances.two_opt_workload(tours=1)
   tours_np = instances.random_tours(instances.TWO_OPT_N, args.tours, instances.TWO_OPT_TOUR_SEED + 1000 * rank)
   n = instances.TWO_OPT_N
-  ctx = ProblemContext(Problem.from_coordinates(coords, "c2"), seed=0)
+  ctx = ProblemContext(Problem.from_coordinates(coords, "clustered1000"), seed=0)
   ops = operands_for(ctx)
   dist_t, stride, _ = ops.distance_args(n)
   coords_t = None
@@ -808,7 +808,7 @@ def main_or_opt(args) -> int:
   n = instances.TWO_OPT_N
   coords, _ = instances.two_opt_workload(tours=1)
   tours_np = instances.random_tours(n, args.tours, instances.TWO_OPT_TOUR_SEED + 1000 * rank)
-  ctx = ProblemContext(Problem.from_coordinates(coords, "c2"), seed=0)
+  ctx = ProblemContext(Problem.from_coordinates(coords, "clustered1000"), seed=0)
   cand_np = ctx.get_cpu_candidate_list(K_CAND)
   config = {"workload": f"Or-opt (best improvement, candidate_k={K_CAND}, segments <= {OR_OPT_SEGMENT}, "
                         f"{OR_OPT_PASSES} passes) on random tours of the 1000-city 20-cluster EUC_2D instance",
@@ -827,7 +827,7 @@ def main_or_opt(args) -> int:
                       "e2e": {"value": cpu["value"], "unit": "entries/s", "h2d_bytes_per_step": 0,
                               "d2h_bytes_per_step": 0}}))
     return 0
-  torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+  world, rank = _init_ranks()  # this rank's GPU and, under torchrun, the NCCL group
   build_library()
   lib = native.load_library()
   ops = operands_for(ctx)
