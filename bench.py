@@ -4,15 +4,27 @@ Workload (one step): 1024 random-permutation tours of a 1000-city, 20-cluster
 Gaussian-mixture EUC_2D instance (sigma 30, [0, 1000]^2, int32 matrix), refined to a
 local optimum with candidate_k=20, once in best mode and once in first mode. The
 metric counts the (i, j) pairs the reference's CPU scan evaluates on the same tours
-(oracle-equivalent 2-opt deltas), summed over every pass of every tour; the kernel
-reports that count itself and tests pin it to the oracle.
+(oracle-equivalent 2-opt deltas), summed over every pass of every tour.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-- `value`: deltas/s with tours already resident in HBM, timed with CUDA events on
-  the launching stream, L2 flushed (256 MiB write) between timed steps.
+- `value`: deltas/s with tours already resident in HBM, timed with CUDA events on the
+  launching stream, L2 flushed (256 MiB write) between timed steps. The timed launches
+  pass no stats buffer, so first mode runs without its pair-count bookkeeping; the pair
+  count comes from one untimed launch of the same tours with stats (the kernel counts the
+  pairs itself, and tests pin the count to the oracle), and every timed launch must
+  return exactly that launch's tours.
 - `e2e`: the same metric through `LocalSearchB200TourTwoOpt.improve_batch` on host
   NumPy tours (pinned H2D, kernel, D2H per call), timed with CUDA events.
+- `parity`: a sample of the timed tours, spread over the batch, refined by the NumPy
+  oracle in both modes on the host cores; tours, passes, pairs and moves must equal the
+  GPU's, or the run exits non-zero after printing its line.
+- `roofline`: the dominant launch against the two ceilings of an L2-resident scan, the
+  L2 gather rate and the INT32 issue rate, both measured in the same run
+  (`tsp_gpu_clean_b200.roofline`), with per-gain counter figures from one ncu capture.
+- `detail.ga1000`: the memetic GA at n = 1000 (population 512, 100 generations, 64
+  elites, best-mode 2-opt k = 20 x 10): device generations/s, end to end, and the NumPy
+  GA on one host core.
 - `--impl reference`: the reference CPU path (the NumPy oracle restatement of
   `LocalSearchCPUTourTwoOpt`) on the host cores, on a bounded sample of tours.
 - N > 1 (torchrun): every rank refines its own 1024 tours (weak scaling, no
@@ -43,15 +55,20 @@ METRIC = "2-opt deltas/s"
 UNIT = "deltas/s"
 MODES = ("best", "first")
 K_CAND = 20
-#: Algorithmic bytes per 2-opt delta: three int32 distances (d(a,c), d(b,d) and the
-#: two retired edges count as one cached read each side) = 12 B, plus the candidate,
-#: position and successor reads = 12 B.
-BYTES_PER_DELTA = 24
+#: Algorithmic work per 2-opt delta: three int32 distances d(a,c), d(b,d) and the retired
+#: edges (12 B, the L2-side figure) and about 12 integer operations.
+ALG_BYTES_PER_DELTA = 12
+ALG_OPS_PER_DELTA = 12
 L2_FLUSH_BYTES = 256 << 20
-#: DRAM bytes (read + write) of one launch of the default workload's scan kernels, from one
-#: ncu capture of this command (profiles/two_opt_scan_c2.md); only the default 1024-tour,
-#: 128-thread scan configuration has a captured figure.
-NCU_DRAM_BYTES_PER_LAUNCH = {"best": 8_833_536, "first": 8_825_856}
+#: Per evaluated gain of the scan kernel with 128-thread CTAs on this workload's tours
+#: (counted launches, first 256 tours of the batch), from one ncu capture:
+#: warp instructions executed (sm__inst_executed.sum), L2 sector bytes
+#: (lts__t_bytes.sum) and DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum,
+#: per 1024-tour launch).
+NCU_PER_GAIN: dict[str, dict[str, float]] = {}
+#: CPU parity sample: tours of the timed batch refined by the oracle (at least this many)
+PARITY_TOURS = 16
+GA_SUB_WORKLOAD = "ga1000"
 
 
 def _peaks() -> dict:
@@ -65,29 +82,63 @@ def _peaks() -> dict:
 
 # ----------------------------------------------------------------------------------- CPU
 def _cpu_worker(args):
-  """Refine one tour in both modes with the oracle; returns (pairs, seconds)."""
+  """Refine one tour in best then first mode with the oracle.
+
+  Returns ({mode: (tour, (passes, pairs, moves))}, seconds of refinement)."""
   coords, tour = args
   from oracle import distances, two_opt
 
   D = distances.euc2d_matrix(coords)
   cand = distances.candidate_list(K_CAND, coords=coords)
   t0 = time.perf_counter()
-  pairs = 0
+  out = {}
   for mode in MODES:
-    _, st = two_opt.improve_batch(tour[None, :], D, cand, mode, 10**9)
-    pairs += int(st[0, 1])
-  return pairs, time.perf_counter() - t0
+    t, st = two_opt.improve_batch(tour[None, :], D, cand, mode, 10**9)
+    out[mode] = (t[0], tuple(int(v) for v in st[0]))
+  return out, time.perf_counter() - t0
 
 
-def cpu_sample(pool, workers: int, seed_offset: int = 0) -> dict:
-  """Oracle deltas/s on `workers` tours in parallel (one tour per process)."""
+def parity_indices(tours: int, count: int) -> list[int]:
+  """`count` tour indices spread evenly over a batch of `tours` (first and last included)."""
+  return sorted({int(round(v)) for v in np.linspace(0, tours - 1, min(count, tours))})
+
+
+def cpu_sample(pool, tours_np: np.ndarray, indices) -> dict:
+  """Oracle deltas/s over the given tours of the batch in parallel (one tour per process),
+  with each tour's refined result per mode for the parity check."""
   coords, _ = instances.two_opt_workload(tours=1)
-  tours = instances.random_tours(instances.TWO_OPT_N, workers, 777 + seed_offset)
   t0 = time.perf_counter()
-  res = pool.map(_cpu_worker, [(coords, tours[i]) for i in range(workers)])
+  res = pool.map(_cpu_worker, [(coords, tours_np[i]) for i in indices])
   wall = time.perf_counter() - t0
-  pairs = sum(r[0] for r in res)
-  return {"value": pairs / wall, "pairs": pairs, "wall_s": wall, "tours": workers}
+  pairs = sum(st[1] for out, _ in res for _, st in out.values())
+  return {"value": pairs / wall, "pairs": pairs, "wall_s": wall, "tours": len(indices),
+          "tours_per_s": len(indices) * len(MODES) / wall, "indices": list(indices),
+          "results": [out for out, _ in res]}
+
+
+def cpu_one_core(pool, tours_np: np.ndarray, index: int) -> dict:
+  """The same oracle on one tour with no other worker busy: deltas/s of one host core."""
+  coords, _ = instances.two_opt_workload(tours=1)
+  out, secs = pool.apply(_cpu_worker, ((coords, tours_np[index]),))
+  pairs = sum(st[1] for _, st in out.values())
+  return {"value": pairs / secs, "pairs": pairs, "seconds": secs, "tours_per_s": len(MODES) / secs, "tour": index}
+
+
+def check_parity(gpu: dict, cpu: dict) -> dict:
+  """Compare the oracle's refinements with the GPU's counted launch at the same indices."""
+  bad = []
+  for i, out in zip(cpu["indices"], cpu["results"]):
+    for m, (tour, st) in out.items():
+      g_tour, g_st = gpu[m]
+      if not np.array_equal(g_tour[i], tour):
+        bad.append(f"{m} tour {i}: tours differ")
+      elif tuple(int(v) for v in g_st[i][:3]) != st:
+        bad.append(f"{m} tour {i}: (passes, pairs, moves) {tuple(int(v) for v in g_st[i][:3])} vs {st}")
+  n = len(cpu["indices"])
+  total = len(next(iter(gpu.values()))[0])
+  return {"ok": not bad, "text": (f"bit-exact on {n}/{total} tours (both modes: tours, passes, pairs, moves)" if not bad
+                                  else f"MISMATCH on {len(bad)} of {n * len(MODES)} refinements"),
+          "mismatches": bad[:8]}
 
 
 # ------------------------------------------------------------------------------ clocks
@@ -197,27 +248,59 @@ def aggregate(units: float, elapsed_s: float, world: int):
   return float(u.item()), float(e.item())
 
 
-def run_gpu(args, pool) -> dict | None:
-  import torch
-  import torch.distributed as dist
+def two_opt_tours(count: int, rank: int) -> np.ndarray:
+  """The workload's random tours of one rank (rank 0: the batch the CPU parity sample reads)."""
+  return instances.random_tours(instances.TWO_OPT_N, count, instances.TWO_OPT_TOUR_SEED + 1000 * rank)
 
-  from tsp_gpu_clean_b200 import native
-  from tsp_gpu_clean_b200.build import build_library
+
+def _roofline(dominant: str, gains: int, launch_s: float, peaks: dict, tours: int, threads: int, kernel: str) -> dict:
+  """The dominant launch against the L2-gather and INT32-issue ceilings measured in this run.
+
+  Counter-based figures (instructions and L2 bytes per evaluated gain, from one ncu capture
+  of the same kernel on this workload's tours) are used where they exist; otherwise the
+  algorithmic ones (12 B and 12 integer operations per gain)."""
+  per = NCU_PER_GAIN.get(dominant) if (kernel == "scan" and threads == 128) else None
+  gps = gains / launch_s
+  int_peak = peaks["int32_tops"]
+  l2_peak = peaks["l2_sector_gbs"]
+  alg = {"l2_gbs": gps * ALG_BYTES_PER_DELTA / 1e9, "int32_tops": gps * ALG_OPS_PER_DELTA / 1e12,
+         "basis": f"{ALG_BYTES_PER_DELTA} B and {ALG_OPS_PER_DELTA} integer ops per evaluated gain"}
+  alg["l2_frac_of_useful"] = alg["l2_gbs"] / peaks["l2_useful_gbs"]
+  alg["int32_frac"] = alg["int32_tops"] / int_peak
+  if per is not None:
+    int_ach = gps * per["inst"] * 32 / 1e12  # warp instructions issued, as lane operations
+    l2_ach = gps * per["lts_bytes"] / 1e9
+    basis = (f"ncu per evaluated gain: {per['inst']:.2f} warp instructions, {per['lts_bytes']:.2f} L2 sector bytes; "
+             f"x {gains} gains per launch / {launch_s * 1e3:.2f} ms")
+  else:
+    int_ach, l2_ach = alg["int32_tops"], alg["l2_gbs"] * 32 / 4
+    basis = "algorithmic (no ncu figure for this launch shape): " + alg["basis"]
+  l2 = {"achieved": l2_ach, "peak": l2_peak, "unit": "GB/s", "frac": l2_ach / l2_peak}
+  i32 = {"achieved": int_ach, "peak": int_peak, "unit": "TOP/s", "frac": int_ach / int_peak}
+  top = i32 if i32["frac"] >= l2["frac"] else l2
+  traffic = None
+  if per is not None and tours == instances.TWO_OPT_TOURS:
+    traffic = per.get("dram_bytes_per_launch")
+  return {"bound": "int32" if top is i32 else "l2", "achieved": top["achieved"], "peak": top["peak"],
+          "unit": top["unit"], "frac": top["frac"], "traffic": traffic,
+          "kernel": f"two_opt_{kernel}_kernel<{dominant}>", "peak_source": "measured in this run: " + peaks["method"],
+          "basis": basis, "int32": i32, "l2": l2, "algorithmic": alg,
+          "hbm_note": "DRAM traffic is the matrix, the packed k-NN table and the tours once per launch; HBM is "
+                      "not the bound"}
+
+
+def run_gpu(args, world: int, rank: int) -> dict:
+  import torch
+
+  from tsp_gpu_clean_b200 import native, roofline
   from tsp_gpu_clean_b200.device import operands_for, ptr, stream_handle
   from tsp_gpu_clean_b200.problem import Problem, ProblemContext
   from tsp_gpu_clean_b200.strategies.local_search import LocalSearchB200TourTwoOpt
 
-  world, rank, local = _dist_env()
-  torch.cuda.set_device(local)
-  if world > 1:
-    import datetime
-
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-  build_library()
+  local = int(os.environ.get("LOCAL_RANK", "0"))
   lib = native.load_library()
-
   coords, _ = instances.two_opt_workload(tours=1)
-  tours_np = instances.random_tours(instances.TWO_OPT_N, args.tours, instances.TWO_OPT_TOUR_SEED + 1000 * rank)
+  tours_np = two_opt_tours(args.tours, rank)
   n = instances.TWO_OPT_N
   ctx = ProblemContext(Problem.from_coordinates(coords, "clustered1000"), seed=0)
   ops = operands_for(ctx)
@@ -234,24 +317,42 @@ def run_gpu(args, pool) -> dict | None:
   rev_idx = tabs.rev_idx if use_rev else None
   packed = tabs.packed if args.kernel == "scan" else None
   pristine = torch.from_numpy(tours_np).cuda()
-  work = torch.empty_like(pristine)
-  stats = {m: torch.zeros((args.tours, 4), dtype=torch.int64, device="cuda") for m in MODES}
+  modes = MODES if args.mode == "both" else (args.mode,)
+  work = {m: torch.empty_like(pristine) for m in modes}
+  stats = {m: torch.zeros((args.tours, 4), dtype=torch.int64, device="cuda") for m in modes}
   status = torch.zeros(args.tours, dtype=torch.int32, device="cuda")
   flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
   stream = torch.cuda.current_stream()
-  modes = MODES if args.mode == "both" else (args.mode,)
 
-  def step(ev_pairs):
+  def launch(m, counted):
+    rc = lib.tspb_two_opt(ptr(work[m]), args.tours, n, ptr(dist_t), stride, ptr(coords_t), ptr(tabs.cand),
+                          ptr(tabs.cand_dist), ptr(rev_off), ptr(rev_idx), ptr(packed), k, native.MODE_CODES[m],
+                          args.max_iter, args.threads, ptr(stats[m]) if counted else None, ptr(status), None, 0,
+                          stream_handle())
+    native.check("tspb_two_opt", rc)
+
+  def check_status():
+    bad = int(status.max().item())
+    if bad != 0:
+      raise RuntimeError(f"2-opt kernel reported {native.status_text(bad)}")
+
+  # the counted launch (untimed): pair, pass, move and gain counts, and the tours every
+  # timed launch must reproduce
+  counted = {}
+  for m in modes:
+    work[m].copy_(pristine)
+    launch(m, True)
+  torch.cuda.synchronize()
+  check_status()
+  for m in modes:
+    counted[m] = (work[m].cpu().numpy(), stats[m].cpu().numpy())
+
+  def step(ev):
     for m in modes:
-      work.copy_(pristine)
-      ev_pairs[m][0].record(stream)
-      rc = lib.tspb_two_opt(ptr(work), args.tours, n, ptr(dist_t), stride, ptr(coords_t), ptr(tabs.cand),
-                            ptr(tabs.cand_dist),
-                            ptr(rev_off), ptr(rev_idx), ptr(packed), k,
-                            native.MODE_CODES[m], args.max_iter, args.threads, ptr(stats[m]), ptr(status), None, 0,
-                            stream_handle())
-      native.check("tspb_two_opt", rc)
-      ev_pairs[m][1].record(stream)
+      work[m].copy_(pristine)
+      ev[m][0].record(stream)
+      launch(m, False)
+      ev[m][1].record(stream)
 
   def new_events():
     return {m: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for m in modes}
@@ -259,12 +360,11 @@ def run_gpu(args, pool) -> dict | None:
   for _ in range(args.warmup):
     step(new_events())
   torch.cuda.synchronize()
-  if int(status.max().item()) != 0:
-    raise RuntimeError("2-opt kernel reported a bad tour")
+  check_status()
+  peaks = roofline.measure_peaks()  # the scan's ceilings on this device, before the timed region
 
   per_step = []
-  if world > 1:
-    dist.barrier()
+  _barrier(world)
   torch.cuda.synchronize()
   with ClockSampler(local) as clocks:
     for _ in range(args.steps):
@@ -273,23 +373,29 @@ def run_gpu(args, pool) -> dict | None:
       step(ev)
       per_step.append(ev)
     torch.cuda.synchronize()
-  if world > 1:
-    dist.barrier()
+  _barrier(world)
+  check_status()
+  for m in modes:
+    if not np.array_equal(work[m].cpu().numpy(), counted[m][0]):
+      raise RuntimeError(f"{m}: a timed launch returned other tours than the counted launch")
   kernel_ms = {m: sum(e[m][0].elapsed_time(e[m][1]) for e in per_step) for m in modes}
   total_ms = sum(kernel_ms.values())
-  st = {m: stats[m].cpu().numpy() for m in modes}
+  st = {m: counted[m][1] for m in modes}
   pairs_step = sum(int(st[m][:, 1].sum()) for m in modes)
   eval_step = sum(int(st[m][:, 3].sum()) for m in modes)
   units_all, elapsed = aggregate(pairs_step * args.steps, total_ms / 1e3, world)
+  tours_all, _ = aggregate(args.tours * len(modes) * args.steps, total_ms / 1e3, world)
   value = units_all / elapsed
 
-  # end to end: the public strategy call on host tours (pinned H2D + kernel + D2H)
+  # end to end: the public strategy call on host tours (pinned H2D + kernel + D2H); no
+  # stats requested, like the timed launches; the counts are the counted launch's
   e2e_ms = 0.0
   strategies = {m: LocalSearchB200TourTwoOpt(max_iterations=args.max_iter, mode=m, candidate_k=K_CAND,
                                               threads_per_block=args.threads) for m in modes}
   for s_ in strategies.values():
     s_.kernel = args.kernel
     s_.incremental_first = args.first_restart == "incremental"
+    s_.collect_stats = False
   for m in modes:
     strategies[m].improve_batch(tours_np, ctx)  # warm
   torch.cuda.synchronize()
@@ -303,42 +409,35 @@ def run_gpu(args, pool) -> dict | None:
       e1.record(stream)
       torch.cuda.synchronize()
       e2e_ms += e0.elapsed_time(e1)
-      e2e_pairs += int(strategies[m].last_stats[:, 1].sum())
+      if not np.array_equal(out, counted[m][0]):
+        raise RuntimeError(f"{m}: the public call returned other tours than the counted launch")
+      e2e_pairs += int(st[m][:, 1].sum())
   e2e_units, e2e_elapsed = aggregate(e2e_pairs, e2e_ms / 1e3, world)
   del out
 
   dominant = max(modes, key=lambda m: kernel_ms[m])
   launches = args.steps * len(modes)
-  dom_ms = kernel_ms[dominant] / args.steps
+  dom_s = kernel_ms[dominant] / args.steps / 1e3
   dom_eval = int(st[dominant][:, 3].sum())
-  achieved_gbs = dom_eval * BYTES_PER_DELTA / (dom_ms / 1e3) / 1e9
-  peaks = _peaks()
-  res = {
+  return {
     "value": value,
     "ms_per_step": total_ms / args.steps,
     "kernel_ms_per_step": {m: kernel_ms[m] / args.steps for m in modes},
+    "tours_per_s": tours_all / elapsed,
     "pairs_per_step": pairs_step,
     "evaluated_per_step": eval_step,
     "passes_per_step": {m: int(st[m][:, 0].sum()) for m in modes},
+    "moves_per_step": {m: int(st[m][:, 2].sum()) for m in modes},
     "clocks": clocks.summary(),
     "e2e": {"value": e2e_units / e2e_elapsed, "unit": UNIT,
             "h2d_bytes_per_step": int(tours_np.nbytes * len(modes)),
-            "d2h_bytes_per_step": int(tours_np.nbytes * len(modes) + args.tours * 32 * len(modes))},
+            "d2h_bytes_per_step": int(tours_np.nbytes * len(modes) + 4 * len(modes))},  # tours + status max
     "gpu_launches": launches,
-    "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                 "frac": achieved_gbs / peaks["hbm_gbs"],
-                 "traffic": (NCU_DRAM_BYTES_PER_LAUNCH[dominant]
-                             if (args.tours, args.threads, args.kernel, args.max_iter)
-                             == (instances.TWO_OPT_TOURS, 128, "scan", 10**9) else None),
-                 "kernel": f"two_opt_{args.kernel}_kernel<{dominant}>",
-                 "peak_source": peaks["source"],
-                 "basis": f"{BYTES_PER_DELTA} B per gain the kernel computed"},
-    "world": world,
-    "rank": rank,
+    "roofline": _roofline(dominant, dom_eval, dom_s, peaks, args.tours, args.threads, args.kernel),
+    "peaks": peaks,
+    "counted": counted,
+    "tours_np": tours_np,
   }
-  if world > 1:
-    dist.destroy_process_group()
-  return res if rank == 0 else None
 
 
 GA_WORKLOADS = {
@@ -393,10 +492,11 @@ def _ga_cpu_gens_per_s(name: str, sample_gens: int) -> dict:
   t0 = time.perf_counter()
   oga.OracleGA(D, provider, cfg, np.random.default_rng(42)).evolve(0, patience=10**9)
   t1 = time.perf_counter()
-  oga.OracleGA(D, provider, cfg, np.random.default_rng(42)).evolve(sample_gens, patience=10**9)
+  res = oga.OracleGA(D, provider, cfg, np.random.default_rng(42)).evolve(sample_gens, patience=10**9)
   t2 = time.perf_counter()
   loop = max((t2 - t1) - (t1 - t0), 1e-9)
-  return {"value": sample_gens / loop, "gens": sample_gens, "loop_s": loop}
+  return {"value": sample_gens / loop, "gens": sample_gens, "loop_s": loop,
+          "history": [float(v) for v in res[3]["convergence_history"]]}
 
 
 def _ga_cpu_sample(name: str, sample_gens: int) -> dict:
@@ -406,7 +506,7 @@ def _ga_cpu_sample(name: str, sample_gens: int) -> dict:
   reps = ga_options(name)["reps"]
   if reps == 1:
     r = _ga_cpu_gens_per_s(name, sample_gens)
-    return {"value": r["value"], "cores": 1, "loop_s": r["loop_s"],
+    return {"value": r["value"], "cores": 1, "loop_s": r["loop_s"], "history": r["history"],
             "sample": f"{sample_gens} generations of the NumPy GA (init excluded), {r['loop_s']:.1f} s"}
   import multiprocessing as mp
 
@@ -419,17 +519,18 @@ def _ga_cpu_sample(name: str, sample_gens: int) -> dict:
                     f"processes, {busy:.1f} s per process"}
 
 
-def run_ga_bench(args) -> dict:
+def ga_measure(workload: str, warmup: int, steps: int, world: int, rank: int, engine: str = "batch", chunk: int = 16,
+               no_graph: bool = False, batch_incremental: str = "off", generations: int | None = None) -> dict:
+  """Device and end-to-end generations/s of one GA workload on this rank's GPU (the
+  process group, if any, is the caller's)."""
   import torch
 
-  from tsp_gpu_clean_b200.build import build_library
   from tsp_gpu_clean_b200.fused import FusedMemeticSolver, LocalSearchConfig
   from tsp_gpu_clean_b200.problem import Problem, ProblemContext
 
-  world, rank = _init_ranks()
-  build_library()
-  n, P, G, elite, post_init, seed, desc = GA_WORKLOADS[args.workload]
-  o = ga_options(args.workload)
+  n, P, G, elite, post_init, seed, desc = GA_WORKLOADS[workload]
+  G = generations or G
+  o = ga_options(workload)
   reps = o["reps"]
   coords = instances.uniform_instance(n, seed)
 
@@ -437,8 +538,8 @@ def run_ga_bench(args) -> dict:
   from tsp_gpu_clean_b200.batch import FusedBatchSolver
 
   tuner = BatchAutotuner()
-  if args.engine != "batch" and (reps > 1 or o != GA_DEFAULT_OPTIONS):
-    raise SystemExit(f"--engine single does not run the {args.workload} workload")
+  if engine != "batch" and (reps > 1 or o != GA_DEFAULT_OPTIONS):
+    raise SystemExit(f"--engine single does not run the {workload} workload")
 
   def run_once():
     # replicas per rank: the same instance, each run's generator seeded per rank and repetition
@@ -448,30 +549,32 @@ def run_ga_bench(args) -> dict:
     ls = LocalSearchConfig("best", 10, 20)
     gc.collect()  # the previous runs' garbage, outside the timed call
     t0 = time.perf_counter()
-    if args.engine == "batch":
+    if engine == "batch":
       solver = FusedBatchSolver(population_size=P, mutation_rate=o["rate"], tournament_k=5, nn_k=5, local_search=ls,
                                 elite_count=elite, post_init=post_init, max_matrix_dimension=None, tuner=tuner,
-                                chunk=args.chunk, use_graph=not args.no_graph, crossover=o["crossover"],
+                                chunk=chunk, use_graph=not no_graph, crossover=o["crossover"],
                                 mutation=o["mutation"], init=o["init"], local_search_stage=o["stage"],
-                                incremental=args.batch_incremental)
+                                incremental=batch_incremental)
       results = solver.evolve(ctxs, G, patience=10**9)
       stats = {"generations_completed": sum(st["generations_completed"] for _, st in results),
-               "best_fitness": min(st["best_fitness"] for _, st in results)}
+               "best_fitness": min(st["best_fitness"] for _, st in results),
+               "history": results[0][1]["convergence_history"]}
     else:
       solver = FusedMemeticSolver(population_size=P, mutation_rate=0.05, tournament_k=5, nn_k=5, local_search=ls,
-                                  elite_count=elite, post_init=post_init, chunk=args.chunk, engine="single",
-                                  use_graph=not args.no_graph)
+                                  elite_count=elite, post_init=post_init, chunk=chunk, engine="single",
+                                  use_graph=not no_graph)
       best, stats = solver.evolve(ctxs[0], list(range(n)), G, patience=10**9)
+      stats = {**stats, "history": stats["convergence_history"]}
     wall = time.perf_counter() - t0
     return solver, stats, wall
 
-  for _ in range(args.warmup):
+  for _ in range(warmup):
     run_once()
   torch.cuda.synchronize()
   _barrier(world)
   loop_ms, walls, launches, gens = [], [], 0, 0
   with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
-    for _ in range(args.steps):
+    for _ in range(steps):
       solver, stats, wall = run_once()
       loop_ms.append(solver.last_timing["loop_ms_device"])
       walls.append(wall)
@@ -481,18 +584,29 @@ def run_ga_bench(args) -> dict:
   _barrier(world)
   units, loop_s = aggregate(gens, sum(loop_ms) / 1e3, world)
   e2e_units, wall_s = aggregate(gens, sum(walls), world)
-  _finish_ranks(world)
   value = units / loop_s
-  return {"value": value, "ms_per_step": 1e3 * loop_s / args.steps, "clocks": clocks.summary(), "world": world,
+  return {"value": value, "ms_per_step": 1e3 * loop_s / steps, "clocks": clocks.summary(), "world": world,
           "rank": rank,
           "e2e": {"value": e2e_units / wall_s, "unit": "generations/s", "h2d_bytes_per_step": int(reps * coords.nbytes),
                   "d2h_bytes_per_step": int(reps * (n * 4 + (G + 1) * 8 + P * n * 4))},
-          "gpu_launches": launches, "desc": desc, "best": stats["best_fitness"],
+          "gpu_launches": launches, "desc": desc, "best": stats["best_fitness"], "history": stats["history"],
           "loop_ms_steps": [round(v, 3) for v in loop_ms], "walls_s": [round(w, 4) for w in walls],
           "buckets": [{"n": [b.lo, b.hi], "two_opt_threads": b.two_opt_threads, "incremental": b.incremental,
                        "offspring_threads": b.offspring_threads} for b in getattr(solver, "buckets", [])],
           "two_opt_totals": getattr(solver, "two_opt_totals", None),
           "timing": {k: round(v, 4) for k, v in solver.last_timing.items() if isinstance(v, (int, float))}}
+
+
+def run_ga_bench(args) -> dict:
+  from tsp_gpu_clean_b200.build import build_library
+
+  world, rank = _init_ranks()
+  build_library()
+  try:
+    return ga_measure(args.workload, args.warmup, args.steps, world, rank, engine=args.engine, chunk=args.chunk,
+                      no_graph=args.no_graph, batch_incremental=args.batch_incremental)
+  finally:
+    _finish_ranks(world)
 
 
 # ------------------------------------------------------------------------ uneven batch
@@ -927,6 +1041,7 @@ def main(argv=None) -> int:
                        "solver's default) uses the plain kernel")
   ap.add_argument("--cpu-workers", type=int, default=0, help="0: all host cores, capped at 64")
   ap.add_argument("--no-cpu-baseline", action="store_true")
+  ap.add_argument("--no-ga", action="store_true", help="two_opt: leave out the ga1000 sub-result")
   ap.add_argument("--workload", default="two_opt", choices=["two_opt", "learned", "uneven", "or_opt", *GA_WORKLOADS])
   ap.add_argument("--instances", type=int, default=256, help="uneven: instances in the batch")
   ap.add_argument("--generations", type=int, default=100, help="uneven: generations")
@@ -966,7 +1081,13 @@ def main(argv=None) -> int:
             "tours": args.tours, "n": instances.TWO_OPT_N, "k": K_CAND, "modes": list(MODES if args.mode == "both" else (args.mode,)),
             "l2": "flushed between timed steps (256 MiB write); the 4 MB matrix is L2-resident within a step",
             "threads_per_cta": args.threads, "kernel": args.kernel, "distances": args.distances,
-            "first_restart": args.first_restart}
+            "first_restart": args.first_restart,
+            "counting": "timed launches pass no stats buffer (first mode then skips its per-row pair-count "
+                        "bookkeeping); the pair count is that of one untimed counted launch of the same tours, "
+                        "whose tours every timed launch reproduces (checked)"}
+  sample_gens = args.cpu_gens or 6
+  tours_np = two_opt_tours(args.tours, rank)
+  indices = parity_indices(args.tours, max(PARITY_TOURS, workers))
 
   if args.impl == "reference":
     if rank != 0:
@@ -974,29 +1095,49 @@ def main(argv=None) -> int:
     ctx = mp.get_context("spawn")
     with ctx.Pool(workers) as pool:
       for w in range(args.warmup):
-        cpu_sample(pool, workers, seed_offset=w)
-      vals = [cpu_sample(pool, workers, seed_offset=100 + s) for s in range(args.steps)]
+        pool.map(_cpu_worker, [(instances.two_opt_workload(tours=1)[0], tours_np[i]) for i in indices[:workers]])
+      vals = [cpu_sample(pool, tours_np, indices) for _ in range(args.steps)]
+      one = cpu_one_core(pool, tours_np, indices[0])
+      ga_cpu = pool.apply(_ga_cpu_gens_per_s, (GA_SUB_WORKLOAD, sample_gens))
     value = sum(v["pairs"] for v in vals) / sum(v["wall_s"] for v in vals)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * sum(v["wall_s"] for v in vals) / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded)", "impl": "reference", "config": config,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port",
-                             "sample": f"{workers} tours per step (one per process), best then first mode to local optimum"},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                             "sample": f"{len(indices)} tours of the batch per step over {workers} processes (one tour "
+                                       "per task), best then first mode to a local optimum",
+                             "tours_per_s": statistics.mean(v["tours_per_s"] for v in vals),
+                             "one_core": {k: one[k] for k in ("value", "tours_per_s", "seconds")}},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "detail": {GA_SUB_WORKLOAD: {"metric": "generations/s", "cpu_one_core": ga_cpu["value"],
+                                         "sample": f"{sample_gens} generations of the NumPy GA on one core, "
+                                                   f"{ga_cpu['loop_s']:.1f} s (init excluded)"}}}
     print(json.dumps(line))
     return 0
 
-  cpu = None
   pool = None
   if rank == 0 and world == 1 and not args.no_cpu_baseline:
     pool = mp.get_context("spawn").Pool(workers)  # before the first CUDA call
-  res = run_gpu(args, pool)
+  from tsp_gpu_clean_b200.build import build_library
+
+  world, rank = _init_ranks()
+  build_library()
+  res = run_gpu(args, world, rank)
+  ga = None
+  if not args.no_ga:
+    ga = ga_measure(GA_SUB_WORKLOAD, max(args.warmup, 1), max(args.steps, 3), world, rank)
+  _finish_ranks(world)
+  cpu = one = ga_cpu = parity = ga_parity = None
   if pool is not None:
-    cpu = cpu_sample(pool, workers)
+    cpu = cpu_sample(pool, res["tours_np"], indices)
+    parity = check_parity(res["counted"], cpu)
+    one = cpu_one_core(pool, res["tours_np"], indices[0])
+    if ga is not None:
+      ga_cpu = pool.apply(_ga_cpu_gens_per_s, (GA_SUB_WORKLOAD, sample_gens))
     pool.close()
     pool.join()
-  if res is None:
+  if rank != 0:
     return 0
   line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
           "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
@@ -1004,12 +1145,40 @@ def main(argv=None) -> int:
           "clocks": res["clocks"], "e2e": res["e2e"], "gpu_launches": res["gpu_launches"],
           "roofline": res["roofline"],
           "detail": {"kernel_ms_per_step": res["kernel_ms_per_step"], "pairs_per_step": res["pairs_per_step"],
-                     "evaluated_per_step": res["evaluated_per_step"], "passes_per_step": res["passes_per_step"]}}
+                     "evaluated_per_step": res["evaluated_per_step"], "passes_per_step": res["passes_per_step"],
+                     "moves_per_step": res["moves_per_step"], "tours_per_s": res["tours_per_s"],
+                     "peaks": res["peaks"]}}
+  if parity is not None:
+    line["parity"] = parity["text"]
+    if parity["mismatches"]:
+      line["detail"]["parity_mismatches"] = parity["mismatches"]
   if cpu is not None:
     line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": workers, "kind": "port",
-                            "sample": f"{cpu['tours']} tours (one per process), best then first mode to local optimum, "
-                                      f"{cpu['wall_s']:.1f} s wall"}
+                            "sample": f"{cpu['tours']} tours of the timed batch (indices spread over it, one per "
+                                      f"process), best then first mode to a local optimum, {cpu['wall_s']:.1f} s wall",
+                            "tours_per_s": cpu["tours_per_s"],
+                            "one_core": {"value": one["value"], "tours_per_s": one["tours_per_s"],
+                                         "seconds": one["seconds"], "tour": one["tour"]}}
+  if ga is not None:
+    sub = {"workload": ga["desc"], "metric": "generations/s", "value": ga["value"], "e2e": ga["e2e"]["value"],
+           "ms_per_run": ga["ms_per_step"], "walls_s": ga["walls_s"], "clocks": ga["clocks"],
+           "gpu_launches": ga["gpu_launches"]}
+    if ga_cpu is not None:
+      sub["cpu_one_core"] = ga_cpu["value"]
+      sub["cpu_sample"] = f"{sample_gens} generations of the NumPy GA on one core, {ga_cpu['loop_s']:.1f} s"
+      sub["vs_cpu_one_core"] = {"device": ga["value"] / ga_cpu["value"], "e2e": ga["e2e"]["value"] / ga_cpu["value"]}
+      # the first generations of the same seeded run on the device, against the oracle's
+      short = ga_measure(GA_SUB_WORKLOAD, 0, 1, 1, 0, generations=sample_gens) if world == 1 else None
+      if short is not None:
+        ok = [float(v) for v in short["history"]] == ga_cpu["history"]
+        sub["parity"] = (f"best-fitness history of the first {sample_gens} generations equal to the oracle GA's"
+                         if ok else "MISMATCH of the best-fitness history against the oracle GA")
+        if not ok:
+          parity = {"ok": False}
+    line["detail"][GA_SUB_WORKLOAD] = sub
   print(json.dumps(line))
+  if parity is not None and not parity["ok"]:
+    return 1
   return 0
 
 

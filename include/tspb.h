@@ -33,6 +33,7 @@ extern "C" {
 #define TSPB_ERR_UNSUPPORTED 5    /* configuration outside the kernels' scope */
 #define TSPB_ERR_WORKSPACE 6      /* caller workspace smaller than tspb_*_workspace_bytes */
 #define TSPB_ERR_BUDGET 7         /* a tour hit the device watchdog before converging */
+#define TSPB_ERR_DEVICE_MEMORY 8  /* the device could not provide memory the library itself holds */
 
 #define TSPB_MODE_BEST 0       /* steepest move per pass; also the "batch" mode */
 #define TSPB_MODE_FIRST 1      /* first improving move in scan order */
@@ -43,6 +44,17 @@ int tspb_version(void);
 
 /* Human-readable text for a TSPB_* status code (static storage). */
 const char* tspb_status_string(int status);
+
+/*
+ * Device watchdog of the local-search kernels (2-opt in every mode, the batch 2-opt,
+ * Or-opt, 3-opt): a tour that has not converged after `cycles` SM clock cycles ends with
+ * TSPB_ERR_BUDGET, its tour left a valid permutation (the moves applied so far) and its
+ * stats counting the passes run. Applies to launches made after the call, process-wide;
+ * a launch captured in a CUDA graph keeps the budget it was captured with. cycles <= 0
+ * restores the default (2^36 cycles, about 35 s at 1.9 GHz). Returns the previous budget.
+ * No counterpart in the reference (its loops run on the host and stop on max_iterations).
+ */
+int64_t tspb_set_watchdog_cycles(int64_t cycles);
 
 /* Bytes of global scratch `tspb_two_opt` needs for this shape (0 when none). */
 size_t tspb_two_opt_workspace_bytes(int32_t num_tours, int32_t n, int32_t k, int32_t mode, int32_t block_threads);
@@ -106,6 +118,14 @@ int tspb_two_opt_gated(const int32_t* skip, int32_t* tours, int32_t num_tours, i
  *     TSPB_STATIC_SCRATCH_BYTES); split the batch into smaller calls then.
  *   - The first call on a device looks up the array's device address (set-up, once per
  *     device, with that device current); make that first call before any stream capture.
+ *     Under lazy module loading (CUDA_MODULE_LOADING=LAZY, CUDA's default) that first call
+ *     is also when the device reserves the array, so a caller that must not allocate later
+ *     makes it during its own set-up. When the device cannot provide the array the call
+ *     returns TSPB_ERR_DEVICE_MEMORY (other lookup failures: TSPB_ERR_CUDA) and clears the
+ *     CUDA error it caused.
+ *   - The address is kept per device with the identity of the context it belongs to; after
+ *     a reset of the device's context (cudaDeviceReset, or the primary context released and
+ *     created again) the next call looks it up again, reserving the array anew.
  *   - All calls share the array: calls whose kernels overlap on the GPU race on it and
  *     must be serialised by the caller.
  */
@@ -589,6 +609,20 @@ int tspb_validate_perm(const int32_t* tours, int32_t num_tours, int32_t n, int32
  *   (src/distances/kernels/pairwise_device.cuh:58-60).
  */
 int tspb_euc2d_matrix(const double* coords, int32_t n, int32_t* dist, int64_t dist_stride, void* stream);
+
+/*
+ * Roofline microbenchmarks (no counterpart in the reference; they measure the ceilings of
+ * the L2-resident 2-opt scan on the machine at hand). Time each launch with CUDA events.
+ *   tspb_microbench_l2_gather: blocks x 256 threads x iters x 8 random 4-byte loads
+ *     (L1 bypassed, one 32-byte L2 sector each) from table[0, table_len), table_len a
+ *     power of two; size the table to fit L2 (the scan's 4 MB matrix does).
+ *   tspb_microbench_int32: blocks x 256 threads x iters x 128 integer instructions
+ *     (alternating add.s32 / xor.b32 over eight independent chains per thread).
+ * `sink` receives at most one store; it only keeps the work from being optimised away.
+ */
+int tspb_microbench_l2_gather(const int32_t* table, int64_t table_len, int32_t iters, int32_t blocks, int32_t* sink,
+                              void* stream);
+int tspb_microbench_int32(int32_t iters, int32_t blocks, int32_t seed, int32_t* sink, void* stream);
 
 #ifdef __cplusplus
 }

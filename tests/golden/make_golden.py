@@ -55,6 +55,14 @@ maximum_2d = maximum_3d = xray1 = _unavailable
 
 
 def _setup(ref_root: str) -> None:
+  """Import root of a reference checkout (its `src/`), with the stand-in dependency."""
+  setup_import_root(os.path.join(ref_root, "src"))
+
+
+def setup_import_root(src: str) -> None:
+  """Put the reference's packages (a checkout's `src/`, or an installed copy holding
+  `algorithms/`, `protocols/`, ...) and this repository on `sys.path`, after a stand-in
+  for the uninstallable `converter` package."""
   tmp = tempfile.mkdtemp(prefix="golden_stub_")
   pkg = os.path.join(tmp, "converter", "utils")
   os.makedirs(pkg)
@@ -63,7 +71,7 @@ def _setup(ref_root: str) -> None:
   with open(os.path.join(pkg, "cost.py"), "w") as fh:
     fh.write(_STUB)
   sys.path.insert(0, tmp)
-  sys.path.insert(0, os.path.join(ref_root, "src"))
+  sys.path.insert(0, src)
   sys.path.insert(0, REPO)
 
 
@@ -545,7 +553,9 @@ def main_three_opt(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-  root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+  if len(sys.argv) < 2:
+    sys.exit("usage: make_golden.py <reference checkout root> [all|core|ox|stage|dist|three_opt]")
+  root = sys.argv[1]
   part = sys.argv[2] if len(sys.argv) > 2 else "all"
   if part in ("all", "core"):
     main(root)

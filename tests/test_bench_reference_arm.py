@@ -41,3 +41,41 @@ def test_reference_arm_prints_one_contract_line(args):
 def test_reference_arm_other_ranks_exit_quietly():
   assert _run(["--workload", "ga100", "--cpu-gens", "3", "--steps", "1", "--warmup", "3"],
               {"RANK": "1", "WORLD_SIZE": "2"}) == []
+
+
+def test_parity_check_flags_a_planted_difference():
+  """bench.check_parity against the oracle's refinements: equal results pass; one move
+  planted into the oracle's copy of a tour, or a changed pair count, fails the run."""
+  import numpy as np
+
+  sys.path.insert(0, ROOT)
+  import bench
+
+  rng = np.random.default_rng(3)
+  tours = np.stack([rng.permutation(12) for _ in range(5)]).astype(np.int32)
+  stats = np.arange(5 * 4, dtype=np.int64).reshape(5, 4)
+  gpu = {m: (tours.copy(), stats.copy()) for m in bench.MODES}
+  idx = bench.parity_indices(5, 3)
+  assert idx == [0, 2, 4]
+
+  def cpu(plant=None):
+    results = []
+    for i in idx:
+      out = {}
+      for m in bench.MODES:
+        t = tours[i].copy()
+        st = tuple(int(v) for v in stats[i][:3])
+        if plant == ("tour", i, m):
+          t[[1, 2]] = t[[2, 1]]
+        if plant == ("pairs", i, m):
+          st = (st[0], st[1] + 1, st[2])
+        out[m] = (t, st)
+      results.append(out)
+    return {"indices": idx, "results": results}
+
+  ok = bench.check_parity(gpu, cpu())
+  assert ok["ok"] and ok["text"].startswith("bit-exact on 3/5 tours")
+  bad = bench.check_parity(gpu, cpu(("tour", 2, "first")))
+  assert not bad["ok"] and "first tour 2" in bad["mismatches"][0]
+  bad = bench.check_parity(gpu, cpu(("pairs", 4, "best")))
+  assert not bad["ok"] and "best tour 4" in bad["mismatches"][0]

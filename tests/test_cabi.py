@@ -17,7 +17,7 @@ def _declared() -> list[str]:
   for h in sorted(os.listdir(os.path.join(ROOT, "include"))):
     if h.endswith(".h"):
       text = open(os.path.join(ROOT, "include", h)).read()
-      names += re.findall(r"^\s*(?:int|size_t|const char\*)\s+(tspb_\w+)\s*\(", text, flags=re.M)
+      names += re.findall(r"^\s*(?:int|int64_t|size_t|const char\*)\s+(tspb_\w+)\s*\(", text, flags=re.M)
   return names
 
 
@@ -55,6 +55,17 @@ def test_host_argument_checks_run_without_a_gpu(lib):
   assert lib.tspb_two_opt(None, 1, 10, None, 0, None, None, None, None, None, None, 0, 7, 1, 256, None, None, None, 0, None) == 1
   assert lib.tspb_tournament(None, 0, None, 4, 0, None, None) == 1
   assert lib.tspb_stable_rank(None, 4, 5, None, None) == 1
+
+
+def test_watchdog_budget_is_a_runtime_setting(lib):
+  # host-only: the setter returns the previous budget; <= 0 restores the default 2^36 cycles
+  default = 1 << 36
+  assert lib.tspb_set_watchdog_cycles(1000) == default
+  assert lib.tspb_set_watchdog_cycles(5) == 1000
+  assert lib.tspb_set_watchdog_cycles(0) == 5
+  assert lib.tspb_set_watchdog_cycles(-1) == default
+  assert lib.tspb_set_watchdog_cycles(0) == default
+  assert b"memory" in lib.tspb_status_string(8)
 
 
 def test_workspace_sizes(lib):

@@ -288,3 +288,54 @@ def test_first_mode_incremental_restart_matches_full_rescan(b200, k, threads, ma
     want, st = otwo.improve_batch(tours, odist.euc2d_matrix(coords), ctx.get_cpu_candidate_list(k), "first", max_iter)
     assert np.array_equal(outs[1][0], want), n
     assert np.array_equal(outs[1][1][:, :3], st), n
+
+
+@pytest.mark.parametrize("threads", [128, 256])
+@pytest.mark.parametrize("rev", [False, True])
+def test_uncounted_launch_equals_counted_launch_and_oracle(b200, threads, rev):
+  """A launch without a stats buffer runs the scan without first mode's per-row pair-count
+  bookkeeping (and with 16n instead of 20n bytes of shared memory per tour); its tours must
+  equal those of the counted launch and of the oracle, in both modes and table layouts."""
+  import torch
+
+  from tsp_gpu_clean_b200 import native
+  from tsp_gpu_clean_b200.device import operands_for, ptr, stream_handle
+
+  coords = instances.clustered_instance(500, 12, 30.0, 81)
+  n, T = 500, 16
+  tours = instances.random_tours(n, T, 82)
+  ctx = _ctx(b200, coords=coords)
+  ops = operands_for(ctx)
+  dist, stride, _ = ops.distance_args(n, None)
+  D = odist.euc2d_matrix(coords)
+  lib = native.load_library()
+  for k in (20, 7):  # grouped (k % 4 == 0) and plain packed words
+    tabs = ops.candidates(k, ctx.get_cpu_candidate_list(k), n, None)
+    for mode in ("best", "first"):
+      outs = []
+      for counted in (True, False):
+        work = torch.from_numpy(tours).cuda()
+        stats = torch.zeros((T, 4), dtype=torch.int64, device="cuda") if counted else None
+        status = torch.zeros(T, dtype=torch.int32, device="cuda")
+        use_rev = rev and mode == "first"
+        rc = lib.tspb_two_opt(ptr(work), T, n, ptr(dist), stride, None, ptr(tabs.cand), ptr(tabs.cand_dist),
+                              ptr(tabs.rev_off) if use_rev else None, ptr(tabs.rev_idx) if use_rev else None,
+                              ptr(tabs.packed), tabs.k, native.MODE_CODES[mode], 10**9, threads, ptr(stats),
+                              ptr(status), None, 0, stream_handle())
+        native.check("tspb_two_opt", rc)
+        assert int(status.max().item()) == 0
+        outs.append(work.cpu().numpy())
+      want, _ = otwo.improve_batch(tours, D, ctx.get_cpu_candidate_list(k), mode, 10**9)
+      assert np.array_equal(outs[0], want), (k, mode)
+      assert np.array_equal(outs[1], want), (k, mode)
+
+
+def test_public_call_without_stats_equals_golden_c2(b200, golden):
+  data = golden("two_opt_c2.npz")
+  ctx = _ctx(b200, coords=data["coords"], cand=data["cand20"], k=20)
+  for mode in ("best", "first"):
+    ls = b200[2](max_iterations=10**9, mode=mode, candidate_k=20, threads_per_block=128)
+    ls.collect_stats = False
+    got = ls.improve_batch(data["tours_in"], ctx)
+    assert ls.last_stats is None
+    assert np.array_equal(got, data[f"{mode}_out"])

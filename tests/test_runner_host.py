@@ -14,7 +14,10 @@ import pytest
 
 REPO = Path(__file__).resolve().parents[1]
 CONFIG = REPO / "tsp_gpu_clean_b200" / "configs" / "algorithms.b200.json"
-REFERENCE = os.environ.get("TSPB_REFERENCE", "/root/reference")
+sys.path.insert(0, str(Path(__file__).resolve().parent))
+from reference_env import import_root  # noqa: E402
+
+REFERENCE_SRC = import_root()  # a checkout's src/ (TSPB_REFERENCE) or the install under baseline/_ref
 
 
 def test_config_instantiates_every_variant():
@@ -76,7 +79,7 @@ def test_fused_algorithm_takes_the_monolithic_keywords():
   assert "optimal_cost" in evolve and "patience" in evolve
 
 
-@pytest.mark.skipif(not os.path.isdir(os.path.join(REFERENCE, "src")), reason="reference checkout not present")
+@pytest.mark.skipif(REFERENCE_SRC is None, reason="reference not present (set TSPB_REFERENCE)")
 def test_reference_config_models_instantiate_the_b200_config():
   """The reference's `AlgorithmConfig.instantiate` builds its own GeneticAlgorithm wired with
   the B200 strategies (file-path specs through `plugin.py`, protocol contracts checked) and
@@ -88,10 +91,10 @@ def test_reference_config_models_instantiate_the_b200_config():
     from pathlib import Path
     sys.path.insert(0, {str(REPO / "tests" / "golden")!r})
     import make_golden
-    make_golden._setup({REFERENCE!r})
+    make_golden.setup_import_root({REFERENCE_SRC!r})
     for pkg, sub in (("benchmarking", "benchmarking"), ("benchmarking.runner", "benchmarking/runner")):
       m = types.ModuleType(pkg)
-      m.__path__ = [str(Path({REFERENCE!r}) / "src" / sub)]
+      m.__path__ = [str(Path({REFERENCE_SRC!r}) / sub)]
       sys.modules[pkg] = m
     from benchmarking.runner.config_models import AlgorithmConfig, GAParams
     path = Path({str(CONFIG)!r})

@@ -12,7 +12,9 @@ from oracle import distances as odist
 from tsp_gpu_clean_b200 import tsplib
 from tsp_gpu_clean_b200.problem import ProblemContext
 
-REFERENCE = os.environ.get("TSPB_REFERENCE", "/root/reference")
+from reference_env import checkout_root  # noqa: E402
+
+REFERENCE = checkout_root() or ""  # the fixture files live only in a checkout (TSPB_REFERENCE)
 
 
 def _layout_values(d: np.ndarray, fmt: str) -> list[int]:
@@ -86,7 +88,7 @@ def test_tours_and_errors():
     tsplib.problem_from_text(_explicit_text(np.zeros((3, 3), np.int32), "UPPER_ROW").replace("UPPER_ROW", "SPIRAL"))
 
 
-@pytest.mark.skipif(not os.path.isdir(os.path.join(REFERENCE, "tests", "fixtures", "tsp")),
+@pytest.mark.skipif(not REFERENCE or not os.path.isdir(os.path.join(REFERENCE, "tests", "fixtures", "tsp")),
                     reason="reference checkout not present")
 def test_reference_fixture_instances_parse():
   """The TSPLIB files of the reference's own test fixtures (EUC_2D, ATT, GEO, and EXPLICIT

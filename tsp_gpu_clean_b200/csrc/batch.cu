@@ -298,7 +298,7 @@ __global__ void batch_pause_kernel(const tspb_batch B) {
 template <int MODE, int THREADS, int U, bool COORDS, int LAYOUT, bool REV = false>
 __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value)
     batch_two_opt_kernel(const tspb_batch B, const int32_t* __restrict__ items, int num_items, int rows, int phase,
-                         long long max_iter, int max_n, unsigned* __restrict__ queue) {
+                         long long max_iter, int max_n, unsigned* __restrict__ queue, long long budget) {
   extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ ScanSmem S;
   __shared__ unsigned s_unit;
@@ -355,6 +355,7 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value)
     T.converged = clean;
     T.rev_off = REV ? I.rev_off : nullptr;
     T.rev_idx = REV ? I.rev_idx : nullptr;
+    T.budget = budget;
     // the refined row's fitness (fit, or off_fit for children); POSTINIT leaves fitness
     // to tspb_batch_init (the tuner's probes refine scratch rows there)
     T.cost = phase == TSPB_BATCH_PHASE_POSTINIT
@@ -447,7 +448,7 @@ static int batch_two_opt_launch(const tspb_batch& b, const int32_t* items, int n
                                 cudaStream_t st) {
   const bool coords = flags & TSPB_BATCH_COORDS, grouped = flags & TSPB_BATCH_GROUPED;
   const bool rev = flags & TSPB_BATCH_INCREMENTAL;
-  using Kern = void (*)(const tspb_batch, const int32_t*, int, int, int, long long, int, unsigned*);
+  using Kern = void (*)(const tspb_batch, const int32_t*, int, int, int, long long, int, unsigned*, long long);
   Kern kern = coords ? (grouped ? batch_two_opt_kernel<MODE, THREADS, U, true, SCAN_GROUPED>
                                 : batch_two_opt_kernel<MODE, THREADS, U, true, SCAN_PACKED>)
                      : (grouped ? batch_two_opt_kernel<MODE, THREADS, U, false, SCAN_GROUPED>
@@ -476,7 +477,7 @@ static int batch_two_opt_launch(const tspb_batch& b, const int32_t* items, int n
   const int pct = carveout_for(per_sm_used < per_sm ? per_sm_used : per_sm, smem);
   if (pct > 0) TSPB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
   TSPB_CUDA_CHECK(cudaMemsetAsync(queue, 0, sizeof(unsigned), st));
-  kern<<<(int)grid, THREADS, smem, st>>>(b, items, num_items, rows, phase, max_iter, max_n, queue);
+  kern<<<(int)grid, THREADS, smem, st>>>(b, items, num_items, rows, phase, max_iter, max_n, queue, watchdog_cycles());
   return tspb_launch_status();
 }
 

@@ -476,6 +476,7 @@ extern "C" const char* tspb_status_string(int status) {
     case TSPB_ERR_UNSUPPORTED: return "unsupported configuration";
     case TSPB_ERR_WORKSPACE: return "workspace too small";
     case TSPB_ERR_BUDGET: return "device watchdog expired before convergence";
+    case TSPB_ERR_DEVICE_MEMORY: return "the device could not provide memory held by the library";
     default: return "unknown status";
   }
 }

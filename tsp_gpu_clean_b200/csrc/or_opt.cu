@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(THREADS) or_opt_kernel(int32_t* __restrict__ t
                                                          const int32_t* __restrict__ cdist,
                                                          const uint32_t* __restrict__ packed, int k, int S,
                                                          long long max_iter, int32_t* __restrict__ status,
-                                                         long long* __restrict__ stats) {
+                                                         long long* __restrict__ stats, long long budget) {
   extern __shared__ __align__(16) int sm[];
   __shared__ OrMove red[33];
   __shared__ long long redll[32];
@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(THREADS) or_opt_kernel(int32_t* __restrict__ t
     const long long t0 = clock64();
     while (passes < max_iter) {
       __syncthreads();  // the state of the last move (or the setup) is visible
-      if (tid == 0) s_flag = clock64() - t0 > BUDGET_CYCLES;
+      if (tid == 0) s_flag = clock64() - t0 > budget;
       __syncthreads();
       if (s_flag) {
         err = TSPB_ERR_BUDGET;
@@ -253,7 +253,8 @@ static int launch_or_opt(int32_t* tours, int num, int n, const DistSrc& ds, cons
   TSPB_CUDA_CHECK(cudaGetDevice(&dev));
   TSPB_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const long long grid = (long long)per_sm * sms < num ? (long long)per_sm * sms : num;
-  kern<<<(int)grid, THREADS, smem, st>>>(tours, num, n, ds, cand, cdist, packed, k, S, max_iter, status, stats);
+  kern<<<(int)grid, THREADS, smem, st>>>(tours, num, n, ds, cand, cdist, packed, k, S, max_iter, status, stats,
+                                         watchdog_cycles());
   return tspb_launch_status();
 }
 

@@ -64,7 +64,8 @@ __device__ __forceinline__ void reverse_segment(int* tour, int lo, int hi) {
 template <bool SMEM_M>
 __global__ void __launch_bounds__(512) three_opt_kernel(int32_t* __restrict__ tours, int num_tours, int n, DistSrc ds,
                                                         long long max_iter, int32_t* __restrict__ workspace,
-                                                        int32_t* __restrict__ status, long long* __restrict__ stats) {
+                                                        int32_t* __restrict__ status, long long* __restrict__ stats,
+                                                        long long budget) {
   extern __shared__ __align__(16) int sm3[];
   int* tour = sm3;                                      // n
   long long* edge = reinterpret_cast<long long*>(sm3 + ((n + 1) & ~1));  // n int64
@@ -83,7 +84,7 @@ __global__ void __launch_bounds__(512) three_opt_kernel(int32_t* __restrict__ to
     int code = 0;
     const long long start = clock64();
     for (long long it = 0; it < max_iter && n >= 4; ++it) {
-      if (clock64() - start > BUDGET_CYCLES) {  // the watchdog of the 2-opt kernels (uniform per CTA)
+      if (clock64() - start > budget) {  // the watchdog of the 2-opt kernels (uniform per CTA)
         code = TSPB_ERR_BUDGET;
         break;
       }
@@ -225,12 +226,12 @@ extern "C" int tspb_three_opt(int32_t* tours, int32_t num_tours, int32_t n, cons
   if (smem_m) {
     TSPB_CUDA_CHECK(cudaFuncSetAttribute(three_opt_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     three_opt_kernel<true><<<ctas, threads, smem, st>>>(tours, num_tours, n, ds, max_iterations, nullptr, status,
-                                                        reinterpret_cast<long long*>(stats));
+                                                        reinterpret_cast<long long*>(stats), watchdog_cycles());
   } else {
     if (smem > 48 * 1024)
       TSPB_CUDA_CHECK(cudaFuncSetAttribute(three_opt_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     three_opt_kernel<false><<<ctas, threads, smem, st>>>(tours, num_tours, n, ds, max_iterations, workspace, status,
-                                                         reinterpret_cast<long long*>(stats));
+                                                         reinterpret_cast<long long*>(stats), watchdog_cycles());
   }
   return tspb_launch_status();
 }

@@ -20,6 +20,7 @@
 // is rebuilt from FP64 coordinates). multi_move sorts its improving moves in a global
 // workspace slice per tour.
 #include <algorithm>
+#include <atomic>
 
 #include "two_opt.cuh"
 
@@ -106,7 +107,7 @@ __global__ void __launch_bounds__(1024) two_opt_kernel(const TwoOptArgs A) {
   if (tid == 0) S.stop = 0;
 
   while (passes < A.max_iter) {
-    if (tid == 0 && clock64() - t_start > BUDGET_CYCLES) S.stop = TSPB_ERR_BUDGET;
+    if (tid == 0 && clock64() - t_start > A.budget) S.stop = TSPB_ERR_BUDGET;
     __syncthreads();
     if (S.stop) {
       err = S.stop;
@@ -390,16 +391,28 @@ __global__ void __launch_bounds__(1024) two_opt_kernel(const TwoOptArgs A) {
   }
 }
 
+static std::atomic<long long> g_watchdog_cycles{BUDGET_CYCLES};
+
+long long watchdog_cycles() { return g_watchdog_cycles.load(std::memory_order_relaxed); }
+
+// Opt-in shared memory per block of the current device, cached per device index (a
+// process may drive GPUs of different models).
 int smem_optin() {
-  static int cached = -1;
-  if (cached < 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
+  constexpr int MAX_DEV = 64;
+  static std::atomic<int> cached[MAX_DEV];  // 0: not yet queried
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return 0;
+  if (dev >= MAX_DEV) {
     int v = 0;
     cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    cached = v;
+    return v;
   }
-  return cached;
+  int v = cached[dev].load(std::memory_order_relaxed);
+  if (v == 0) {
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cached[dev].store(v, std::memory_order_relaxed);
+  }
+  return v;
 }
 
 struct Layout {
@@ -514,6 +527,7 @@ static int two_opt_impl(int32_t* tours, int32_t num_tours, int32_t n, const int3
     c.ws_tour_bytes = per;
     c.arrays_in_smem = per == 0 ? 1 : 0;
     c.skip = skip;
+    c.budget = watchdog_cycles();
     if (has_rev && mode == TSPB_MODE_FIRST) {  // incremental restart of first mode
       c.rev_off = rev_off;
       c.rev_idx = rev_idx;
@@ -544,6 +558,7 @@ static int two_opt_impl(int32_t* tours, int32_t num_tours, int32_t n, const int3
     c.rev_off = rev_off;
     c.rev_idx = rev_idx;
     c.skip = skip;
+    c.budget = watchdog_cycles();
     return launch_two_opt_cached(c, mode, threads, st);
   }
   const Layout L = two_opt_layout(n, use_cand ? k : 0, mode, use_cand);
@@ -568,6 +583,7 @@ static int two_opt_impl(int32_t* tours, int32_t num_tours, int32_t n, const int3
   a.ws_keys_off = L.ws_keys_off;
   a.arrays_in_smem = L.arrays_in_smem ? 1 : 0;
   a.skip = skip;
+  a.budget = watchdog_cycles();
   if (use_cand) {
     switch (mode) {
       case TSPB_MODE_BEST: return launch<TSPB_MODE_BEST, true>(a, threads, L.smem_bytes, st);
@@ -580,6 +596,10 @@ static int two_opt_impl(int32_t* tours, int32_t num_tours, int32_t n, const int3
     case TSPB_MODE_FIRST: return launch<TSPB_MODE_FIRST, false>(a, threads, L.smem_bytes, st);
     default: return launch<TSPB_MODE_MULTI_MOVE, false>(a, threads, L.smem_bytes, st);
   }
+}
+
+extern "C" int64_t tspb_set_watchdog_cycles(int64_t cycles) {
+  return g_watchdog_cycles.exchange(cycles > 0 ? (long long)cycles : BUDGET_CYCLES);
 }
 
 extern "C" int tspb_two_opt(int32_t* tours, int32_t num_tours, int32_t n, const int32_t* dist, int64_t dist_stride,

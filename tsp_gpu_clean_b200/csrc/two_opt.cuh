@@ -24,6 +24,7 @@ struct TwoOptArgs {
   const int32_t* rev_idx;  // cached kernel: flat entries a * k + r grouped by candidate node
   const uint32_t* cand_packed;  // scan kernel: c | d(a, c) << 16 per entry (optional)
   const int32_t* skip;          // optional device flag: non-zero makes the launch a no-op
+  long long budget;             // watchdog: SM cycles a tour may run (watchdog_cycles())
 };
 
 // Order-preserving u64 key: negative int32 gain in the high word, scan index low.
@@ -38,8 +39,10 @@ constexpr unsigned long long NO_KEY = ~0ull;
 constexpr unsigned NO_IDX = ~0u;
 
 // Watchdog: a tour that has not converged after this many SM cycles (about 35 s at
-// 1.9 GHz) ends with TSPB_ERR_BUDGET instead of running on.
+// 1.9 GHz) ends with TSPB_ERR_BUDGET instead of running on. This is the default;
+// tspb_set_watchdog_cycles changes the budget that later launches are given.
 constexpr long long BUDGET_CYCLES = 1LL << 36;
+long long watchdog_cycles();
 
 int smem_optin();
 size_t align256(size_t v);

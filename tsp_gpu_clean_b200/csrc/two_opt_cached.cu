@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(THREADS, MinBlocks<THREADS>::value) two_opt_ca
   int err = TSPB_OK;
   const long long t_start = clock64();
   while (passes < A.max_iter) {
-    if (tid == 0 && clock64() - t_start > BUDGET_CYCLES) S.stop = TSPB_ERR_BUDGET;
+    if (tid == 0 && clock64() - t_start > A.budget) S.stop = TSPB_ERR_BUDGET;
     __syncthreads();
     if (S.stop) {
       err = S.stop;

@@ -12,7 +12,8 @@ namespace tspb {
 
 // SMEM: the tour state lives in shared memory (the compiler then addresses it with
 // shared-memory instructions); otherwise in the per-tour global workspace slice.
-template <int MODE, int THREADS, int U, int LAYOUT, bool SMEM>
+// COUNT: first mode keeps the reference's pair count (launched when stats are requested).
+template <int MODE, int THREADS, int U, int LAYOUT, bool SMEM, bool COUNT>
 __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value) two_opt_scan_kernel(const TwoOptArgs A) {
   extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ ScanSmem S;
@@ -36,21 +37,28 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value) two_op
   T.converged = nullptr;
   T.rev_off = A.rev_off;
   T.rev_idx = A.rev_idx;
-  scan_tour<MODE, THREADS, U, LAYOUT>(T, S);
+  T.budget = A.budget;
+  scan_tour<MODE, THREADS, U, LAYOUT, false, COUNT>(T, S);
 }
 
 size_t two_opt_scan_tour_bytes(int n, int mode) { return scan_tour_state_bytes(n, mode); }
 
+// First mode without stats needs no per-row counts: 16n bytes instead of 20n.
+static bool scan_counts(const TwoOptArgs& a, int mode) { return mode == TSPB_MODE_FIRST && a.stats != nullptr; }
+
 // Shared-memory carveout (percent of the unified L1/shared array) that holds exactly
 // `ctas_per_sm` CTAs of `smem_per_cta` dynamic bytes; the rest stays L1 for the k-NN
 // tables. The default lets the driver take the largest split, which leaves too little L1.
+// An attribute of the current device (queried on every call: a process may drive GPUs of
+// different models, and the query is cheap next to a launch).
+static int current_device_attr(cudaDeviceAttr attr) {
+  int dev = 0, v = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&v, attr, dev) != cudaSuccess) return 0;
+  return v;
+}
+
 int carveout_for(int ctas_per_sm, size_t smem_per_cta) {
-  static int smem_sm = 0;
-  if (smem_sm == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-  }
+  const int smem_sm = current_device_attr(cudaDevAttrMaxSharedMemoryPerMultiprocessor);
   if (smem_sm <= 0 || ctas_per_sm <= 0) return -1;
   const long long need = (long long)ctas_per_sm * (long long)(smem_per_cta + sizeof(ScanSmem) + 1024);
   int pct = (int)((need * 100 + smem_sm - 1) / smem_sm);
@@ -58,12 +66,7 @@ int carveout_for(int ctas_per_sm, size_t smem_per_cta) {
 }
 
 static int carveout_percent(int num_tours, size_t smem_per_cta, int max_ctas_per_sm) {
-  static int sms = 0;
-  if (sms == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  }
+  const int sms = current_device_attr(cudaDevAttrMultiProcessorCount);
   if (sms <= 0) return -1;
   int per_sm = (num_tours + sms - 1) / sms;
   if (per_sm > max_ctas_per_sm) per_sm = max_ctas_per_sm;
@@ -75,13 +78,18 @@ static int launch_scan(const TwoOptArgs& a, size_t smem, cudaStream_t st) {
   // the grouped layout loads U packed words at once: k % U == 0 and a U*4-byte aligned table
   const bool aligned = (reinterpret_cast<uintptr_t>(a.cand_packed) % (U * sizeof(uint32_t))) == 0;
   const int layout = a.cand_packed ? (a.k % U == 0 && aligned ? SCAN_GROUPED : SCAN_PACKED) : SCAN_PLAIN;
-  auto pick = [&](auto smem_tag) {
+  // best mode has no per-row counts: one instance serves both
+  constexpr bool CAN_SKIP = MODE == TSPB_MODE_FIRST;
+  auto pick = [&](auto smem_tag, auto count_tag) {
     constexpr bool SM = decltype(smem_tag)::value;
-    return layout == SCAN_GROUPED  ? two_opt_scan_kernel<MODE, THREADS, U, SCAN_GROUPED, SM>
-           : layout == SCAN_PACKED ? two_opt_scan_kernel<MODE, THREADS, U, SCAN_PACKED, SM>
-                                   : two_opt_scan_kernel<MODE, THREADS, U, SCAN_PLAIN, SM>;
+    constexpr bool CT = decltype(count_tag)::value || !CAN_SKIP;
+    return layout == SCAN_GROUPED  ? two_opt_scan_kernel<MODE, THREADS, U, SCAN_GROUPED, SM, CT>
+           : layout == SCAN_PACKED ? two_opt_scan_kernel<MODE, THREADS, U, SCAN_PACKED, SM, CT>
+                                   : two_opt_scan_kernel<MODE, THREADS, U, SCAN_PLAIN, SM, CT>;
   };
-  auto kern = a.arrays_in_smem ? pick(std::true_type{}) : pick(std::false_type{});
+  const bool count = scan_counts(a, MODE);
+  auto kern = a.arrays_in_smem ? (count ? pick(std::true_type{}, std::true_type{}) : pick(std::true_type{}, std::false_type{}))
+                               : (count ? pick(std::false_type{}, std::true_type{}) : pick(std::false_type{}, std::false_type{}));
   if (smem > 48 * 1024) TSPB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int pct = carveout_percent(a.num_tours, smem, ScanMinBlocks<THREADS>::value);
   if (pct > 0) TSPB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
@@ -103,7 +111,7 @@ static int launch_scan_mode(const TwoOptArgs& a, int threads, size_t smem, cudaS
 }
 
 int launch_two_opt_scan(const TwoOptArgs& a, int mode, int threads, cudaStream_t st) {
-  const size_t smem = a.arrays_in_smem ? two_opt_scan_tour_bytes(a.n, mode) : 0;
+  const size_t smem = a.arrays_in_smem ? scan_tour_state_bytes(a.n, mode, false, scan_counts(a, mode)) : 0;
   if (mode == TSPB_MODE_BEST) return launch_scan_mode<TSPB_MODE_BEST>(a, threads, smem, st);
   return launch_scan_mode<TSPB_MODE_FIRST>(a, threads, smem, st);
 }

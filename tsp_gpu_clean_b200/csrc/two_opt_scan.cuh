@@ -54,10 +54,11 @@ struct ScanMinBlocks {
   static constexpr int value = THREADS == 64 ? 16 : THREADS == 128 ? 8 : THREADS == 256 ? 4 : THREADS == 512 ? 2 : 1;
 };
 
-// Bytes of tour state per tour: tour, pos, succ, eout (+ per-row valid counts for first;
-// best with incremental row keys adds the keys, valid counts and a row list).
-__host__ __device__ inline size_t scan_tour_state_bytes(int n, int mode, bool incremental = false) {
-  if (mode == TSPB_MODE_FIRST) return (size_t)20 * (size_t)n;
+// Bytes of tour state per tour: tour, pos, succ, eout (+ per-row valid counts for first
+// when it counts pairs; best with incremental row keys adds the keys, valid counts and a
+// row list).
+__host__ __device__ inline size_t scan_tour_state_bytes(int n, int mode, bool incremental = false, bool count = true) {
+  if (mode == TSPB_MODE_FIRST) return (size_t)(count ? 20 : 16) * (size_t)n;
   return (size_t)(incremental ? 30 : 16) * (size_t)n;
 }
 
@@ -80,6 +81,7 @@ struct ScanTour {
   const int32_t* rev_off = nullptr;  // optional (first mode): CSR reverse k-NN index, n + 1 offsets
   const int32_t* rev_idx = nullptr;  // flat entries a * k + r grouped by candidate node
   double* cost = nullptr;  // optional: the refined tour's length (exact int64 sum of eout, as float64)
+  long long budget = BUDGET_CYCLES;  // watchdog: SM cycles before the tour ends with TSPB_ERR_BUDGET
 };
 
 // k-NN table layouts of scan_tour: plain int32 candidates (+ optional distances), packed
@@ -107,7 +109,13 @@ __device__ __forceinline__ void load_words(const uint32_t* p, uint32_t (&w)[U]) 
 }
 
 // Refines one tour with the whole CTA. Every thread of the CTA must call it.
-template <int MODE, int THREADS, int U, int LAYOUT, bool INC = false>
+//
+// COUNT: first mode (and incremental best) keeps every row's valid-pair count so that
+// stats[1] holds the reference's pair count. No decision of the scan reads these counts,
+// and refreshing them after a move visits every candidate of every row in the reversed
+// window, so a caller that passes no stats runs the COUNT = false instance (or, with
+// COUNT = true, skips the refresh at run time): same moves, same tours.
+template <int MODE, int THREADS, int U, int LAYOUT, bool INC = false, bool COUNT = true>
 __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
   constexpr bool PACKED = LAYOUT != SCAN_PLAIN;
   constexpr bool GROUPED = LAYOUT == SCAN_GROUPED;
@@ -124,7 +132,8 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
   unsigned long long* rkey = reinterpret_cast<unsigned long long*>(eout + n);
   int* rcnt = inc_best ? reinterpret_cast<int*>(rkey + n) : eout + n;  // valid entries per row (position)
   uint16_t* rlist = reinterpret_cast<uint16_t*>(rcnt + n);
-  constexpr bool track_rows = MODE == TSPB_MODE_FIRST || inc_best;
+  constexpr bool track_rows_ct = COUNT && (MODE == TSPB_MODE_FIRST || inc_best);
+  const bool track_rows = track_rows_ct && T.stats != nullptr;
   const DistSrc ds = T.ds;
   const uint32_t* __restrict__ packed = T.packed;
   const int32_t* __restrict__ cand = T.cand;
@@ -215,7 +224,7 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
 
   while (passes < T.max_iter) {
     if (tid == 0) {
-      if (clock64() - t_start > BUDGET_CYCLES) S.stop = TSPB_ERR_BUDGET;
+      if (clock64() - t_start > T.budget) S.stop = TSPB_ERR_BUDGET;
       S.first = NO_IDX;
     }
     __syncthreads();

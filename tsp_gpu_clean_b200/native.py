@@ -11,7 +11,7 @@ import ctypes
 import os
 import threading
 
-from .errors import GPUUnavailableError, KernelError, NotPermutationError
+from .errors import GPUUnavailableError, KernelError, NotPermutationError, VRAMInsufficientError
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "libtspb.so")
@@ -24,6 +24,7 @@ TSPB_ERR_RANGE = 4
 TSPB_ERR_UNSUPPORTED = 5
 TSPB_ERR_WORKSPACE = 6
 TSPB_ERR_BUDGET = 7
+TSPB_ERR_DEVICE_MEMORY = 8
 
 MODE_CODES = {"best": 0, "batch": 0, "first": 1, "multi_move": 2}
 
@@ -37,6 +38,9 @@ _f64 = ctypes.c_double
 SIGNATURES: dict[str, tuple] = {
   "tspb_version": (ctypes.c_int, []),
   "tspb_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+  "tspb_set_watchdog_cycles": (_i64, [_i64]),
+  "tspb_microbench_l2_gather": (ctypes.c_int, [_p, _i64, _i32, _i32, _p, _p]),
+  "tspb_microbench_int32": (ctypes.c_int, [_i32, _i32, _i32, _p, _p]),
   "tspb_two_opt_workspace_bytes": (_sz, [_i32, _i32, _i32, _i32, _i32]),
   "tspb_two_opt": (ctypes.c_int, [_p, _i32, _i32, _p, _i64, _p, _p, _p, _p, _p, _p, _i32, _i32, _i64, _i32, _p, _p, _p, _sz, _p]),
   "tspb_two_opt_gated": (ctypes.c_int, [_p, _p, _i32, _i32, _p, _i64, _p, _p, _p, _p, _p, _p, _i32, _i32, _i64, _i32, _p,
@@ -192,6 +196,8 @@ def check(func: str, code: int) -> None:
     raise NotPermutationError(f"{func}: {status_text(code)}")
   if code == TSPB_ERR_ARG:
     raise ValueError(f"{func}: {status_text(code)}")
+  if code == TSPB_ERR_DEVICE_MEMORY:
+    raise VRAMInsufficientError(f"{func}: {status_text(code)}")
   raise KernelError(func, code, status_text(code))
 
 
