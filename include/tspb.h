@@ -301,6 +301,29 @@ int tspb_three_opt(int32_t* tours, int32_t num_tours, int32_t n, const int32_t* 
 int tspb_three_opt_workspace_bytes(int32_t n, int32_t ctas, size_t* bytes);
 
 /*
+ * 3-opt with the rules of the reference's grid kernels, for the two parts of its 3-opt
+ * that only its CUDA kernels define (benchmark_scripts/experiments-and-examples/
+ * experiment-comparing-3opt-and-2opt/kernels/three_opt_common.cuh:155-447,
+ * three_opt_batch.cu, three_opt_multi_move.cu; driven by LocalSearchGPUThreeOpt._improve_grid,
+ * gpu_three_opt.py:452-537):
+ *   - k > 0: the candidate-pruned scan (cand: n x k sorted k-NN table, cand_dist its
+ *     distances; inner_k <= 0 means k), one move per pass (multi_move = 0) or multi_move;
+ *   - k == 0: the exhaustive scan, multi_move only (one-move exhaustive passes are
+ *     tspb_three_opt, which follows the reference's CPU 3-opt).
+ * The moves are those of the reference's kernel launched with
+ * tspb_three_opt_grid_threads(threads_per_block, n) threads per tour (its
+ * prev_power_of_2(min(threads_per_block, n)) clamped to 256). Open (cyclic TSP) tours of
+ * every city, in place; up to max_iterations passes, stopping after a pass that applies
+ * nothing. stats (optional, num_tours x 3): passes, moves applied, candidate moves
+ * evaluated. Exhaustive n <= 4095; candidate n up to what 20 n bytes of shared memory hold.
+ */
+int tspb_three_opt_grid(int32_t* tours, int32_t num_tours, int32_t n, const int32_t* dist, int64_t dist_stride,
+                        const double* coords, const int32_t* cand, const int32_t* cand_dist, int32_t k,
+                        int32_t inner_k, int32_t multi_move, int32_t threads_per_block, int64_t max_iterations,
+                        int32_t* status, int64_t* stats, void* stream);
+int tspb_three_opt_grid_threads(int32_t threads_per_block, int32_t n);
+
+/*
  * Candidate-list Or-opt of open (cyclic TSP) tours in place, best improvement, up to
  * max_iterations passes each. No reference counterpart (the reference's local search has
  * 2-opt and an experimental 3-opt); it widens the family with the reference's candidate

@@ -12,7 +12,10 @@ baseline. The product package `tsp_gpu_clean_b200` never imports it; its GPU
 path fails loudly when the CUDA library is missing.
 
 Pinning: the oracle is checked against golden vectors produced by running the
-reference itself (`tests/golden/make_golden.py`, committed with its outputs)
-and against the reference's own scalar 2-opt rules (restated in
-`tests/test_oracle_scalar_rules.py`).
+reference itself (`tests/golden/make_golden.py`, committed with its outputs; the
+checks are `tests/test_oracle_golden.py`). `three_opt_kernel.py` restates two
+parts of the reference's 3-opt that exist only as CUDA kernels; it is pinned to
+outputs of those kernels, compiled from the reference's sources by
+`oracle/build_ref.py` and run by `tests/golden/make_three_opt_kernel_golden.py`.
+Or-opt has no reference counterpart (`or_opt.py` pins itself two ways).
 """

@@ -77,10 +77,6 @@ def test_three_opt_rejects_what_it_does_not_cover(torch_mod):
   c = instances.uniform_instance(12, 1)
   ctx = _ctx(c)
   t = instances.random_tours(12, 2, 3)
-  with pytest.raises(NotImplementedError):
-    LocalSearchB200ThreeOpt(mode="multi_move").improve_batch(t, ctx)
-  with pytest.raises(NotImplementedError):
-    LocalSearchB200ThreeOpt(candidate_k=5).improve_batch(t, ctx)
   bad = t.copy()
   bad[1, 3] = bad[1, 4]
   with pytest.raises(NotPermutationError):

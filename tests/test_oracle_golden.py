@@ -257,3 +257,42 @@ def test_three_opt_matches_reference(golden, tag):
   for iters in (1, 3, 1000):
     got, _ = three_opt.improve_batch(g[f"{tag}_tours"], D, iters)
     assert np.array_equal(got, g[f"{tag}_refined{iters}"]), iters
+
+
+@pytest.mark.parametrize("tag", THREE_OPT_TAGS)
+def test_three_opt_kernel_rules_with_one_thread_equal_the_cpu_three_opt(golden, tag):
+  """With one thread per tour the reference's grid kernels scan every anchor in the CPU
+  3-opt's order and keep the first strictly smallest move, and multi_move applies at most
+  min(1, n // 2) = 1 move per pass: the kernel restatement must then give the reference's
+  CPU 3-opt refinements (which `three_opt.npz` records)."""
+  from oracle import three_opt_kernel as tk
+
+  g = golden("three_opt.npz")
+  D = _three_opt_matrix(g[f"{tag}_coords"])
+  for iters in (1, 3, 1000):
+    for t, want in zip(g[f"{tag}_tours"], g[f"{tag}_refined{iters}"]):
+      for mode in ("batch", "multi_move"):
+        got, _ = tk.refine(t, D, None, 0, 1, mode, iters)
+        assert np.array_equal(got, want), (tag, iters, mode)
+
+
+def test_three_opt_kernel_rules_match_reference_kernels(golden):
+  """The restatement against outputs of the reference's own 3-opt CUDA kernels
+  (`three_opt_kernel.npz`, recorded by make_three_opt_kernel_golden.py)."""
+  import os
+
+  from conftest import GOLDEN
+  from oracle import three_opt_kernel as tk
+
+  if not os.path.exists(os.path.join(GOLDEN, "three_opt_kernel.npz")):
+    pytest.skip("three_opt_kernel.npz not recorded yet")
+  g = golden("three_opt_kernel.npz")
+  for tag in g["tags"]:
+    n, k, inner, tpb, multi, iters, B = (int(v) for v in g[f"{tag}_meta"])
+    assert tk.virtual_threads(tpb, n) == B
+    D = distances.euc2d_matrix(g[f"{tag}_coords"])
+    cand = g[f"{tag}_cand"] if k > 0 else None
+    mode = "multi_move" if multi else "batch"
+    for t, want in zip(g[f"{tag}_in"], g[f"{tag}_out"]):
+      got, _ = tk.refine(t, D, cand, inner, tpb, mode, iters)
+      assert np.array_equal(got, want), str(tag)

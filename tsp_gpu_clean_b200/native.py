@@ -39,6 +39,8 @@ SIGNATURES: dict[str, tuple] = {
   "tspb_version": (ctypes.c_int, []),
   "tspb_status_string": (ctypes.c_char_p, [ctypes.c_int]),
   "tspb_set_watchdog_cycles": (_i64, [_i64]),
+  "tspb_three_opt_grid": (ctypes.c_int, [_p, _i32, _i32, _p, _i64, _p, _p, _p, _i32, _i32, _i32, _i32, _i64, _p, _p, _p]),
+  "tspb_three_opt_grid_threads": (ctypes.c_int, [_i32, _i32]),
   "tspb_microbench_l2_gather": (ctypes.c_int, [_p, _i64, _i32, _i32, _p, _p]),
   "tspb_microbench_int32": (ctypes.c_int, [_i32, _i32, _i32, _p, _p]),
   "tspb_two_opt_workspace_bytes": (_sz, [_i32, _i32, _i32, _i32, _i32]),

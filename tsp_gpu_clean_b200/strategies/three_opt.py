@@ -1,13 +1,22 @@
 """B200 3-opt local search (drop-in for the reference's experimental 3-opt strategy).
 
 `LocalSearchB200ThreeOpt` keeps the constructor and call shape of `LocalSearchGPUThreeOpt`
-(`benchmark_scripts/experiments-and-examples/experiment-comparing-3opt-and-2opt/gpu_three_opt.py:280-340`)
-and computes exactly what the reference's CPU 3-opt computes (`cpu_three_opt_refine`,
-`:256-277`): up to `max_iterations` passes, each applying the steepest of all 3-opt moves
-(seven reconnection cases, first in scan order on ties) to every tour. `mode` `"batch"`
-and `"naive"` both name this steepest refinement; the reference's `"multi_move"` and its
-candidate-pruned scan (`candidate_k`) are defined only by its CUDA kernels and are not
-offered here (they raise NotImplementedError). Open cyclic TSP tours only.
+(`benchmark_scripts/experiments-and-examples/experiment-comparing-3opt-and-2opt/gpu_three_opt.py:280-340`):
+
+- exhaustive `"batch"` / `"naive"` (`candidate_k=None`): exactly what the reference's CPU
+  3-opt computes (`cpu_three_opt_refine`, `:256-277`), up to `max_iterations` passes,
+  each applying the steepest of all 3-opt moves (seven reconnection cases, first in scan
+  order on ties);
+- `candidate_k > 0` (any mode) and exhaustive `"multi_move"`: the moves of the
+  reference's grid kernels (`three_opt_batch.cu`, `three_opt_multi_move.cu` with
+  `three_opt_common.cuh`), which alone define these parts: the candidate-pruned scan with
+  `candidate_k` / `inner_candidate_k`, and the greedy disjoint multi_move, both as the
+  reference launches them with `threads_per_block` threads per tour (`_improve_grid`,
+  `:452-537`). Refinement stops after a pass that applies nothing, where the reference's
+  remaining launches change nothing.
+
+Open cyclic TSP tours only (the candidate scan, like the reference's, needs tours of
+every city; otherwise it falls back to the exhaustive scan as `_uses_candidates` does).
 
 Host arrays in, host arrays out; CUDA tensors in, CUDA tensors out. Inputs are never
 modified. No CPU fallback.
@@ -67,13 +76,17 @@ class LocalSearchB200ThreeOpt(StrategyBase):
   def improve(self, route: Any, context: Any) -> Any:
     return self.improve_batch(route, context)
 
+  def _uses_candidates(self, context: Any, n: int) -> bool:
+    """`_uses_candidates` of the reference (`gpu_three_opt.py:367-373`) for open tours."""
+    if self.candidate_k is None or self.candidate_k <= 0:
+      return False
+    if str(context.problem.problem_type) in {"CVRP", "OVRP", "DCVRP"}:
+      return False
+    return n >= int(context.dimension)
+
   @time_strategy
   def improve_batch(self, routes: Any, context: Any) -> Any:
     require_gpu()
-    if self.mode == "multi_move":
-      raise NotImplementedError("multi_move 3-opt is defined only by the reference's CUDA kernel; use mode='batch'")
-    if self.candidate_k is not None and self.candidate_k > 0:
-      raise NotImplementedError("candidate-pruned 3-opt is not provided; use candidate_k=None (exhaustive)")
     batch, was_1d = ensure_routes_batch(routes)
     num, n = int(batch.shape[0]), int(batch.shape[1])
     on_device = not isinstance(batch, np.ndarray)
@@ -101,6 +114,9 @@ class LocalSearchB200ThreeOpt(StrategyBase):
     self.kernel_launches += 1
     if int(bad.max().item()) != 0:
       raise NotPermutationError("improve_batch: a route is not a permutation of 0..n-1")
+    use_cand = self._uses_candidates(context, n)
+    if use_cand or self.mode == "multi_move":
+      return self._improve_grid(d_tours, num, n, dist, stride, coords, use_cand, context, on_device, was_1d)
     threads = 512 if self.threads_per_block >= 512 else (256 if self.threads_per_block >= 256 else 128)
     import ctypes
 
@@ -116,6 +132,34 @@ class LocalSearchB200ThreeOpt(StrategyBase):
     code = int(status.max().item())
     if code != 0:
       raise RuntimeError(f"3-opt kernel reported {native.status_text(code)}")
+    return self._finish(d_tours, stats, on_device, was_1d)
+
+  def _improve_grid(self, d_tours, num, n, dist, stride, coords, use_cand, context, on_device, was_1d):
+    """Candidate-pruned scan or multi_move with the reference's grid-kernel rules."""
+    from ..device import candidate_list
+
+    cand = cand_dist = None
+    k = inner = 0
+    if use_cand:
+      ops = operands_for(context)
+      before = ops.h2d_bytes
+      tabs = ops.candidates(int(self.candidate_k), candidate_list(context, int(self.candidate_k)), n,
+                            self.max_matrix_dimension)
+      self.h2d_bytes += ops.h2d_bytes - before
+      cand, cand_dist, k = tabs.cand, tabs.cand_dist, int(tabs.k)
+      inner = int(self.inner_candidate_k) if self.inner_candidate_k else 0
+    stats = torch.empty((num, 3), dtype=torch.int64, device="cuda")
+    status = torch.empty(num, dtype=torch.int32, device="cuda")
+    native.call("tspb_three_opt_grid", ptr(d_tours), num, n, ptr(dist), stride, ptr(coords), ptr(cand),
+                ptr(cand_dist), k, inner, 1 if self.mode == "multi_move" else 0, int(self.threads_per_block),
+                int(self.max_iterations), ptr(status), ptr(stats), stream_handle())
+    self.kernel_launches += 1
+    code = int(status.max().item())
+    if code != 0:
+      raise RuntimeError(f"3-opt kernel reported {native.status_text(code)}")
+    return self._finish(d_tours, stats, on_device, was_1d)
+
+  def _finish(self, d_tours, stats, on_device, was_1d):
     self.last_stats = stats.cpu().numpy()
     if on_device:
       return restore_shape(d_tours, was_1d)
