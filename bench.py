@@ -520,7 +520,8 @@ def _ga_cpu_sample(name: str, sample_gens: int) -> dict:
 
 
 def ga_measure(workload: str, warmup: int, steps: int, world: int, rank: int, engine: str = "batch", chunk: int = 16,
-               no_graph: bool = False, batch_incremental: str = "off", generations: int | None = None) -> dict:
+               no_graph: bool = False, batch_incremental: str = "off", generations: int | None = None,
+               batch_pair: str = "auto") -> dict:
   """Device and end-to-end generations/s of one GA workload on this rank's GPU (the
   process group, if any, is the caller's)."""
   import torch
@@ -554,7 +555,7 @@ def ga_measure(workload: str, warmup: int, steps: int, world: int, rank: int, en
                                 elite_count=elite, post_init=post_init, max_matrix_dimension=None, tuner=tuner,
                                 chunk=chunk, use_graph=not no_graph, crossover=o["crossover"],
                                 mutation=o["mutation"], init=o["init"], local_search_stage=o["stage"],
-                                incremental=batch_incremental)
+                                incremental=batch_incremental, pair=batch_pair)
       results = solver.evolve(ctxs, G, patience=10**9)
       stats = {"generations_completed": sum(st["generations_completed"] for _, st in results),
                "best_fitness": min(st["best_fitness"] for _, st in results),
@@ -591,7 +592,7 @@ def ga_measure(workload: str, warmup: int, steps: int, world: int, rank: int, en
                   "d2h_bytes_per_step": int(reps * (n * 4 + (G + 1) * 8 + P * n * 4))},
           "gpu_launches": launches, "desc": desc, "best": stats["best_fitness"], "history": stats["history"],
           "loop_ms_steps": [round(v, 3) for v in loop_ms], "walls_s": [round(w, 4) for w in walls],
-          "buckets": [{"n": [b.lo, b.hi], "two_opt_threads": b.two_opt_threads, "incremental": b.incremental,
+          "buckets": [{"n": [b.lo, b.hi], "two_opt_threads": b.two_opt_threads, "incremental": b.incremental, "pair": b.pair,
                        "offspring_threads": b.offspring_threads} for b in getattr(solver, "buckets", [])],
           "two_opt_totals": getattr(solver, "two_opt_totals", None),
           "timing": {k: round(v, 4) for k, v in solver.last_timing.items() if isinstance(v, (int, float))}}
@@ -604,7 +605,7 @@ def run_ga_bench(args) -> dict:
   build_library()
   try:
     return ga_measure(args.workload, args.warmup, args.steps, world, rank, engine=args.engine, chunk=args.chunk,
-                      no_graph=args.no_graph, batch_incremental=args.batch_incremental)
+                      no_graph=args.no_graph, batch_incremental=args.batch_incremental, batch_pair=args.batch_pair)
   finally:
     _finish_ranks(world)
 
@@ -690,7 +691,8 @@ def run_uneven_bench(args) -> dict:
     solver = FusedBatchSolver(population_size=64, mutation_rate=0.05, tournament_k=5, nn_k=5,
                               local_search=LocalSearchConfig("best", 10, 20), elite_count=8, post_init=True,
                               max_matrix_dimension=4096, tuner=tuner, chunk=args.chunk,
-                              use_graph=not args.no_graph, incremental=args.batch_incremental)
+                              use_graph=not args.no_graph, incremental=args.batch_incremental,
+                              pair=args.batch_pair)
     gc.collect()  # the previous runs' garbage, outside the timed call
     t0 = time.perf_counter()
     res = solver.evolve(ctxs, G, patience=10**9)
@@ -733,7 +735,7 @@ def run_uneven_bench(args) -> dict:
                      "generations_per_step": gens // args.steps,
                      "elite_edge_ties_per_step": ties // args.steps, "host_pauses_per_step": pauses // args.steps,
                      "buckets": [{"n": [b.lo, b.hi], "coords": b.coords, "instances": len(b.items),
-                                  "two_opt_threads": b.two_opt_threads, "incremental": b.incremental,
+                                  "two_opt_threads": b.two_opt_threads, "incremental": b.incremental, "pair": b.pair,
                                   "offspring_threads": b.offspring_threads}
                                  for b in solver.buckets],
                      "setup_s": solver.last_timing["setup_s"], "tune_s_total": tune_s,
@@ -1039,6 +1041,8 @@ def main(argv=None) -> int:
                   help="GA/uneven: 2-opt with the reverse k-NN index (best: only the rows a move can change are "
                        "recomputed; first: incremental restart); auto lets the tuner measure both; off (the "
                        "solver's default) uses the plain kernel")
+  ap.add_argument("--batch-pair", default="auto", choices=["auto", "on", "off"],
+                  help="GA/uneven: best-mode 2-opt of a row by a two-CTA cluster; auto lets the tuner measure it")
   ap.add_argument("--cpu-workers", type=int, default=0, help="0: all host cores, capped at 64")
   ap.add_argument("--no-cpu-baseline", action="store_true")
   ap.add_argument("--no-ga", action="store_true", help="two_opt: leave out the ga1000 sub-result")

@@ -558,6 +558,12 @@ int tspb_batch_survival(const tspb_batch* b, void* stream);
  * CTA instead of 16 n); first mode restarts from the move's row after checking the
  * affected entries (as tspb_two_opt with the reverse index). Same results either way. */
 #define TSPB_BATCH_INCREMENTAL 4
+/* best mode, GROUPED, not INCREMENTAL: every row is refined by a two-CTA thread-block
+ * cluster; both CTAs keep the tour state and apply every move, each scans alternate
+ * rounds of a pass, and the pass minimum is exchanged through distributed shared memory.
+ * Same results; for phases with fewer units than SMs (elites of a few runs). threads counts
+ * per CTA, and tspb_batch_two_opt_occupancy then reports co-resident CTAs of such pairs. */
+#define TSPB_BATCH_PAIR 8
 /* 2-opt over the (item, row) units of one phase: persistent CTAs (ctas <= 0: every CTA
  * that fits) take units from the device counter `queue` (zeroed by this call) in item
  * order; put the largest instances first. `flags` (TSPB_BATCH_*) state what holds for

@@ -137,6 +137,38 @@ def test_batch_first_mode_and_early_stop_match_oracle(batch_mod, incremental):
   assert any(b.incremental for b in solver.buckets) == (incremental == "on")
 
 
+@pytest.mark.parametrize("threads", [128, 1024])
+def test_cta_pairs_match_oracle(batch_mod, threads):
+  """Best-mode 2-opt with every row refined by a two-CTA cluster (pair="on"): post-init on
+  every row, elites each generation, lattices whose elite edges tie, a rebuilt-distance
+  bucket. Runs must equal the oracle's exactly (tours, fitness, history, generator)."""
+  from tsp_gpu_clean_b200.fused import LocalSearchConfig
+  from tsp_gpu_clean_b200.instances import clustered_instance, uniform_instance
+  from tsp_gpu_clean_b200.problem import Problem, ProblemContext
+
+  from tsp_gpu_clean_b200.autotune import BatchAutotuner
+
+  class Pick(BatchAutotuner):
+    """Pairs of `threads`-thread CTAs for the 2-opt; the middle candidate elsewhere."""
+
+    def choose(self, key, candidates, probe):
+      if "|two_opt|" in key:
+        return next(c for c in candidates if c // 8 == threads and c & 4)
+      return super().choose(key, candidates, probe)
+
+  insts = [(uniform_instance(57, 31), 41), (clustered_instance(260, 8, 30.0, 32), 42), (_lattice(7, 7), 43),
+           (uniform_instance(300, 33), 44)]
+  ctxs = [ProblemContext(Problem.from_coordinates(c), seed=s) for c, s in insts]
+  solver = batch_mod.FusedBatchSolver(population_size=32, mutation_rate=0.2, elite_count=6, post_init=True,
+                                      local_search=LocalSearchConfig("best", 10, 8), max_matrix_dimension=280,
+                                      pair="on", tuner=Pick(enabled=False), bucket_bounds=(64, 256), chunk=4)
+  res = solver.evolve(ctxs, 25, patience=10**9)
+  assert all(b.pair and b.two_opt_threads == threads for b in solver.buckets)
+  assert any(b.coords for b in solver.buckets)
+  for idx, (coords, seed) in enumerate(insts):
+    _check_run(solver, res, ctxs, idx, _oracle_run(coords, seed, 32, 0.2, 6, True, "best", 10, 8, 25, 10**9))
+
+
 def test_converged_row_skipping_changes_nothing(batch_mod):
   """Skipping the refinement of converged rows gives the same runs, with less 2-opt work."""
   from tsp_gpu_clean_b200.fused import LocalSearchConfig

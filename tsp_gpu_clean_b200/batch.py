@@ -103,6 +103,7 @@ class Bucket:
   grouped: bool = False  # every item's k % 4 == 0 and its packed table 16-byte aligned
   can_rebuild: bool = False  # every item has coordinates: the tuner may pick them over the matrix
   incremental: bool = False  # the 2-opt runs with the reverse k-NN index (TSPB_BATCH_INCREMENTAL)
+  pair: bool = False  # every row is refined by a two-CTA cluster (TSPB_BATCH_PAIR, best mode)
   two_opt_threads: int = 128
   offspring_threads: int = 128
   d_items: Any = None
@@ -139,7 +140,7 @@ class FusedBatchSolver:
                tuner: BatchAutotuner | None = None, bucket_bounds: Sequence[int] = DEFAULT_BUCKET_BOUNDS,
                chunk: int = 16, skip_converged: bool = True, concurrent_buckets: bool = True,
                crossover: str = "pmx", mutation: str = "inversion", init: str = "nn",
-               local_search_stage: str = "none", incremental: str = "off") -> None:
+               local_search_stage: str = "none", incremental: str = "off", pair: str = "auto") -> None:
     if population_size < 2:
       raise ValueError("population_size must be >= 2")
     if init not in ("nn", "random"):
@@ -155,6 +156,12 @@ class FusedBatchSolver:
     if incremental not in ("auto", "on", "off"):
       raise ValueError("incremental must be 'auto', 'on' or 'off'")
     self.incremental = incremental
+    # best-mode 2-opt of a row by a two-CTA cluster (both CTAs apply every move, each scans
+    # half of every pass): pays off when a phase has fewer rows than SMs, e.g. the elites of
+    # one run; "auto" lets the tuner measure it beside the one-CTA kernel
+    if pair not in ("auto", "on", "off"):
+      raise ValueError("pair must be 'auto', 'on' or 'off'")
+    self.pair = pair
     if crossover not in CROSSOVER_CODES:
       raise ValueError(f"crossover must be one of {sorted(CROSSOVER_CODES)}")
     if mutation not in MUTATION_CODES:
@@ -246,7 +253,8 @@ class FusedBatchSolver:
   @staticmethod
   def _flags(bucket: Bucket) -> int:
     return ((native.TSPB_BATCH_COORDS if bucket.coords else 0) | (native.TSPB_BATCH_GROUPED if bucket.grouped else 0)
-            | (native.TSPB_BATCH_INCREMENTAL if bucket.incremental else 0))
+            | (native.TSPB_BATCH_INCREMENTAL if bucket.incremental else 0)
+            | (native.TSPB_BATCH_PAIR if bucket.pair else 0))
 
   def _two_opt(self, st_ref, bucket: Bucket, phase: int, threads: int | None = None) -> None:
     rc = native.load_library().tspb_batch_two_opt(
@@ -329,20 +337,30 @@ class FusedBatchSolver:
     for b in self.buckets:
       if self._ls_rows:
         units = len(b.items) * self._ls_rows
+        pairable = b.grouped and self.ls.mode in ("best", "batch")
         key = self.tuner.key(name, "two_opt", mode=self.ls.mode, k=self.k, iters=int(self.ls.max_iterations),
                              lo=b.lo, hi=b.hi, coords=b.coords, rebuild=b.can_rebuild, units=units,
-                             inc=self.incremental if b.grouped else "off")
-        # candidate = 4 * threads + 2 * incremental + source (1: distances rebuilt from coordinates)
+                             inc=self.incremental if b.grouped else "off", pair=self.pair if pairable else "off")
+        # candidate = 8 * threads + 4 * pair + 2 * incremental + source (1: distances rebuilt
+        # from coordinates); a pair runs without the incremental row keys
         incs = {"auto": (0, 1), "on": (1,), "off": (0,)}[self.incremental] if b.grouped else (0,)
+        pairs = {"auto": (0, 1), "on": (1,), "off": (0,)}[self.pair] if pairable else (0,)
         sources = (0, 1) if (b.can_rebuild and not b.coords) else ((1,) if b.coords else (0,))
-        cands = [4 * t + 2 * inc + src for t in TWO_OPT_THREADS for inc in incs for src in sources
-                 if lib.tspb_batch_two_opt_occupancy(
-                   b.max_n, self._mode, t, native.TSPB_BATCH_GROUPED | native.TSPB_BATCH_INCREMENTAL if inc else 0) > 0]
+
+        def fits(t, inc, pr):
+          flags = ((native.TSPB_BATCH_GROUPED if b.grouped else 0) | (native.TSPB_BATCH_INCREMENTAL if inc else 0)
+                   | (native.TSPB_BATCH_PAIR if pr else 0))
+          return lib.tspb_batch_two_opt_occupancy(b.max_n, self._mode, t, flags) > 0
+
+        cands = [8 * t + 4 * pr + 2 * inc + src for t in TWO_OPT_THREADS for pr in pairs for inc in incs
+                 for src in sources if not (pr and inc) and fits(t, inc, pr)]
         if not cands:
           raise ValueError(f"instances of n={b.max_n} do not fit the batch 2-opt's shared memory")
         choice = self.tuner.choose(key, cands,
-                                   lambda c, b=b: self._probe_two_opt(b, c // 4, bool(c & 1), bool(c & 2)))
-        b.two_opt_threads = choice // 4
+                                   lambda c, b=b: self._probe_two_opt(b, c // 8, bool(c & 1), bool(c & 2),
+                                                                      bool(c & 4)))
+        b.two_opt_threads = choice // 8
+        b.pair = bool(choice & 4)
         b.incremental = bool(choice & 2)
         if choice & 1 and not b.coords:
           self._rebuild_from_coordinates(b)
@@ -373,7 +391,8 @@ class FusedBatchSolver:
     self.d_inst.copy_(torch.frombuffer(bytearray(self.h_inst), dtype=torch.uint8))
     b.coords = True
 
-  def _probe_two_opt(self, b: Bucket, threads: int, rebuild: bool = False, incremental: bool = False) -> float:
+  def _probe_two_opt(self, b: Bucket, threads: int, rebuild: bool = False, incremental: bool = False,
+                     pair: bool = False) -> float:
     """The generation's 2-opt work shape for one bucket on scratch copies of the initial
     tours: the first `elite` rows of every instance (every row with the post_mutation
     stage), refined for up to max_iterations passes, with the bucket's matrices or
@@ -393,7 +412,8 @@ class FusedBatchSolver:
         inst[i].dist_stride = 0
     d_inst = torch.frombuffer(bytearray(inst), dtype=torch.uint8).cuda()
     flags = ((native.TSPB_BATCH_COORDS if (b.coords or rebuild) else 0)
-             | (native.TSPB_BATCH_GROUPED if b.grouped else 0) | (native.TSPB_BATCH_INCREMENTAL if incremental else 0))
+             | (native.TSPB_BATCH_GROUPED if b.grouped else 0) | (native.TSPB_BATCH_INCREMENTAL if incremental else 0)
+             | (native.TSPB_BATCH_PAIR if pair else 0))
     status = torch.zeros((self.I, e), dtype=torch.int32, device="cuda")
     st = self._state()
     st.P = e

@@ -294,8 +294,11 @@ __global__ void batch_pause_kernel(const tspb_batch B) {
 // LAYOUT: SCAN_GROUPED when every item's k is a multiple of U and its packed table is
 // U*4-byte aligned, else SCAN_PACKED. REV (TSPB_BATCH_INCREMENTAL): the items carry their
 // reverse k-NN index; best mode then keeps incremental row keys (INC, grouped layout only)
-// and first mode restarts incrementally.
-template <int MODE, int THREADS, int U, bool COORDS, int LAYOUT, bool REV = false>
+// and first mode restarts incrementally. CL = 2 (TSPB_BATCH_PAIR, best mode, grouped, no
+// REV): the grid is made of two-CTA clusters, CTA 0 of a cluster takes each unit from the
+// queue and hands it to CTA 1 through distributed shared memory, and the pair refines the
+// row together (scan_tour's CTA pair).
+template <int MODE, int THREADS, int U, bool COORDS, int LAYOUT, bool REV = false, int CL = 1>
 __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value)
     batch_two_opt_kernel(const tspb_batch B, const int32_t* __restrict__ items, int num_items, int rows, int phase,
                          long long max_iter, int max_n, unsigned* __restrict__ queue, long long budget) {
@@ -304,10 +307,19 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value)
   __shared__ unsigned s_unit;
   const unsigned units = (unsigned)num_items * (unsigned)rows;
   for (;;) {
-    if (threadIdx.x == 0) s_unit = atomicAdd(queue, 1u);
-    __syncthreads();
-    const unsigned u = s_unit;
-    __syncthreads();  // every thread has read s_unit before thread 0 takes the next unit
+    unsigned u;
+    if constexpr (CL == 1) {
+      if (threadIdx.x == 0) s_unit = atomicAdd(queue, 1u);
+      __syncthreads();
+      u = s_unit;
+      __syncthreads();  // every thread has read s_unit before thread 0 takes the next unit
+    } else {
+      cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+      if (cl.block_rank() == 0 && threadIdx.x == 0) s_unit = atomicAdd(queue, 1u);
+      cl.sync();
+      u = *cl.map_shared_rank(&s_unit, 0u);
+      cl.sync();  // both CTAs hold the unit before CTA 0 takes the next one
+    }
     if (u >= units) return;
     const int it = (int)(u / (unsigned)rows), e = (int)(u - (unsigned)it * (unsigned)rows);
     const int i = items[it];
@@ -361,7 +373,7 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value)
     T.cost = phase == TSPB_BATCH_PHASE_POSTINIT
                  ? nullptr
                  : (offspring ? B.off_fit : fit_buf(B, parity)) + (long long)i * B.P + row;
-    scan_tour<MODE, THREADS, U, LAYOUT, REV && MODE == TSPB_MODE_BEST>(T, S);
+    scan_tour<MODE, THREADS, U, LAYOUT, REV && MODE == TSPB_MODE_BEST, true, CL>(T, S);
   }
 }
 
@@ -462,6 +474,45 @@ static int batch_two_opt_launch(const tspb_batch& b, const int32_t* items, int n
     else
       return TSPB_ERR_ARG;
   }
+  if (flags & TSPB_BATCH_PAIR) {
+    // two-CTA clusters, one per unit at a time (best mode, grouped layout; checked by the caller)
+    if constexpr (MODE == TSPB_MODE_BEST && U == 4) {
+      Kern pk = coords ? batch_two_opt_kernel<MODE, THREADS, U, true, SCAN_GROUPED, false, 2>
+                       : batch_two_opt_kernel<MODE, THREADS, U, false, SCAN_GROUPED, false, 2>;
+      TSPB_CUDA_CHECK(cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      cudaLaunchConfig_t cfg = {};
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = 2;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.blockDim = dim3(THREADS);
+      cfg.dynamicSmemBytes = smem;
+      cfg.stream = st;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      int clusters = 0;
+      cfg.gridDim = dim3(2);
+      TSPB_CUDA_CHECK(cudaOccupancyMaxActiveClusters(&clusters, pk, &cfg));
+      if (clusters <= 0) return TSPB_ERR_UNSUPPORTED;
+      const long long units = (long long)num_items * rows;
+      long long pairs = clusters;
+      if (ctas > 0 && ctas / 2 < pairs) pairs = ctas / 2 > 0 ? ctas / 2 : 1;
+      if (pairs > units) pairs = units;
+      int sms = 0, dev = 0;
+      TSPB_CUDA_CHECK(cudaGetDevice(&dev));
+      TSPB_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      const int pct = carveout_for((int)((2 * pairs + sms - 1) / sms), smem);
+      if (pct > 0) TSPB_CUDA_CHECK(cudaFuncSetAttribute(pk, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+      TSPB_CUDA_CHECK(cudaMemsetAsync(queue, 0, sizeof(unsigned), st));
+      cfg.gridDim = dim3((unsigned)(2 * pairs));
+      TSPB_CUDA_CHECK(cudaLaunchKernelEx(&cfg, pk, b, items, num_items, rows, phase, max_iter, max_n, queue,
+                                         watchdog_cycles()));
+      return tspb_launch_status();
+    } else {
+      return TSPB_ERR_ARG;
+    }
+  }
   TSPB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   TSPB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem));
@@ -482,7 +533,32 @@ static int batch_two_opt_launch(const tspb_batch& b, const int32_t* items, int n
 }
 
 template <int MODE, int THREADS, int U>
-static int batch_two_opt_occ(size_t smem, bool rev) {
+static int batch_two_opt_occ(size_t smem, bool rev, bool pair) {
+  if (pair) {  // co-resident two-CTA clusters, in CTAs
+    if constexpr (MODE == TSPB_MODE_BEST && U == 4) {
+      auto pk = batch_two_opt_kernel<MODE, THREADS, U, false, SCAN_GROUPED, false, 2>;
+      if (cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+      cudaLaunchConfig_t cfg = {};
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = 2;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.gridDim = dim3(2);
+      cfg.blockDim = dim3(THREADS);
+      cfg.dynamicSmemBytes = smem;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      int clusters = 0;
+      if (cudaOccupancyMaxActiveClusters(&clusters, pk, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+      }
+      return 2 * clusters;
+    } else {
+      return 0;
+    }
+  }
   auto kern = rev ? batch_two_opt_kernel<MODE, THREADS, U, false, SCAN_GROUPED, true>
                   : batch_two_opt_kernel<MODE, THREADS, U, false, SCAN_GROUPED>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
@@ -524,13 +600,13 @@ static int batch_two_opt_mode(const tspb_batch& b, const int32_t* items, int num
 }
 
 template <int MODE>
-static int batch_two_opt_occ_mode(int threads, size_t smem, bool rev) {
+static int batch_two_opt_occ_mode(int threads, size_t smem, bool rev, bool pair) {
   switch (threads) {
-    case 64: return batch_two_opt_occ<MODE, 64, 4>(smem, rev);
-    case 128: return batch_two_opt_occ<MODE, 128, 4>(smem, rev);
-    case 256: return batch_two_opt_occ<MODE, 256, 4>(smem, rev);
-    case 512: return batch_two_opt_occ<MODE, 512, 4>(smem, rev);
-    case 1024: return batch_two_opt_occ<MODE, 1024, 4>(smem, rev);
+    case 64: return batch_two_opt_occ<MODE, 64, 4>(smem, rev, pair);
+    case 128: return batch_two_opt_occ<MODE, 128, 4>(smem, rev, pair);
+    case 256: return batch_two_opt_occ<MODE, 256, 4>(smem, rev, pair);
+    case 512: return batch_two_opt_occ<MODE, 512, 4>(smem, rev, pair);
+    case 1024: return batch_two_opt_occ<MODE, 1024, 4>(smem, rev, pair);
     default: return 0;
   }
 }
@@ -603,17 +679,22 @@ extern "C" int tspb_batch_survival(const tspb_batch* b, void* stream) {
 extern "C" int tspb_batch_two_opt_occupancy(int32_t max_n, int32_t mode, int32_t threads, int32_t flags) {
   if (max_n < 4 || (mode != TSPB_MODE_BEST && mode != TSPB_MODE_FIRST)) return 0;
   const bool rev = flags & TSPB_BATCH_INCREMENTAL;
+  const bool pair = flags & TSPB_BATCH_PAIR;
+  if (pair && (rev || mode != TSPB_MODE_BEST)) return 0;
   const size_t smem = scan_tour_state_bytes(max_n, mode, rev);
   if (smem > (size_t)smem_optin() - 2048) return 0;
-  return mode == TSPB_MODE_BEST ? batch_two_opt_occ_mode<TSPB_MODE_BEST>(threads, smem, rev)
-                                : batch_two_opt_occ_mode<TSPB_MODE_FIRST>(threads, smem, rev);
+  return mode == TSPB_MODE_BEST ? batch_two_opt_occ_mode<TSPB_MODE_BEST>(threads, smem, rev, pair)
+                                : batch_two_opt_occ_mode<TSPB_MODE_FIRST>(threads, smem, rev, pair);
 }
 
 extern "C" int tspb_batch_two_opt(const tspb_batch* b, const int32_t* items, int32_t num_items, int32_t max_n,
                                   int32_t flags, int32_t phase, int32_t mode, int64_t max_iterations, int32_t threads,
                                   int32_t ctas, uint32_t* queue, void* stream) {
   if (!batch_ok(b) || num_items < 0 || max_n < 4 || !queue) return TSPB_ERR_ARG;
-  if (flags & ~(TSPB_BATCH_COORDS | TSPB_BATCH_GROUPED | TSPB_BATCH_INCREMENTAL)) return TSPB_ERR_ARG;
+  if (flags & ~(TSPB_BATCH_COORDS | TSPB_BATCH_GROUPED | TSPB_BATCH_INCREMENTAL | TSPB_BATCH_PAIR)) return TSPB_ERR_ARG;
+  if ((flags & TSPB_BATCH_PAIR) &&
+      (mode != TSPB_MODE_BEST || !(flags & TSPB_BATCH_GROUPED) || (flags & TSPB_BATCH_INCREMENTAL)))
+    return TSPB_ERR_ARG;
   const bool rev = flags & TSPB_BATCH_INCREMENTAL;
   if (rev && !(flags & TSPB_BATCH_GROUPED)) return TSPB_ERR_ARG;
   if (phase < TSPB_BATCH_PHASE_POSTINIT || phase > TSPB_BATCH_PHASE_OFFSPRING) return TSPB_ERR_ARG;

@@ -15,8 +15,9 @@
 //   FP64 rebuild from coordinates when the instance has no matrix).
 //
 // best keeps a per-thread (gain, i*k + r) minimum and reduces once per pass. first
-// publishes the smallest improving index of a round with a shared atomicMin; once set,
-// later rounds only count the pairs the reference still evaluates (validity, no gains).
+// publishes improving indices with a shared atomicMin; each thread stops scanning as soon
+// as the published minimum lies below all of its remaining entries (no barrier per round),
+// and one barrier at the end of the scan makes the minimum the pass's first improving entry.
 //
 // best with incremental row keys (INC, grouped layout, reverse k-NN index): every row keeps
 // the minimum key of its improving entries. After a move with window [bi, bj] only the rows
@@ -33,7 +34,15 @@
 // [bi, bj], where pos/succ/eout of c may have changed. The next pass therefore evaluates
 // just those affected entries (found through the reverse index) and, when none improves,
 // scans from row bi on: the first improving entry it finds is the reference's.
+//
+// best over a CTA pair (CL = 2, a thread-block cluster of two CTAs; grouped layout): both
+// CTAs hold the whole tour state and apply every move; CTA r scans the rounds r, r + 2, ...
+// of each pass, and the two per-CTA minima meet through distributed shared memory (one
+// cluster barrier per pass), so both take the same move. The watchdog flags of both CTAs
+// travel with the minima, so both stop together.
 #pragma once
+
+#include <cooperative_groups.h>
 
 #include "two_opt.cuh"
 
@@ -47,6 +56,9 @@ struct ScanSmem {
   int nlist;        // incremental best: rows to recompute in this pass
   int bad;
   int stop;
+  unsigned long long xkey[2];  // CTA pair: this CTA's pass minimum (by pass parity)
+  int xstop[2];                // CTA pair: this CTA's watchdog flag of that pass
+  long long xcnt[2];           // CTA pair: this CTA's pair and gain counts at exit
 };
 
 template <int THREADS>
@@ -115,10 +127,13 @@ __device__ __forceinline__ void load_words(const uint32_t* p, uint32_t (&w)[U]) 
 // and refreshing them after a move visits every candidate of every row in the reversed
 // window, so a caller that passes no stats runs the COUNT = false instance (or, with
 // COUNT = true, skips the refresh at run time): same moves, same tours.
-template <int MODE, int THREADS, int U, int LAYOUT, bool INC = false, bool COUNT = true>
+template <int MODE, int THREADS, int U, int LAYOUT, bool INC = false, bool COUNT = true, int CL = 1>
 __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
   constexpr bool PACKED = LAYOUT != SCAN_PLAIN;
   constexpr bool GROUPED = LAYOUT == SCAN_GROUPED;
+  static_assert(CL == 1 || (CL == 2 && MODE == TSPB_MODE_BEST && GROUPED && !INC),
+                "a CTA pair runs best mode on the grouped layout only");
+  const unsigned rank = CL > 1 ? cooperative_groups::this_cluster().block_rank() : 0u;
   const int n = T.n, k = T.k, rows = n - 2;
   const int tid = threadIdx.x;
   int32_t* g_tour = T.g_tour;
@@ -228,7 +243,7 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
       S.first = NO_IDX;
     }
     __syncthreads();
-    if (S.stop) {
+    if (CL == 1 && S.stop) {  // a CTA pair stops only after exchanging its flags (below)
       err = S.stop;
       break;
     }
@@ -361,9 +376,17 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
       // nothing to scan: first mode's smallest improving affected entry is the first of the
       // pass; incremental best already holds this thread's share of the row keys
     } else if constexpr (GROUPED) {
-      // entries [e0 + tid*U, e0 + tid*U + U) of round e0 lie in row gi, columns gr..gr+U-1
+      // entries [e0 + tid*U, e0 + tid*U + U) of round e0 lie in row gi, columns gr..gr+U-1;
+      // a CTA pair takes alternate rounds
       int gi = g_row0 + start_row, gr = g_col0;
-      for (int e0 = start_row * k; e0 < E; e0 += STEP) {
+      int e_first = start_row * k;
+      if constexpr (CL > 1) {
+        e_first += (int)rank * STEP;
+        const int eb0 = e_first + tid * U;
+        gi = eb0 / k;
+        gr = eb0 - gi * k;
+      }
+      for (int e0 = e_first; e0 < E; e0 += CL * STEP) {
         const int eb = e0 + tid * U;
         if (eb < E) {
           const int a = tour[gi];
@@ -400,16 +423,21 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
             }
           }
         }
-        gr += sr;
-        gi += sq;
+        if constexpr (CL > 1) {
+          gr += (CL * STEP) % k;
+          gi += (CL * STEP) / k;
+        } else {
+          gr += sr;
+          gi += sq;
+        }
         if (gr >= k) {
           gr -= k;
           ++gi;
         }
-        if (MODE == TSPB_MODE_FIRST) {
-          __syncthreads();
-          if (S.first != NO_IDX) break;
-        }
+        // first: no barrier per round; a thread stops once an improving index below all of
+        // its remaining entries (>= e0 + STEP) is known. S.first only decreases, so every
+        // entry below the pass's final minimum is still evaluated by its thread.
+        if (MODE == TSPB_MODE_FIRST && *reinterpret_cast<volatile unsigned*>(&S.first) < (unsigned)(e0 + STEP)) break;
       }
     } else {
     int ri[U], rr[U], ee[U];
@@ -481,10 +509,7 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
           ++ri[u];
         }
       }
-      if (MODE == TSPB_MODE_FIRST) {
-        __syncthreads();
-        if (S.first != NO_IDX) break;
-      }
+      if (MODE == TSPB_MODE_FIRST && *reinterpret_cast<volatile unsigned*>(&S.first) < (unsigned)(e0 + STEP)) break;
     }
     }
     my_pairs += cnt;
@@ -492,7 +517,25 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
     unsigned idx;
     if (MODE == TSPB_MODE_BEST) {
       const unsigned long long key = bidx == NO_IDX ? NO_KEY : gain_key(bgain, bidx);
-      const unsigned long long best = block_min(key, S.red64);
+      unsigned long long best = block_min(key, S.red64);
+      if constexpr (CL > 1) {
+        // the two CTAs' minima and watchdog flags meet through distributed shared memory;
+        // slots alternate by pass, so one cluster barrier per pass suffices
+        cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+        const int slot = (int)(passes & 1);
+        if (tid == 0) {
+          S.xkey[slot] = best;
+          S.xstop[slot] = S.stop;
+        }
+        cl.sync();
+        const unsigned long long peer = *cl.map_shared_rank(&S.xkey[slot], rank ^ 1u);
+        const int peer_stop = *cl.map_shared_rank(&S.xstop[slot], rank ^ 1u);
+        best = peer < best ? peer : best;
+        if (S.stop || peer_stop) {
+          err = TSPB_ERR_BUDGET;
+          break;
+        }
+      }
       if (best == NO_KEY) {
         converged = true;
         break;
@@ -554,9 +597,24 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
   }
 
   __syncthreads();
-  for (int p = tid; p < n; p += THREADS) g_tour[p] = tour[p];
-  const long long tp = block_sum(my_pairs, S.redll);
-  const long long te = block_sum(my_eval, S.redll);
+  if (rank == 0)
+    for (int p = tid; p < n; p += THREADS) g_tour[p] = tour[p];
+  long long tp = block_sum(my_pairs, S.redll);
+  long long te = block_sum(my_eval, S.redll);
+  if constexpr (CL > 1) {  // the pair's counts add up in CTA 0, which alone writes the results
+    cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+    if (tid == 0) {
+      S.xcnt[0] = tp;
+      S.xcnt[1] = te;
+    }
+    cl.sync();
+    if (rank == 0) {
+      tp += *cl.map_shared_rank(&S.xcnt[0], 1u);
+      te += *cl.map_shared_rank(&S.xcnt[1], 1u);
+    }
+    cl.sync();  // CTA 1's shared memory stays valid until CTA 0 has read it
+    if (rank != 0) return;
+  }
   if (T.cost != nullptr) {  // eout[x] = d(x, succ[x]) of the final tour: its edges, each once
     long long len = 0;
     for (int p = tid; p < n; p += THREADS) len += eout[p];

@@ -117,6 +117,7 @@ TSPB_MUT_SWAP = 1
 TSPB_BATCH_COORDS = 1
 TSPB_BATCH_GROUPED = 2
 TSPB_BATCH_INCREMENTAL = 4
+TSPB_BATCH_PAIR = 8
 
 
 class Pcg64(ctypes.Structure):
