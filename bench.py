@@ -803,12 +803,16 @@ def run_learned_bench(args) -> dict:
   """Learned top-10 vs k-NN top-20 candidates for 2-opt at equal wall time.
 
   Train: `args.train_instances` generated instances (n log-uniform in [200, 2000], half
-  uniform, half 10-50-cluster mixtures); labels are the edges of the best 2-opt local
-  optimum of nearest-neighbour starts (optionally GA-refined). Evaluate at n = 1000,
-  5000, 10000: both methods refine the same nearest-neighbour starts to a local optimum
-  (best mode); the learned method, being faster per start, keeps refining further starts
-  until it has used the k-NN method's device time. Gap = best length / best length found
-  by either method - 1.
+  uniform, half 10-50-cluster mixtures); labels are the edges of the best tour that the
+  memetic GA produces on the instance (nearest-neighbour starts refined to a 2-opt local
+  optimum, then `args.ga_label_generations` generations of the fused GA).
+  Evaluate at n = 1000, 5000, 10000: both arms run iterated 2-opt under the same CUDA-event
+  time budget (`args.ils_factor` times the k-NN arm's first descent): the same
+  nearest-neighbour starts refined to a local optimum (best mode) with the arm's table, then
+  rounds of `args.ils_kicks` double-bridge kicks of the best tour, refined in one launch.
+  The learned arm's budget also pays for building its table (features, MLP, top-k). Gap =
+  best length / best length found by any arm - 1. Learned lists of 12 and 14 entries are
+  reported beside the 10-entry headline.
   """
   import torch
 
@@ -843,6 +847,7 @@ def run_learned_bench(args) -> dict:
     torch.cuda.synchronize()
     return out, e0.elapsed_time(e1) / 1e3
 
+  sizes = (10, 12, 14)
   rows = []
   for n in (1000, 5000, 10000):
     for j in range(args.eval_instances):
@@ -851,34 +856,39 @@ def run_learned_bench(args) -> dict:
       inst = learned.device_instance(coords, 30)
       starts = learned.nn_starts(inst, args.eval_starts, seed)
       knn20 = inst.pool[:, :20].contiguous()
-      (t_k, _), time_k = timed(lambda: learned.two_opt_table(inst, starts, knn20, mode="best"))
-      best_k = learned.tour_lengths(inst, t_k).min()
-      tab, time_tab = timed(lambda: lc.table(inst, 10))
-      used = time_tab
-      best_l = np.inf
-      rounds = 0
-      while used < time_k or rounds == 0:
-        st = starts if rounds == 0 else learned.nn_starts(inst, args.eval_starts, seed + 7 * rounds)
-        (t_l, _), dt = timed(lambda: learned.two_opt_table(inst, st, tab, mode="best"))
-        used += dt
-        best_l = min(best_l, learned.tour_lengths(inst, t_l).min())
-        rounds += 1
-        if rounds >= 64:
-          break
-      ref = min(best_k, best_l)
-      rows.append({"n": n, "knn_gap": best_k / ref - 1, "learned_gap": best_l / ref - 1, "knn_s": time_k,
-                   "learned_s": used, "learned_rounds": rounds})
+      (t_k, _), descent_k = timed(lambda: learned.two_opt_table(inst, starts, knn20, mode="best"))
+      budget = args.ils_factor * descent_k
+      knn = learned.iterated_two_opt(inst, starts, knn20, budget, args.ils_kicks, seed)
+      row = {"n": n, "budget_s": budget, "knn": knn["length"], "knn_rounds": knn["rounds"],
+             "knn_recall": learned.edge_recall(knn20, knn["tour"])}
+      for k in sizes:
+        tab, t_tab = timed(lambda: lc.table(inst, k))
+        got = learned.iterated_two_opt(inst, starts, tab, budget, args.ils_kicks, seed, spent_s=t_tab)
+        row[f"learned{k}"] = got["length"]
+        row[f"learned{k}_rounds"] = got["rounds"]
+        row[f"learned{k}_table_s"] = t_tab
+        row[f"learned{k}_recall_of_knn_tour"] = learned.edge_recall(tab, knn["tour"])
+      ref = min(row["knn"], *(row[f"learned{k}"] for k in sizes))
+      row["knn_gap"] = row["knn"] / ref - 1
+      for k in sizes:
+        row[f"learned{k}_gap"] = row[f"learned{k}"] / ref - 1
+      rows.append(row)
   by_n = {}
   for n in (1000, 5000, 10000):
     rs = [r for r in rows if r["n"] == n]
-    by_n[str(n)] = {"learned_gap_pct": 100 * float(np.mean([r["learned_gap"] for r in rs])),
-                    "knn_gap_pct": 100 * float(np.mean([r["knn_gap"] for r in rs])),
-                    "knn_s": float(np.mean([r["knn_s"] for r in rs])),
-                    "learned_s": float(np.mean([r["learned_s"] for r in rs])),
-                    "learned_rounds": float(np.mean([r["learned_rounds"] for r in rs]))}
-  return {"value": 100 * float(np.mean([r["learned_gap"] for r in rows])),
-          "knn": 100 * float(np.mean([r["knn_gap"] for r in rows])), "by_n": by_n,
+    d = {"knn_gap_pct": 100 * float(np.mean([r["knn_gap"] for r in rs])),
+         "budget_s": float(np.mean([r["budget_s"] for r in rs])),
+         "knn_rounds": float(np.mean([r["knn_rounds"] for r in rs]))}
+    for k in sizes:
+      d[f"learned{k}_gap_pct"] = 100 * float(np.mean([r[f"learned{k}_gap"] for r in rs]))
+      d[f"learned{k}_rounds"] = float(np.mean([r[f"learned{k}_rounds"] for r in rs]))
+    by_n[str(n)] = d
+  return {"value": 100 * float(np.mean([r["learned10_gap"] for r in rows])),
+          "knn": 100 * float(np.mean([r["knn_gap"] for r in rows])),
+          "by_list_size": {str(k): 100 * float(np.mean([r[f"learned{k}_gap"] for r in rows])) for k in sizes},
+          "by_n": by_n,
           "train": {"instances": args.train_instances, "edges": edges, "data_s": t_data, "train_s": t_train,
+                    "ga_label_generations": args.ga_label_generations,
                     "final_loss": float(np.mean(lc.train_log[-20:]))}}
 
 
@@ -1052,7 +1062,11 @@ def main(argv=None) -> int:
   ap.add_argument("--train-instances", type=int, default=2000)
   ap.add_argument("--eval-instances", type=int, default=4)
   ap.add_argument("--eval-starts", type=int, default=8)
-  ap.add_argument("--ga-label-generations", type=int, default=0)
+  ap.add_argument("--ga-label-generations", type=int, default=8,
+                  help="learned: generations of the fused GA that refine each training instance's labels")
+  ap.add_argument("--ils-factor", type=float, default=6.0,
+                  help="learned: equal time budget per arm, in units of the k-NN arm's first descent")
+  ap.add_argument("--ils-kicks", type=int, default=128, help="learned: double-bridge kicks per round")
   ap.add_argument("--chunk", type=int, default=16, help="GA: generations replayed between host checks")
   ap.add_argument("--no-graph", action="store_true",
                   help="GA/uneven: launch every generation directly instead of replaying a captured graph "
@@ -1066,11 +1080,13 @@ def main(argv=None) -> int:
     print(json.dumps({"metric": "tour gap @ equal wall time, learned top-10 vs k-NN top-20", "value": res["value"],
                       "unit": "% above best found", "n_gpus": 1, "higher_is_better": False, "data": "synthetic (seeded)",
                       "dtype": "bf16 weights / fp32 accumulate; int32 tours", "knn_gap_pct": res["knn"],
-                      "by_n": res["by_n"], "train": res["train"],
-                      "config": {"workload": "learned candidates: train on generated instances n in [200, 2000], "
-                                             "evaluate n = 1000, 5000, 10000 (2-opt best, nearest-neighbour starts)",
+                      "by_list_size": res["by_list_size"], "by_n": res["by_n"], "train": res["train"],
+                      "config": {"workload": "learned candidates: train on GA tours of generated instances n in "
+                                             "[200, 2000], evaluate n = 1000, 5000, 10000 with iterated 2-opt (best "
+                                             "mode, double-bridge kicks) under equal CUDA-event time per arm",
                                  "train_instances": args.train_instances, "eval_instances_per_n": args.eval_instances,
-                                 "starts": args.eval_starts}}))
+                                 "starts": args.eval_starts, "ils_factor": args.ils_factor,
+                                 "ils_kicks": args.ils_kicks}}))
     return 0
   if args.workload == "uneven":
     return main_uneven(args)

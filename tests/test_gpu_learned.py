@@ -5,6 +5,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
+from oracle import distances as odist
 from oracle import mlp as omlp
 from tsp_gpu_clean_b200 import instances
 
@@ -118,3 +119,34 @@ def test_learned_candidates_beat_plain_knn_at_equal_size(torch_mod):
   print("recall learned/knn", np.mean(rec_l), np.mean(rec_k), "2-opt length learned/knn", np.mean(len_l), np.mean(len_k))
   assert np.mean(rec_l) > np.mean(rec_k)
   assert np.mean(len_l) < np.mean(len_k)
+
+
+def test_iterated_two_opt_under_a_budget():
+  """Double-bridge kicks keep permutations; iterated 2-opt never ends above its first
+  descent and stops once the CUDA-event budget is used."""
+  import torch
+
+  if not torch.cuda.is_available():
+    pytest.skip("no CUDA device")
+  from tsp_gpu_clean_b200 import learned
+  from tsp_gpu_clean_b200.build import build_library
+
+  build_library()
+  coords = instances.uniform_instance(400, 77)
+  inst = learned.device_instance(coords, 30)
+  g = torch.Generator().manual_seed(3)
+  base = torch.randperm(400, generator=g).to(torch.int32).cuda()
+  kicked = learned.double_bridge(base, 16, g)
+  assert kicked.shape == (16, 400)
+  for row in kicked.cpu().numpy():
+    assert np.array_equal(np.sort(row), np.arange(400))
+  starts = learned.nn_starts(inst, 4, 5)
+  table = inst.pool[:, :10].contiguous()
+  first, _ = learned.two_opt_table(inst, starts, table, mode="best")
+  first_best = float(learned.tour_lengths(inst, first).min())
+  res = learned.iterated_two_opt(inst, starts, table, budget_s=0.05, kicks=32, seed=1)
+  assert res["length"] <= first_best and res["rounds"] >= 1 and res["used_s"] >= 0.05
+  t = res["tour"].cpu().numpy()
+  assert np.array_equal(np.sort(t), np.arange(400))
+  D = odist.euc2d_matrix(coords)
+  assert int(D[t, np.roll(t, -1)].sum()) == int(res["length"])

@@ -99,6 +99,64 @@ def tour_lengths(inst: InstanceTensors, tours: "torch.Tensor") -> np.ndarray:
   return out.cpu().numpy()
 
 
+def double_bridge(tour: "torch.Tensor", count: int, gen: "torch.Generator") -> "torch.Tensor":
+  """`count` copies of `tour`, each with one random double-bridge kick: cuts 0 < p1 < p2 <
+  p3 < n turn A B C D into A C B D (four edges replaced; position 0 stays first)."""
+  n = int(tour.shape[0])
+  dev = tour.device
+  cuts = torch.randint(1, n, (count, 3), generator=gen)
+  while True:  # three distinct cuts per row
+    cuts, _ = torch.sort(cuts, dim=1)
+    dup = (cuts[:, 0] == cuts[:, 1]) | (cuts[:, 1] == cuts[:, 2])
+    if not bool(dup.any()):
+      break
+    cuts[dup] = torch.randint(1, n, (int(dup.sum()), 3), generator=gen)
+  p1, p2, p3 = (cuts[:, c:c + 1].to(dev) for c in range(3))
+  j = torch.arange(n, device=dev).unsqueeze(0).expand(count, n)
+  lc = p3 - p2
+  src = torch.where(j < p1, j, torch.where(j < p1 + lc, p2 + (j - p1), torch.where(j < p3, p1 + (j - p1 - lc), j)))
+  return tour.long()[src].to(torch.int32).contiguous()
+
+
+def iterated_two_opt(inst: InstanceTensors, starts: "torch.Tensor", table: "torch.Tensor", budget_s: float,
+                     kicks: int, seed: int, spent_s: float = 0.0) -> dict:
+  """Iterated 2-opt with double-bridge kicks under a device-time budget.
+
+  The starts are refined to a 2-opt local optimum (best mode, this candidate table); then,
+  while the CUDA-event time used is below `budget_s`, the best tour so far gets `kicks`
+  kicked copies, all refined in one launch, and the shortest replaces it when shorter.
+  `spent_s` is time already used (for example building the table). Returns the best
+  length, the time used and the rounds run."""
+  gen = torch.Generator().manual_seed(seed)
+
+  def timed(fn):
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    out = fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return out, e0.elapsed_time(e1) / 1e3
+
+  (t, _), used = timed(lambda: two_opt_table(inst, starts, table, mode="best"))
+  used += spent_s
+  lengths = tour_lengths(inst, t)
+  best_i = int(np.argmin(lengths))
+  best, best_len = t[best_i].clone(), float(lengths[best_i])
+  rounds = 0
+  while used < budget_s:
+    def one_round():
+      kicked = double_bridge(best, kicks, gen)
+      out, _ = two_opt_table(inst, kicked, table, mode="best")
+      return out, tour_lengths(inst, out)
+    (out, ls), dt = timed(one_round)
+    used += dt
+    rounds += 1
+    i = int(np.argmin(ls))
+    if float(ls[i]) < best_len:
+      best, best_len = out[i].clone(), float(ls[i])
+  return {"length": best_len, "used_s": used, "rounds": rounds, "tour": best}
+
+
 def random_starts(n: int, count: int, seed: int) -> "torch.Tensor":
   rng = np.random.default_rng(seed)
   return torch.from_numpy(np.stack([rng.permutation(n) for _ in range(count)]).astype(np.int32)).cuda()
