@@ -65,7 +65,9 @@ L2_FLUSH_BYTES = 256 << 20
 #: warp instructions executed (sm__inst_executed.sum), L2 sector bytes
 #: (lts__t_bytes.sum) and DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum,
 #: per 1024-tour launch).
-NCU_PER_GAIN: dict[str, dict[str, float]] = {}
+NCU_PER_GAIN: dict[str, dict[str, float]] = {
+  "first": {"inst": 4.380, "lts_bytes": 38.30, "dram_bytes_per_launch": 8_556_800},
+}
 #: CPU parity sample: tours of the timed batch refined by the oracle (at least this many)
 PARITY_TOURS = 16
 GA_SUB_WORKLOAD = "ga1000"
@@ -145,6 +147,9 @@ def check_parity(gpu: dict, cpu: dict) -> dict:
 class ClockSampler:
   FIELDS = "clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
 
+  #: sampling period of nvidia-smi (ms); --clock-interval-ms changes it
+  interval_ms = 200
+
   def __init__(self, device: int):
     self.device = device
     self.proc = None
@@ -157,7 +162,7 @@ class ClockSampler:
     self.first = []
     try:
       self.proc = subprocess.Popen(
-        ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
+        ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", str(self.interval_ms)],
         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
       ready, _, _ = select.select([self.proc.stdout], [], [], 5.0)
       if ready:
@@ -272,9 +277,10 @@ def _roofline(dominant: str, gains: int, launch_s: float, peaks: dict, tours: in
     l2_ach = gps * per["lts_bytes"] / 1e9
     basis = (f"ncu per evaluated gain: {per['inst']:.2f} warp instructions, {per['lts_bytes']:.2f} L2 sector bytes; "
              f"x {gains} gains per launch / {launch_s * 1e3:.2f} ms")
-  else:
-    int_ach, l2_ach = alg["int32_tops"], alg["l2_gbs"] * 32 / 4
-    basis = "algorithmic (no ncu figure for this launch shape): " + alg["basis"]
+  else:  # one 32-byte sector per gain (the matrix gather) and the algorithmic integer work
+    int_ach, l2_ach = alg["int32_tops"], gps * 32 / 1e9
+    basis = ("no ncu figure for this launch shape: one 32-byte L2 sector and " f"{ALG_OPS_PER_DELTA} integer ops "
+             "per evaluated gain")
   l2 = {"achieved": l2_ach, "peak": l2_peak, "unit": "GB/s", "frac": l2_ach / l2_peak}
   i32 = {"achieved": int_ach, "peak": int_peak, "unit": "TOP/s", "frac": int_ach / int_peak}
   top = i32 if i32["frac"] >= l2["frac"] else l2
@@ -1074,7 +1080,9 @@ def main(argv=None) -> int:
   ap.add_argument("--engine", default="batch", choices=["single", "batch"],
                   help="GA: the multi-instance batch engine with one instance, or the one-run graph engine")
   ap.add_argument("--cpu-gens", type=int, default=0, help="GA: generations in the CPU sample (0: workload default)")
+  ap.add_argument("--clock-interval-ms", type=int, default=200, help="nvidia-smi clock sampling period")
   args = ap.parse_args(argv)
+  ClockSampler.interval_ms = max(20, int(args.clock_interval_ms))
   if args.workload == "learned":
     res = run_learned_bench(args)
     print(json.dumps({"metric": "tour gap @ equal wall time, learned top-10 vs k-NN top-20", "value": res["value"],
