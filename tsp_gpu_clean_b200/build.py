@@ -23,6 +23,8 @@ OBJ = os.path.join(PKG, "_build")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
+#: extra nvcc arguments (for example -D tuning constants of the kernels), space-separated
+EXTRA = os.environ.get("TSPB_NVCC_EXTRA", "").split()
 
 
 def _nvcc() -> str:
@@ -55,7 +57,7 @@ def build_library(force: bool = False, verbose: bool = False, jobs: int | None =
   for src in sources():
     obj = os.path.join(OBJ, os.path.basename(src)[:-3] + ".o")
     objs.append(obj)
-    cmd = [nvcc, *ARCH, *FLAGS, "-I", INCLUDE, "-I", CSRC, "-c", src, "-o", obj]
+    cmd = [nvcc, *ARCH, *FLAGS, *EXTRA, "-I", INCLUDE, "-I", CSRC, "-c", src, "-o", obj]
     if verbose:
       cmd.insert(1, "-Xptxas=-v")
       print(" ".join(cmd))

@@ -44,6 +44,13 @@
 
 #include <cooperative_groups.h>
 
+// First mode's incremental restart checks the entries that point into the last move's
+// window (about 30 warp instructions per window position) instead of rescanning the rows
+// before it (about 9 per row); it is taken when RATIO x window length <= the move's row.
+#ifndef TSPB_RESTART_RATIO
+#define TSPB_RESTART_RATIO 2
+#endif
+
 #include "two_opt.cuh"
 
 namespace tspb {
@@ -235,6 +242,13 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
   bool converged = false;  // the last pass found no improving move: a local optimum
   const long long t_start = clock64();
   const bool incremental = MODE == TSPB_MODE_FIRST && T.rev_off != nullptr && T.rev_idx != nullptr;
+  // entry e = a * k + r of the reverse index -> a, as a multiply-high by ceil(2^32 / k):
+  // exact for every e < n k when n k k < 2^32 (else a plain division)
+  const unsigned kmag = (unsigned)(((1ull << 32) + (unsigned)k - 1) / (unsigned)k);
+  const bool kmag_exact = (unsigned long long)n * (unsigned)k * (unsigned)k < (1ull << 32);
+  auto entry_node = [&](int e) -> int {
+    return kmag_exact ? (int)__umulhi((unsigned)e, kmag) : e / k;
+  };
   int win_lo = -1, win_hi = -1;  // window [bi, bj] of the last move (incremental first mode)
 
   while (passes < T.max_iter) {
@@ -254,7 +268,7 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
     int cnt = 0, evals = 0;
     int start_row = 0;        // first row of this pass's scan
     bool found = false;       // the affected entries already hold the first improving one
-    if (incremental && win_lo >= 0 && 2 * (win_hi - win_lo + 1) <= win_lo) {
+    if (incremental && win_lo >= 0 && TSPB_RESTART_RATIO * (win_hi - win_lo + 1) <= win_lo) {
       // affected entries of rows < win_lo: candidate c at a position of the window
       const int lane = tid & 31, wid = tid >> 5;
       constexpr int NW = THREADS / 32;
@@ -264,7 +278,7 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
         const int sc = succ[c], ec = eout[c];
         for (int sx = s0 + lane; sx < s1; sx += 32) {
           const int e = __ldg(T.rev_idx + sx);
-          const int a = e / k;
+          const int a = entry_node(e);
           const int i = pos[a];
           if (i >= win_lo) continue;  // rows from win_lo on are scanned below
           if ((unsigned)(q - (i + 2)) >= (unsigned)(n - (i == 0) - (i + 2))) continue;
@@ -333,7 +347,7 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
           const int c = tour[q];
           const int s0 = __ldg(T.rev_off + c), s1 = __ldg(T.rev_off + c + 1);
           for (int sx = s0 + lane; sx < s1; sx += 32) {
-            const int i = pos[__ldg(T.rev_idx + sx) / k];
+            const int i = pos[entry_node(__ldg(T.rev_idx + sx))];
             if (i < win_lo) rkey[i] = DIRTY;
           }
         }
