@@ -48,7 +48,7 @@
 // window (about 30 warp instructions per window position) instead of rescanning the rows
 // before it (about 9 per row); it is taken when RATIO x window length <= the move's row.
 #ifndef TSPB_RESTART_RATIO
-#define TSPB_RESTART_RATIO 2
+#define TSPB_RESTART_RATIO 3
 #endif
 
 #include "two_opt.cuh"
@@ -282,11 +282,13 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
           const int i = pos[a];
           if (i >= win_lo) continue;  // rows from win_lo on are scanned below
           if ((unsigned)(q - (i + 2)) >= (unsigned)(n - (i == 0) - (i + 2))) continue;
-          ++evals;
           const int dac = PACKED ? (int)(__ldg(packed + e) >> 16) : (cdist ? __ldg(cdist + e) : ds(a, c));
+          const int lbe = (dac - eout[a]) - ec;
+          if (lbe >= 0) continue;  // cannot improve whatever d(succ a, succ c) is
+          ++evals;
           const int sa = succ[a];
           const int dbd = dist ? __ldcg(dist + ((unsigned)sa * stride + (unsigned)sc)) : ds(sa, sc);
-          if ((dac - eout[a]) + (dbd - ec) < 0) atomicMin(&S.first, (unsigned)(i * k + (e - a * k)));
+          if (lbe + dbd < 0) atomicMin(&S.first, (unsigned)(i * k + (e - a * k)));
         }
       }
       __syncthreads();
@@ -308,7 +310,10 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
         for (int u = 0; u < U; ++u) {
           c[u] = (int)(w[u] & 0xffffu);
           ok[u] = (unsigned)c[u] < (unsigned)n && (unsigned)(pos[c[u]] - lo) < span;
-          if (ok[u]) sc[u] = succ[c[u]];
+          if (ok[u]) {
+            sc[u] = succ[c[u]];
+            ok[u] = ((int)(w[u] >> 16) - ea) - eout[c[u]] < 0;  // only improving entries hold keys
+          }
         }
 #pragma unroll
         for (int u = 0; u < U; ++u)
@@ -410,13 +415,20 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
           const int lo = gi + 2;
           const unsigned span = (unsigned)(n - (gi == 0) - lo);
           bool ok[U];
-          int c[U], sc[U];
+          int c[U], sc[U], lb[U];
+          const int bound = MODE == TSPB_MODE_BEST ? bgain : 0;
 #pragma unroll
           for (int u = 0; u < U; ++u) {
             c[u] = (int)(w[u] & 0xffffu);
             ok[u] = (unsigned)c[u] < (unsigned)n && (unsigned)(pos[c[u]] - lo) < span;
             if (MODE == TSPB_MODE_BEST) cnt += ok[u];
-            if (ok[u]) sc[u] = succ[c[u]];
+            if (ok[u]) {
+              sc[u] = succ[c[u]];
+              // gain >= lb (the gathered distance is >= 0): an entry whose lb cannot beat
+              // this thread's bound is settled without its L2 gather
+              lb[u] = ((int)(w[u] >> 16) - ea) - eout[c[u]];
+              ok[u] = lb[u] < bound;
+            }
           }
           int dbd[U];
 #pragma unroll
@@ -426,7 +438,7 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
           for (int u = 0; u < U; ++u) {
             if (!ok[u]) continue;
             ++evals;
-            const int gain = ((int)(w[u] >> 16) - ea) + (dbd[u] - eout[c[u]]);
+            const int gain = lb[u] + dbd[u];
             if (MODE == TSPB_MODE_BEST) {
               if (gain < bgain) {
                 bgain = gain;
@@ -480,7 +492,8 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
         }
       }
       bool ok[U];
-      int sa[U], sc[U];
+      int sa[U], sc[U], lb[U];
+      const int bound = MODE == TSPB_MODE_BEST ? bgain : 0;
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         ok[u] = false;
@@ -492,6 +505,9 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
         if (ok[u]) {
           sa[u] = succ[a[u]];
           sc[u] = succ[c[u]];
+          const int dac = (PACKED || cd[u] >= 0) ? cd[u] : ds(a[u], c[u]);
+          lb[u] = (dac - eout[a[u]]) - eout[c[u]];  // gain >= lb: skip the gather when lb cannot win
+          ok[u] = lb[u] < bound;
         }
       }
       int dbd[U];
@@ -502,8 +518,7 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
       for (int u = 0; u < U; ++u) {
         if (!ok[u]) continue;
         ++evals;
-        const int dac = (PACKED || cd[u] >= 0) ? cd[u] : ds(a[u], c[u]);
-        const int gain = (dac - eout[a[u]]) + (dbd[u] - eout[c[u]]);
+        const int gain = lb[u] + dbd[u];
         if (MODE == TSPB_MODE_BEST) {
           if (gain < bgain) {
             bgain = gain;
