@@ -154,7 +154,7 @@ def test_batch_chapter4_runs_of_mixed_sizes_match_oracle(torch_mod, skip_converg
   """Instances of sizes across several buckets, Chapter-4 configuration, each run equal to
   the oracle GA (random init, OX, swap, 2-opt on every child) with its own seed. With the
   reverse k-NN index (incremental "on") best mode recomputes only the rows a move can
-  change: fewer gains evaluated than the pairs the reference scans, the same runs."""
+  change; the same runs either way."""
   from tsp_gpu_clean_b200 import instances
   from tsp_gpu_clean_b200.batch import FusedBatchSolver
   from tsp_gpu_clean_b200.fused import LocalSearchConfig
@@ -170,10 +170,9 @@ def test_batch_chapter4_runs_of_mixed_sizes_match_oracle(torch_mod, skip_converg
   results = solver.evolve(ctxs, G, patience=10**9)
   assert all(b.incremental == (incremental == "on") for b in solver.buckets)
   tot = solver.two_opt_totals
-  if incremental == "on":
-    assert tot["evaluated"] < tot["pairs"]
-  else:
-    assert tot["evaluated"] == tot["pairs"]
+  # gains computed: below the pairs scanned either way (an entry whose lower bound cannot
+  # improve is settled without its gather); with the reverse index also fewer rows rescanned
+  assert 0 < tot["evaluated"] < tot["pairs"]
   for j, ((best, stats), c) in enumerate(zip(results, coords)):
     cache = {}
 
