@@ -621,6 +621,16 @@ int tspb_edge_features(const double* coords, int32_t n, const int32_t* pool, int
 int tspb_mlp_infer(const float* params, const uint16_t* x, int64_t num_edges, float* logits, void* stream);
 int tspb_mlp_train_grad(const float* params, const uint16_t* x, const float* labels, int64_t num_edges,
                         float* grad, float* loss, void* stream);
+/*
+ * tspb_mlp_train_grad on the fifth-generation tensor cores (tcgen05, accumulators in tensor
+ * memory): the same gradient, with the hidden-layer products, the back-propagation
+ * product and the weight-gradient sums over the batch as tcgen05 MMAs on 128-edge tiles.
+ * One more rounding point than tspb_mlp_train_grad: dh1 enters dW1 and db1 in BF16. x must
+ * be 16-byte aligned. status (optional) receives TSPB_ERR_BUDGET if an MMA completion wait
+ * runs out (about a second). No reference counterpart (the reference has no learned lists).
+ */
+int tspb_mlp_train_grad_tc(const float* params, const uint16_t* x, const float* labels, int64_t num_edges,
+                           float* grad, float* loss, int32_t* status, void* stream);
 int tspb_mlp_adam(float* params, float* grad, float* m, float* v, int32_t step, float lr, float beta1,
                   float beta2, float eps, float weight_decay, void* stream);
 int tspb_select_topk(const int32_t* pool, const float* scores, int32_t n, int32_t pool_k, int32_t k,

@@ -42,8 +42,9 @@ def forward(p: np.ndarray, x: np.ndarray):
   return xb, h1, h2, logit.astype(np.float32)
 
 
-def grads(p: np.ndarray, x: np.ndarray, y: np.ndarray):
-  """d(mean BCE with logits)/dp and the summed loss."""
+def grads(p: np.ndarray, x: np.ndarray, y: np.ndarray, dh1_bf16: bool = False):
+  """d(mean BCE with logits)/dp and the summed loss. `dh1_bf16`: dh1 enters dW1 and db1
+  rounded to BF16, as in the tensor-core (tcgen05) training kernel of `csrc/mlp_tc.cu`."""
   W1, b1, W2, b2, w3, b3 = unpack(p.astype(np.float32))
   xb, h1, h2, logit = forward(p, x)
   E = x.shape[0]
@@ -51,6 +52,8 @@ def grads(p: np.ndarray, x: np.ndarray, y: np.ndarray):
   d = ((prob - y) / E).astype(np.float32)
   dh2 = bf16(d[:, None] * bf16(w3)[None, :] * (h2 > 0))
   dh1 = (dh2 @ bf16(W2).T) * (h1 > 0)
+  if dh1_bf16:
+    dh1 = bf16(dh1.astype(np.float32))
   g = np.zeros(COUNT, dtype=np.float64)
   g[O_W1 : O_W1 + F * H] = (xb[:, :F].T.astype(np.float64) @ dh1).ravel()
   g[O_B1:O_W2] = dh1.sum(0)

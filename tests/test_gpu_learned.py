@@ -150,3 +150,46 @@ def test_iterated_two_opt_under_a_budget():
   assert np.array_equal(np.sort(t), np.arange(400))
   D = odist.euc2d_matrix(coords)
   assert int(D[t, np.roll(t, -1)].sum()) == int(res["length"])
+
+
+@pytest.mark.parametrize("E", [128, 3001, 70000])
+def test_tensor_core_gradient_matches_oracle_and_mma_sync_kernel(torch_mod, E):
+  """The tcgen05 training gradient (tensor-memory accumulators, 128-edge tiles, partial last
+  tile) against the NumPy oracle with its rounding points (dh1 in BF16 for dW1/db1) and
+  against the mma.sync kernel, within the tolerances of the oracle test above."""
+  torch = torch_mod
+  from tsp_gpu_clean_b200 import native
+  from tsp_gpu_clean_b200.device import ptr, stream_handle
+  from tsp_gpu_clean_b200.learned import EdgeScorer
+
+  rng = np.random.default_rng(11 + E)
+  feats = rng.uniform(-2, 2, (E, 5)).astype(np.float32)
+  x = np.zeros((E, 16), dtype=np.float32)
+  x[:, :5] = feats
+  y = (rng.random(E) < 0.2).astype(np.float32)
+  sc = EdgeScorer(seed=5)
+  p = sc.params.cpu().numpy()
+  p[omlp.O_B1 : omlp.O_W2] = rng.normal(0, 0.1, 64)
+  p[omlp.O_B2 : omlp.O_W3] = rng.normal(0, 0.1, 64)
+  sc.params.copy_(torch.from_numpy(p))
+  xb16 = (omlp.bf16(x).view(np.uint32) >> 16).astype(np.uint16).view(np.int16)
+  dx = torch.from_numpy(xb16.copy()).cuda()
+  dy = torch.from_numpy(y).cuda()
+  out = {}
+  for name in ("tspb_mlp_train_grad_tc", "tspb_mlp_train_grad"):
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    grad = torch.zeros_like(sc.params)
+    if name.endswith("_tc"):
+      status = torch.zeros(1, dtype=torch.int32, device="cuda")
+      native.call(name, ptr(sc.params), ptr(dx), ptr(dy), E, ptr(grad), ptr(loss), ptr(status), stream_handle())
+      assert int(status.item()) == 0
+    else:
+      native.call(name, ptr(sc.params), ptr(dx), ptr(dy), E, ptr(grad), ptr(loss), stream_handle())
+    out[name] = (grad.cpu().numpy(), float(loss.item()))
+  g_tc, l_tc = out["tspb_mlp_train_grad_tc"]
+  g_mma, _ = out["tspb_mlp_train_grad"]
+  g_want, l_want = omlp.grads(p, x, y, dh1_bf16=True)
+  scale = np.abs(g_want).max()
+  np.testing.assert_allclose(g_tc, g_want, rtol=0, atol=3e-3 * scale)
+  np.testing.assert_allclose(g_tc, g_mma, rtol=0, atol=3e-3 * scale)
+  assert abs(l_tc - l_want) <= 1e-3 * abs(l_want)

@@ -21,19 +21,9 @@
 #include <cuda_bf16.h>
 
 #include "common.cuh"
+#include "mlp.cuh"
 
 namespace tspb {
-
-constexpr int MLP_F = 5;    // features per edge
-constexpr int MLP_KX = 16;  // padded input width (one k-tile)
-constexpr int MLP_H = 64;   // hidden width
-constexpr int OFF_W1 = 0;
-constexpr int OFF_B1 = OFF_W1 + MLP_KX * MLP_H;
-constexpr int OFF_W2 = OFF_B1 + MLP_H;
-constexpr int OFF_B2 = OFF_W2 + MLP_H * MLP_H;
-constexpr int OFF_W3 = OFF_B2 + MLP_H;
-constexpr int OFF_B3 = OFF_W3 + MLP_H;
-constexpr int MLP_PARAMS = OFF_B3 + 1;
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);

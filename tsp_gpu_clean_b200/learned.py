@@ -199,6 +199,10 @@ class EdgeScorer:
     self.m = torch.zeros_like(self.params)
     self.v = torch.zeros_like(self.params)
     self.step = 0
+    #: gradient on the tcgen05 tensor cores (accumulators in tensor memory); False: the
+    #: mma.sync kernel with the same rounding points except dh1, kept as its cross-check
+    self.tensor_cores = True
+    self._status = torch.zeros(1, dtype=torch.int32, device="cuda")
 
   def logits(self, x: "torch.Tensor") -> "torch.Tensor":
     E = int(x.shape[0])
@@ -209,10 +213,16 @@ class EdgeScorer:
   def train_step(self, x: "torch.Tensor", y: "torch.Tensor", lr: float = 3e-3) -> float:
     loss = torch.zeros(1, dtype=torch.float32, device="cuda")
     E = int(x.shape[0])
-    _call("tspb_mlp_train_grad", ptr(self.params), ptr(x), ptr(y), E, ptr(self.grad), ptr(loss), stream_handle())
+    if self.tensor_cores:
+      _call("tspb_mlp_train_grad_tc", ptr(self.params), ptr(x), ptr(y), E, ptr(self.grad), ptr(loss),
+            ptr(self._status), stream_handle())
+    else:
+      _call("tspb_mlp_train_grad", ptr(self.params), ptr(x), ptr(y), E, ptr(self.grad), ptr(loss), stream_handle())
     self.step += 1
     _call("tspb_mlp_adam", ptr(self.params), ptr(self.grad), ptr(self.m), ptr(self.v), self.step, lr, 0.9, 0.999, 1e-8,
           0.0, stream_handle())
+    if self.tensor_cores and int(self._status.item()) != 0:
+      raise RuntimeError(f"tspb_mlp_train_grad_tc: {native.status_text(int(self._status.item()))}")
     return float(loss.item()) / max(E, 1)
 
 

@@ -73,6 +73,7 @@ SIGNATURES: dict[str, tuple] = {
   "tspb_edge_features": (ctypes.c_int, [_p, _i32, _p, _i32, _p, _i64, _p, _p, _p, _p]),
   "tspb_mlp_infer": (ctypes.c_int, [_p, _p, _i64, _p, _p]),
   "tspb_mlp_train_grad": (ctypes.c_int, [_p, _p, _p, _i64, _p, _p, _p]),
+  "tspb_mlp_train_grad_tc": (ctypes.c_int, [_p, _p, _p, _i64, _p, _p, _p, _p]),
   "tspb_mlp_adam": (ctypes.c_int, [_p, _p, _p, _p, _i32, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                    ctypes.c_float, _p]),
   "tspb_select_topk": (ctypes.c_int, [_p, _p, _i32, _i32, _i32, _p, _p]),
