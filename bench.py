@@ -60,13 +60,14 @@ K_CAND = 20
 ALG_BYTES_PER_DELTA = 12
 ALG_OPS_PER_DELTA = 12
 L2_FLUSH_BYTES = 256 << 20
-#: Per evaluated gain of the scan kernel with 128-thread CTAs on this workload's tours
-#: (counted launches, first 256 tours of the batch), from one ncu capture:
-#: warp instructions executed (sm__inst_executed.sum), L2 sector bytes
-#: (lts__t_bytes.sum) and DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum,
-#: per 1024-tour launch).
+#: Per gain the scan kernel computed (128-thread CTAs, the uncounted launch of first mode,
+#: the best-mode launch), from one ncu capture on the first 256 tours of the batch: warp
+#: instructions executed (sm__inst_executed.sum), L2 sector bytes (lts__t_bytes.sum), and
+#: DRAM bytes read + written scaled to a 1024-tour launch (the tours' 4 KB each is the part
+#: that grows). A gain is computed only for entries whose lower bound could improve.
 NCU_PER_GAIN: dict[str, dict[str, float]] = {
-  "first": {"inst": 4.380, "lts_bytes": 38.30, "dram_bytes_per_launch": 8_556_800},
+  "first": {"inst": 8.327, "lts_bytes": 45.25, "dram_bytes_per_launch": 8_298_496},
+  "best": {"inst": 9.030, "lts_bytes": 33.36, "dram_bytes_per_launch": 8_215_040},
 }
 #: CPU parity sample: tours of the timed batch refined by the oracle (at least this many)
 PARITY_TOURS = 16
@@ -805,6 +806,80 @@ def main_uneven(args) -> int:
   return 0
 
 
+#: Algorithmic FLOPs of one edge's training gradient: the three row-wise products
+#: (x W1 with K padded to 16, h1 W2, dh2 W2^T) and the sums over edges for dW2 and dW1.
+MLP_FLOPS_PER_EDGE = 2 * (16 * 64 + 64 * 64 + 64 * 64 + 64 * 64 + 16 * 64)
+
+
+def main_mlp_train(args) -> int:
+  """Training-gradient throughput of the edge-scoring MLP: the tcgen05 kernel (accumulators
+  in tensor memory) against the mma.sync kernel, on one synthetic batch of 65,536 edges
+  (the training batch of the learned-candidate workload), CUDA-event timed."""
+  import torch
+
+  from tsp_gpu_clean_b200 import native
+  from tsp_gpu_clean_b200.build import build_library
+  from tsp_gpu_clean_b200.device import ptr, stream_handle
+  from tsp_gpu_clean_b200.learned import EdgeScorer
+
+  build_library()
+  E = args.mlp_edges
+  rng = np.random.default_rng(7)
+  x = np.zeros((E, 16), dtype=np.float32)
+  x[:, :5] = rng.uniform(-2, 2, (E, 5))
+  xb = (x.view(np.uint32) >> 16).astype(np.uint16)  # truncation suffices for synthetic inputs
+  dx = torch.from_numpy(xb.view(np.int16).copy()).cuda()
+  dy = torch.from_numpy((rng.random(E) < 0.1).astype(np.float32)).cuda()
+  sc = EdgeScorer(seed=1)
+  grad = torch.zeros_like(sc.params)
+  loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+  status = torch.zeros(1, dtype=torch.int32, device="cuda")
+  lib = native.load_library()
+
+  def launch(tc: bool):
+    if tc:
+      rc = lib.tspb_mlp_train_grad_tc(ptr(sc.params), ptr(dx), ptr(dy), E, ptr(grad), ptr(loss), ptr(status),
+                                      stream_handle())
+    else:
+      rc = lib.tspb_mlp_train_grad(ptr(sc.params), ptr(dx), ptr(dy), E, ptr(grad), ptr(loss), stream_handle())
+    native.check("mlp train", rc)
+
+  res = {}
+  for name, tc in (("tcgen05", True), ("mma_sync", False)):
+    for _ in range(args.warmup):
+      launch(tc)
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(args.steps):
+      e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+      e0.record()
+      launch(tc)
+      e1.record()
+      e1.synchronize()
+      ms.append(e0.elapsed_time(e1))
+    res[name] = statistics.median(ms)
+  if int(status.item()) != 0:
+    raise RuntimeError("tcgen05 kernel reported a completion wait that ran out")
+  peak = 1590.0  # dense BF16 TFLOP/s: MEASURED_PEAKS.json when present, else the pool's fallback
+  src = "fallback"
+  path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+  if os.path.exists(path):
+    with open(path) as fh:
+      d = json.load(fh)
+    if "bf16_tflops" in d:
+      peak, src = float(d["bf16_tflops"]), "measured"
+  tf = {k: E * MLP_FLOPS_PER_EDGE / (v / 1e3) / 1e12 for k, v in res.items()}
+  print(json.dumps({"metric": "MLP training-gradient edges/s", "value": E / (res["tcgen05"] / 1e3), "unit": "edges/s",
+                    "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                    "dtype": "bf16 operands, fp32 accumulate", "data": "synthetic (seeded)",
+                    "config": {"workload": "edge-scoring MLP 5(16)-64-64-1 training gradient, one batch", "edges": E},
+                    "ms": res, "tflops": tf,
+                    "roofline": {"bound": "tensor", "achieved": tf["tcgen05"], "peak": peak, "unit": "TFLOP/s",
+                                 "frac": tf["tcgen05"] / peak, "peak_source": src,
+                                 "basis": f"{MLP_FLOPS_PER_EDGE} algorithmic FLOPs per edge"}}))
+  return 0
+
+
 def run_learned_bench(args) -> dict:
   """Learned top-10 vs k-NN top-20 candidates for 2-opt at equal wall time.
 
@@ -1062,7 +1137,9 @@ def main(argv=None) -> int:
   ap.add_argument("--cpu-workers", type=int, default=0, help="0: all host cores, capped at 64")
   ap.add_argument("--no-cpu-baseline", action="store_true")
   ap.add_argument("--no-ga", action="store_true", help="two_opt: leave out the ga1000 sub-result")
-  ap.add_argument("--workload", default="two_opt", choices=["two_opt", "learned", "uneven", "or_opt", *GA_WORKLOADS])
+  ap.add_argument("--workload", default="two_opt",
+                  choices=["two_opt", "learned", "uneven", "or_opt", "mlp_train", *GA_WORKLOADS])
+  ap.add_argument("--mlp-edges", type=int, default=1 << 16, help="mlp_train: edges in the batch")
   ap.add_argument("--instances", type=int, default=256, help="uneven: instances in the batch")
   ap.add_argument("--generations", type=int, default=100, help="uneven: generations")
   ap.add_argument("--train-instances", type=int, default=2000)
@@ -1098,6 +1175,8 @@ def main(argv=None) -> int:
     return 0
   if args.workload == "uneven":
     return main_uneven(args)
+  if args.workload == "mlp_train":
+    return main_mlp_train(args)
   if args.workload == "or_opt":
     return main_or_opt(args)
   if args.workload != "two_opt":
