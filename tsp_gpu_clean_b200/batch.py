@@ -451,7 +451,32 @@ class FusedBatchSolver:
     st_ref = ctypes.byref(self.state)
     return self._timed(lambda: self._offspring(st_ref, b, threads))
 
-  def _draw_tapes(self, rngs: list, ns: list[int]) -> None:
+  def _host_tapes(self, rngs: list, ns: list[int]) -> bool:
+    """Whether this batch draws its tapes on the host (a few runs; any bit generator)."""
+    gens_pcg = all(native.Pcg64.from_state(r.bit_generator.state) is not None for r in rngs)
+    return self.G > 0 and not (gens_pcg and self.I >= DEVICE_TAPE_MIN_RUNS)
+
+  def _start_host_tapes(self, rngs: list, ns: list[int]):
+    """Start the host draws of every run's tape in a thread; None when the device draws."""
+    if not self._host_tapes(rngs, ns):
+      return None
+    import threading
+
+    G, P, kt = self.G, self.P, self.kt
+    job = {"tapes": [None] * len(rngs), "error": None}
+
+    def work():
+      try:
+        for i, (r, n) in enumerate(zip(rngs, ns)):
+          job["tapes"][i] = draw_generation_tape(r, G, P, kt, n)
+      except BaseException as exc:  # re-raised by the caller
+        job["error"] = exc
+
+    job["thread"] = threading.Thread(target=work, daemon=True)
+    job["thread"].start()
+    return job
+
+  def _draw_tapes(self, rngs: list, ns: list[int], job=None) -> None:
     """Every run's random tape, drawn on the device by `tspb_tape_draw` (one thread per run,
     NumPy's PCG64 stream restated) when every generator is PCG64, else by NumPy on the host.
     Each generator ends in the state it has after the reference draws G generations."""
@@ -463,11 +488,17 @@ class FusedBatchSolver:
                  torch.empty((I, G, P), dtype=torch.float64, device=dev),
                  torch.empty((I, G, P), dtype=torch.int32, device=dev),
                  torch.empty((I, G, P), dtype=torch.int32, device=dev)]
-    gens = [native.Pcg64.from_state(r.bit_generator.state) for r in rngs]
     self._dev_states = None
     self.states = []
     if G == 0:
       return
+    if job is not None:  # the host draws already running: no generator is read before they end
+      job["thread"].join()
+      if job["error"] is not None:
+        raise job["error"]
+      self._store_host_tapes(job["tapes"])
+      return
+    gens = [native.Pcg64.from_state(r.bit_generator.state) for r in rngs]
     # one device thread per run pays only with many runs; a few runs draw faster on the host
     if all(g is not None for g in gens) and I >= DEVICE_TAPE_MIN_RUNS:
       h_gens = (native.Pcg64 * I)(*gens)
@@ -481,9 +512,12 @@ class FusedBatchSolver:
       for r, g in zip(rngs, final):
         r.bit_generator.state = g.to_state()
       return
+    self._store_host_tapes([draw_generation_tape(r, G, P, kt, n) for r, n in zip(rngs, ns)])
+
+  def _store_host_tapes(self, drawn) -> None:
+    """Copy the host-drawn tapes (one (arrays, states) pair per run) to the device tape."""
     host = [np.empty(tuple(t.shape), dtype=np.float64 if t.dtype == torch.float64 else np.int32) for t in self.tape]
-    for i, (r, n) in enumerate(zip(rngs, ns)):
-      tape, states = draw_generation_tape(r, G, P, kt, n)
+    for i, (tape, states) in enumerate(drawn):
       for h, a in zip(host, tape):
         h[i] = a
       self.states.append(states)
@@ -602,8 +636,12 @@ class FusedBatchSolver:
     rebuildable = []
     t_ops = t_tape = 0.0
     all_tabs = []
-    for i, (ctx, n, rng) in enumerate(zip(contexts, ns, rngs)):
+    for i, rng in enumerate(rngs):
       seeds_all[i] = draw_row_seeds(rng, P)  # nearest_neighbor_init.py:118-121, random_init.py:42
+    # every generator's next draws are its generations' tape: a few runs draw it on the
+    # host, in a thread (the C++ draw releases the GIL) while the operands are built here
+    tape_job = self._start_host_tapes(rngs, ns)
+    for i, (ctx, n, rng) in enumerate(zip(contexts, ns, rngs)):
       if self.init == "nn":
         nn_tables.append(np.ascontiguousarray(candidate_list(ctx, self.nn_k), dtype=np.int32))
       t0 = time.perf_counter()
@@ -647,7 +685,7 @@ class FusedBatchSolver:
     else:
       self._random_init(h_jobs, seeds_all, ns)
     t1 = time.perf_counter()
-    self._draw_tapes(rngs, ns)  # after the row seeds, like the reference
+    self._draw_tapes(rngs, ns, tape_job)  # after the row seeds, like the reference
     t_nn, t_tape = t1 - t0, time.perf_counter() - t1
     self.h_inst = h_inst
     self.d_inst = torch.frombuffer(bytearray(h_inst), dtype=torch.uint8).cuda()
