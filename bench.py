@@ -35,6 +35,7 @@ from __future__ import annotations
 
 import argparse
 import gc
+import hashlib
 import json
 import multiprocessing as mp
 import os
@@ -101,17 +102,33 @@ def _cpu_worker(args):
   return out, time.perf_counter() - t0
 
 
+def _ref_worker(args):
+  """Refine one tour in best then first mode with the reference's own CPU 2-opt (installed
+  under baseline/_ref). Returns ({mode: (tour, (passes, pairs))}, seconds of refinement)."""
+  coords, tour = args
+  from baseline import reference_arm
+
+  return reference_arm.two_opt_worker((coords, tour, MODES, K_CAND))
+
+
+def cpu_path() -> tuple[str, object]:
+  """The CPU 2-opt to time: the reference itself when it is installed, else the oracle port."""
+  from baseline import reference_arm
+
+  return ("reference", _ref_worker) if reference_arm.import_root() is not None else ("port", _cpu_worker)
+
+
 def parity_indices(tours: int, count: int) -> list[int]:
   """`count` tour indices spread evenly over a batch of `tours` (first and last included)."""
   return sorted({int(round(v)) for v in np.linspace(0, tours - 1, min(count, tours))})
 
 
-def cpu_sample(pool, tours_np: np.ndarray, indices) -> dict:
-  """Oracle deltas/s over the given tours of the batch in parallel (one tour per process),
+def cpu_sample(pool, tours_np: np.ndarray, indices, worker=_cpu_worker) -> dict:
+  """CPU deltas/s over the given tours of the batch in parallel (one tour per process),
   with each tour's refined result per mode for the parity check."""
   coords, _ = instances.two_opt_workload(tours=1)
   t0 = time.perf_counter()
-  res = pool.map(_cpu_worker, [(coords, tours_np[i]) for i in indices])
+  res = pool.map(worker, [(coords, tours_np[i]) for i in indices])
   wall = time.perf_counter() - t0
   pairs = sum(st[1] for out, _ in res for _, st in out.values())
   return {"value": pairs / wall, "pairs": pairs, "wall_s": wall, "tours": len(indices),
@@ -119,29 +136,71 @@ def cpu_sample(pool, tours_np: np.ndarray, indices) -> dict:
           "results": [out for out, _ in res]}
 
 
-def cpu_one_core(pool, tours_np: np.ndarray, index: int) -> dict:
-  """The same oracle on one tour with no other worker busy: deltas/s of one host core."""
+def cpu_one_core(pool, tours_np: np.ndarray, index: int, worker=_cpu_worker) -> dict:
+  """The same CPU 2-opt on one tour with no other worker busy: deltas/s of one host core."""
   coords, _ = instances.two_opt_workload(tours=1)
-  out, secs = pool.apply(_cpu_worker, ((coords, tours_np[index]),))
+  out, secs = pool.apply(worker, ((coords, tours_np[index]),))
   pairs = sum(st[1] for _, st in out.values())
   return {"value": pairs / secs, "pairs": pairs, "seconds": secs, "tours_per_s": len(MODES) / secs, "tour": index}
 
 
-def check_parity(gpu: dict, cpu: dict) -> dict:
-  """Compare the oracle's refinements with the GPU's counted launch at the same indices."""
+def refined_digest(results: list, modes=MODES) -> str:
+  """sha256 over the refined tours of each sampled tour, mode by mode (equal digests from
+  two arms mean identical refinements)."""
+  h = hashlib.sha256()
+  for out in results:
+    for m in modes:
+      h.update(np.ascontiguousarray(out[m][0], dtype=np.int32).tobytes())
+  return h.hexdigest()
+
+
+def check_parity(gpu: dict, cpu: dict, kind: str = "port") -> dict:
+  """Compare the CPU refinements (the reference's or the oracle's) with the GPU's counted
+  launch at the same indices."""
   bad = []
   for i, out in zip(cpu["indices"], cpu["results"]):
     for m, (tour, st) in out.items():
       g_tour, g_st = gpu[m]
       if not np.array_equal(g_tour[i], tour):
         bad.append(f"{m} tour {i}: tours differ")
-      elif tuple(int(v) for v in g_st[i][:3]) != st:
-        bad.append(f"{m} tour {i}: (passes, pairs, moves) {tuple(int(v) for v in g_st[i][:3])} vs {st}")
+      elif tuple(int(v) for v in g_st[i][: len(st)]) != tuple(st):
+        bad.append(f"{m} tour {i}: (passes, pairs[, moves]) {tuple(int(v) for v in g_st[i][:len(st)])} vs {st}")
   n = len(cpu["indices"])
   total = len(next(iter(gpu.values()))[0])
-  return {"ok": not bad, "text": (f"bit-exact on {n}/{total} tours (both modes: tours, passes, pairs, moves)" if not bad
-                                  else f"MISMATCH on {len(bad)} of {n * len(MODES)} refinements"),
+  what = "the reference's CPU 2-opt" if kind == "reference" else "the oracle port"
+  return {"ok": not bad, "text": (f"bit-exact against {what} on {n}/{total} tours (both modes: tours, passes, pairs)"
+                                  if not bad else f"MISMATCH on {len(bad)} of {n * len(MODES)} refinements"),
           "mismatches": bad[:8]}
+
+
+class GcWatch:
+  """Time spent in Python's cyclic garbage collector while the block runs, per generation
+  (collections pause the host thread that enqueues the GPU work)."""
+
+  def __enter__(self):
+    self.ms = [0.0, 0.0, 0.0]
+    self.count = [0, 0, 0]
+    self._t0 = None
+
+    def cb(phase, info):
+      if phase == "start":
+        self._t0 = time.perf_counter()
+      elif self._t0 is not None:
+        g = int(info.get("generation", 0))
+        self.ms[g] += 1e3 * (time.perf_counter() - self._t0)
+        self.count[g] += 1
+        self._t0 = None
+
+    self._cb = cb
+    gc.callbacks.append(cb)
+    return self
+
+  def __exit__(self, *exc):
+    gc.callbacks.remove(self._cb)
+    return False
+
+  def summary(self) -> dict:
+    return {"collections": self.count, "ms": [round(v, 2) for v in self.ms]}
 
 
 # ------------------------------------------------------------------------------ clocks
@@ -477,13 +536,20 @@ def ga_options(name: str) -> dict:
 
 
 def _ga_cpu_gens_per_s(name: str, sample_gens: int) -> dict:
-  """Oracle GA (NumPy restatement of the reference GA) generations/s on one core."""
-  from oracle import distances as odist
-  from oracle import ga as oga
-
+  """GA generations/s on one core: the reference's own `GeneticAlgorithm.evolve` with its
+  CPU strategies when it is installed (baseline/_ref), else the oracle GA (the NumPy
+  restatement of the same GA, pinned to the reference's recorded runs)."""
   n, P, G, elite, post_init, seed, _ = GA_WORKLOADS[name]
   o = ga_options(name)
   coords = instances.uniform_instance(n, seed)
+  if cpu_path()[0] == "reference":
+    from baseline import reference_arm
+
+    r = reference_arm.ga_gens_per_s(coords, P, elite, post_init, sample_gens, o)
+    return {**r, "kind": "reference", "what": "the reference's GeneticAlgorithm.evolve with its CPU strategies"}
+  from oracle import distances as odist
+  from oracle import ga as oga
+
   D = odist.euc2d_matrix(coords)
   cache = {}
 
@@ -503,7 +569,7 @@ def _ga_cpu_gens_per_s(name: str, sample_gens: int) -> dict:
   t2 = time.perf_counter()
   loop = max((t2 - t1) - (t1 - t0), 1e-9)
   return {"value": sample_gens / loop, "gens": sample_gens, "loop_s": loop,
-          "history": [float(v) for v in res[3]["convergence_history"]]}
+          "history": [float(v) for v in res[3]["convergence_history"]], "kind": "port", "what": "the NumPy GA"}
 
 
 def _ga_cpu_sample(name: str, sample_gens: int) -> dict:
@@ -513,16 +579,16 @@ def _ga_cpu_sample(name: str, sample_gens: int) -> dict:
   reps = ga_options(name)["reps"]
   if reps == 1:
     r = _ga_cpu_gens_per_s(name, sample_gens)
-    return {"value": r["value"], "cores": 1, "loop_s": r["loop_s"], "history": r["history"],
-            "sample": f"{sample_gens} generations of the NumPy GA (init excluded), {r['loop_s']:.1f} s"}
+    return {"value": r["value"], "cores": 1, "loop_s": r["loop_s"], "history": r["history"], "kind": r["kind"],
+            "sample": f"{sample_gens} generations of {r['what']} (init excluded), {r['loop_s']:.1f} s"}
   import multiprocessing as mp
 
   workers = max(1, min(reps, os.cpu_count() or 1, 64))
   with mp.get_context("spawn").Pool(workers) as pool:
     res = pool.starmap(_ga_cpu_gens_per_s, [(name, sample_gens)] * reps)
   busy = sum(r["loop_s"] for r in res) / workers
-  return {"value": reps * sample_gens / busy, "cores": workers, "loop_s": busy,
-          "sample": f"{reps} runs x {sample_gens} generations of the NumPy GA (init excluded) on {workers} "
+  return {"value": reps * sample_gens / busy, "cores": workers, "loop_s": busy, "kind": res[0]["kind"],
+          "sample": f"{reps} runs x {sample_gens} generations of {res[0]['what']} (init excluded) on {workers} "
                     f"processes, {busy:.1f} s per process"}
 
 
@@ -580,11 +646,14 @@ def ga_measure(workload: str, warmup: int, steps: int, world: int, rank: int, en
     run_once()
   torch.cuda.synchronize()
   _barrier(world)
-  loop_ms, walls, launches, gens = [], [], 0, 0
-  with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+  loop_ms, walls, launches, gens, phases = [], [], 0, 0, []
+  with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks, GcWatch() as gcw:
     for _ in range(steps):
+      solver = stats = None  # the previous run's buffers are released before the next timed call
       solver, stats, wall = run_once()
       loop_ms.append(solver.last_timing["loop_ms_device"])
+      phases.append({k: round(solver.last_timing[k] * 1e3, 2) for k in ("setup_s", "postinit_s", "capture_s", "loop_s")
+                     if k in solver.last_timing})
       walls.append(wall)
       launches += solver.kernel_launches
       gens += stats["generations_completed"]
@@ -599,6 +668,7 @@ def ga_measure(workload: str, warmup: int, steps: int, world: int, rank: int, en
                   "d2h_bytes_per_step": int(reps * (n * 4 + (G + 1) * 8 + P * n * 4))},
           "gpu_launches": launches, "desc": desc, "best": stats["best_fitness"], "history": stats["history"],
           "loop_ms_steps": [round(v, 3) for v in loop_ms], "walls_s": [round(w, 4) for w in walls],
+          "phase_ms_steps": phases, "gc": gcw.summary(),
           "buckets": [{"n": [b.lo, b.hi], "two_opt_threads": b.two_opt_threads, "incremental": b.incremental, "pair": b.pair,
                        "offspring_threads": b.offspring_threads} for b in getattr(solver, "buckets", [])],
           "two_opt_totals": getattr(solver, "two_opt_totals", None),
@@ -711,11 +781,17 @@ def run_uneven_bench(args) -> dict:
   torch.cuda.synchronize()
   _barrier(world)
   loop_ms, walls, launches, gens, pairs, tune_s, pauses, ties = [], [], 0, 0, 0, 0.0, 0, 0
-  with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+  phases = []
+  with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks, GcWatch() as gcw:
     for _ in range(args.steps):
+      solver = res = None  # the previous run's buffers are released before the next timed call
+      mallocs = torch.cuda.memory_stats().get("segment.all.allocated", 0)
       solver, res, wall = run_once()
       loop_ms.append(solver.last_timing["loop_ms_device"])
       walls.append(wall)
+      phases.append({**{k: round(solver.last_timing[k] * 1e3, 2)
+                        for k in ("setup_s", "setup_operands_s", "postinit_s", "capture_s", "loop_s", "results_s")},
+                     "device_mallocs": torch.cuda.memory_stats().get("segment.all.allocated", 0) - mallocs})
       launches += solver.kernel_launches
       gens += sum(st["generations_completed"] for _, st in res)
       pairs += solver.two_opt_totals["pairs"]
@@ -747,7 +823,7 @@ def run_uneven_bench(args) -> dict:
                                  for b in solver.buckets],
                      "setup_s": solver.last_timing["setup_s"], "tune_s_total": tune_s,
                      "last_run": {k: round(v, 4) for k, v in solver.last_timing.items() if isinstance(v, (int, float))},
-                     "walls_s": [round(w, 4) for w in walls],
+                     "walls_s": [round(w, 4) for w in walls], "gc": gcw.summary(), "phase_ms_steps": phases,
                      "setup_parts_s": {k: round(solver.last_timing[k], 3)
                                        for k in ("setup_operands_s", "setup_tape_s", "setup_nn_init_s")}}}
 
@@ -1079,12 +1155,13 @@ def main_or_opt(args) -> int:
   ls = LocalSearchB200OrOpt(max_iterations=OR_OPT_PASSES, candidate_k=K_CAND, max_segment=OR_OPT_SEGMENT)
   ls.improve_batch(tours_np[:2], ctx)
   walls, e2e_eval = [], 0
-  for _ in range(args.steps):
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    out = ls.improve_batch(tours_np, ctx)
-    walls.append(time.perf_counter() - t0)
-    e2e_eval += int(ls.last_stats[:, 2].sum())
+  with GcWatch() as gcw:
+    for _ in range(args.steps):
+      torch.cuda.synchronize()
+      t0 = time.perf_counter()
+      out = ls.improve_batch(tours_np, ctx)
+      walls.append(time.perf_counter() - t0)
+      e2e_eval += int(ls.last_stats[:, 2].sum())
   assert np.array_equal(out, device_out)
   e2e_units, e2e_s = aggregate(e2e_eval, sum(walls), world)
   _finish_ranks(world)
@@ -1096,7 +1173,8 @@ def main_or_opt(args) -> int:
           "clocks": clocks.summary(),
           "e2e": {"value": e2e_units / e2e_s, "unit": "entries/s", "h2d_bytes_per_step": int(tours_np.nbytes),
                   "d2h_bytes_per_step": int(tours_np.nbytes)},
-          "gpu_launches": launches}
+          "gpu_launches": launches,
+          "detail": {"e2e_walls_s": [round(w, 4) for w in walls], "e2e_gc": gcw.summary()}}
   per_launch = evaluated / len(ms) * OR_OPT_BYTES_PER_ENTRY
   peaks = _peaks()
   achieved = per_launch / (sum(ms) / len(ms) / 1e3) / 1e9
@@ -1199,31 +1277,38 @@ def main(argv=None) -> int:
   if args.impl == "reference":
     if rank != 0:
       return 0
+    kind, worker = cpu_path()
     ctx = mp.get_context("spawn")
     with ctx.Pool(workers) as pool:
-      for w in range(args.warmup):
-        pool.map(_cpu_worker, [(instances.two_opt_workload(tours=1)[0], tours_np[i]) for i in indices[:workers]])
-      vals = [cpu_sample(pool, tours_np, indices) for _ in range(args.steps)]
-      one = cpu_one_core(pool, tours_np, indices[0])
+      small = instances.clustered_instance(60, 4, 30.0, 5)
+      for w in range(args.warmup):  # imports and first calls in every worker, on a 60-city tour
+        pool.map(worker, [(small, instances.random_tours(60, 1, w)[0])] * workers)
+      vals = [cpu_sample(pool, tours_np, indices, worker) for _ in range(args.steps)]
+      one = cpu_one_core(pool, tours_np, indices[0], worker)
       ga_cpu = pool.apply(_ga_cpu_gens_per_s, (GA_SUB_WORKLOAD, sample_gens))
     value = sum(v["pairs"] for v in vals) / sum(v["wall_s"] for v in vals)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * sum(v["wall_s"] for v in vals) / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded)", "impl": "reference", "config": config,
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": kind,
+                             "implementation": ("LocalSearchCPUTourTwoOpt.improve_batch of the installed reference "
+                                                "(baseline/_ref)" if kind == "reference" else "oracle/two_opt.py"),
                              "sample": f"{len(indices)} tours of the batch per step over {workers} processes (one tour "
                                        "per task), best then first mode to a local optimum",
+                             "refined_digest": refined_digest(vals[0]["results"]) if vals else None,
                              "tours_per_s": statistics.mean(v["tours_per_s"] for v in vals),
                              "one_core": {k: one[k] for k in ("value", "tours_per_s", "seconds")}},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "detail": {GA_SUB_WORKLOAD: {"metric": "generations/s", "cpu_one_core": ga_cpu["value"],
-                                         "sample": f"{sample_gens} generations of the NumPy GA on one core, "
+                                         "kind": ga_cpu["kind"],
+                                         "sample": f"{sample_gens} generations of {ga_cpu['what']} on one core, "
                                                    f"{ga_cpu['loop_s']:.1f} s (init excluded)"}}}
     print(json.dumps(line))
     return 0
 
   pool = None
+  kind, worker = cpu_path()
   if rank == 0 and world == 1 and not args.no_cpu_baseline:
     pool = mp.get_context("spawn").Pool(workers)  # before the first CUDA call
   from tsp_gpu_clean_b200.build import build_library
@@ -1237,9 +1322,9 @@ def main(argv=None) -> int:
   _finish_ranks(world)
   cpu = one = ga_cpu = parity = ga_parity = None
   if pool is not None:
-    cpu = cpu_sample(pool, res["tours_np"], indices)
-    parity = check_parity(res["counted"], cpu)
-    one = cpu_one_core(pool, res["tours_np"], indices[0])
+    cpu = cpu_sample(pool, res["tours_np"], indices, worker)
+    parity = check_parity(res["counted"], cpu, kind)
+    one = cpu_one_core(pool, res["tours_np"], indices[0], worker)
     if ga is not None:
       ga_cpu = pool.apply(_ga_cpu_gens_per_s, (GA_SUB_WORKLOAD, sample_gens))
     pool.close()
@@ -1255,12 +1340,18 @@ def main(argv=None) -> int:
                      "evaluated_per_step": res["evaluated_per_step"], "passes_per_step": res["passes_per_step"],
                      "moves_per_step": res["moves_per_step"], "tours_per_s": res["tours_per_s"],
                      "peaks": res["peaks"]}}
+  line["detail"]["refined_digest"] = {
+    "indices": list(indices),
+    "sha256": refined_digest([{m: (res["counted"][m][0][i],) for m in res["counted"]} for i in indices],
+                             [m for m in MODES if m in res["counted"]])}
   if parity is not None:
     line["parity"] = parity["text"]
     if parity["mismatches"]:
       line["detail"]["parity_mismatches"] = parity["mismatches"]
   if cpu is not None:
-    line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": workers, "kind": "port",
+    line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": workers, "kind": kind,
+                            "implementation": ("LocalSearchCPUTourTwoOpt.improve_batch of the installed reference "
+                                               "(baseline/_ref)" if kind == "reference" else "oracle/two_opt.py"),
                             "sample": f"{cpu['tours']} tours of the timed batch (indices spread over it, one per "
                                       f"process), best then first mode to a local optimum, {cpu['wall_s']:.1f} s wall",
                             "tours_per_s": cpu["tours_per_s"],
@@ -1272,14 +1363,15 @@ def main(argv=None) -> int:
            "gpu_launches": ga["gpu_launches"]}
     if ga_cpu is not None:
       sub["cpu_one_core"] = ga_cpu["value"]
-      sub["cpu_sample"] = f"{sample_gens} generations of the NumPy GA on one core, {ga_cpu['loop_s']:.1f} s"
+      sub["cpu_kind"] = ga_cpu["kind"]
+      sub["cpu_sample"] = f"{sample_gens} generations of {ga_cpu['what']} on one core, {ga_cpu['loop_s']:.1f} s"
       sub["vs_cpu_one_core"] = {"device": ga["value"] / ga_cpu["value"], "e2e": ga["e2e"]["value"] / ga_cpu["value"]}
       # the first generations of the same seeded run on the device, against the oracle's
       short = ga_measure(GA_SUB_WORKLOAD, 0, 1, 1, 0, generations=sample_gens) if world == 1 else None
       if short is not None:
         ok = [float(v) for v in short["history"]] == ga_cpu["history"]
-        sub["parity"] = (f"best-fitness history of the first {sample_gens} generations equal to the oracle GA's"
-                         if ok else "MISMATCH of the best-fitness history against the oracle GA")
+        sub["parity"] = (f"best-fitness history of the first {sample_gens} generations equal to that of "
+                         f"{ga_cpu['what']}" if ok else f"MISMATCH of the best-fitness history against {ga_cpu['what']}")
         if not ok:
           parity = {"ok": False}
     line["detail"][GA_SUB_WORKLOAD] = sub
@@ -1310,8 +1402,8 @@ def main_ga(args) -> int:
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value * G, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)", "impl": "reference",
             "config": config,
-            "cpu_baseline": {"value": value, "unit": "generations/s", "cores": vals[0]["cores"], "kind": "port",
-                             "sample": f"per step: {vals[0]['sample']}"},
+            "cpu_baseline": {"value": value, "unit": "generations/s", "cores": vals[0]["cores"],
+                             "kind": vals[0]["kind"], "sample": f"per step: {vals[0]['sample']}"},
             "e2e": {"value": value, "unit": "generations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -1324,13 +1416,14 @@ def main_ga(args) -> int:
           "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)", "config": config, "clocks": res["clocks"],
           "e2e": res["e2e"], "gpu_launches": res["gpu_launches"],
           "detail": {"best_fitness": res["best"], "engine": args.engine, "last_run": res["timing"],
-                     "loop_ms_steps": res["loop_ms_steps"], "walls_s": res["walls_s"], "buckets": res["buckets"],
+                     "loop_ms_steps": res["loop_ms_steps"], "walls_s": res["walls_s"],
+                     "phase_ms_steps": res["phase_ms_steps"], "gc": res["gc"], "buckets": res["buckets"],
                      "two_opt_totals": res["two_opt_totals"]}}
   if res["world"] > 1:
     config["parallelism"] = f"{res['world']} independent replicas (one GA run per GPU, generator seeded per rank)"
   if not args.no_cpu_baseline and res["world"] == 1:
     cpu = _ga_cpu_sample(args.workload, sample)
-    line["cpu_baseline"] = {"value": cpu["value"], "unit": "generations/s", "cores": cpu["cores"], "kind": "port",
+    line["cpu_baseline"] = {"value": cpu["value"], "unit": "generations/s", "cores": cpu["cores"], "kind": cpu["kind"],
                             "sample": cpu["sample"]}
   print(json.dumps(line))
   return 0

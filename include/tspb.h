@@ -663,6 +663,23 @@ int tspb_microbench_l2_gather(const int32_t* table, int64_t table_len, int32_t i
                               void* stream);
 int tspb_microbench_int32(int32_t iters, int32_t blocks, int32_t seed, int32_t* sink, void* stream);
 
+/*
+ * CUDA graphs of this library's launches (no counterpart in the reference, whose GA loop
+ * launches every kernel from Python each generation: genetic_algorithm.py:789-965).
+ *   tspb_graph_capture_begin: start capturing `stream` (not the legacy default stream),
+ *     relaxed mode; every tspb_* launch on that stream until the end call is recorded.
+ *   tspb_graph_capture_end: end the capture, instantiate and upload the graph; *exec_out
+ *     receives the executable graph (TSPB_ERR_CUDA and NULL if the capture was invalidated).
+ *   tspb_graph_launch: replay it on `stream`.
+ *   tspb_graph_destroy: free it (a replay still running finishes first).
+ * The captured launches keep the device pointers they were given: a replay reads and
+ * writes the same buffers, which must outlive the executable graph.
+ */
+int tspb_graph_capture_begin(void* stream);
+int tspb_graph_capture_end(void* stream, void** exec_out);
+int tspb_graph_launch(void* exec, void* stream);
+int tspb_graph_destroy(void* exec);
+
 #ifdef __cplusplus
 }
 #endif

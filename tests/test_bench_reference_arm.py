@@ -31,7 +31,12 @@ def test_reference_arm_prints_one_contract_line(args):
   assert len(lines) == 1
   d = lines[0]
   assert d["impl"] == "reference" and d["value"] > 0 and d["higher_is_better"] is True
-  assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
+  sys.path.insert(0, ROOT)
+  from baseline import reference_arm
+
+  # the reference's own CPU code when it is installed; Or-opt has no reference counterpart
+  want = "port" if args[1] == "or_opt" or reference_arm.import_root() is None else "reference"
+  assert d["cpu_baseline"]["kind"] == want and d["cpu_baseline"]["cores"] >= 1
   assert d["cpu_baseline"]["value"] == d["value"] and d["e2e"]["value"] == d["value"]
   assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
   assert d["unit"] == d["e2e"]["unit"] and d["config"]["workload"]
@@ -74,8 +79,57 @@ def test_parity_check_flags_a_planted_difference():
     return {"indices": idx, "results": results}
 
   ok = bench.check_parity(gpu, cpu())
-  assert ok["ok"] and ok["text"].startswith("bit-exact on 3/5 tours")
+  assert ok["ok"] and ok["text"].startswith("bit-exact against the oracle port on 3/5 tours")
   bad = bench.check_parity(gpu, cpu(("tour", 2, "first")))
   assert not bad["ok"] and "first tour 2" in bad["mismatches"][0]
   bad = bench.check_parity(gpu, cpu(("pairs", 4, "best")))
   assert not bad["ok"] and "best tour 4" in bad["mismatches"][0]
+
+
+def test_parity_check_against_the_reference_compares_passes_and_pairs():
+  """The reference's worker reports (passes, pairs) per mode; the check compares those
+  two counters and the tours, and names the reference."""
+  import numpy as np
+
+  sys.path.insert(0, ROOT)
+  import bench
+
+  rng = np.random.default_rng(4)
+  tours = np.stack([rng.permutation(10) for _ in range(4)]).astype(np.int32)
+  stats = np.arange(4 * 4, dtype=np.int64).reshape(4, 4)
+  gpu = {m: (tours.copy(), stats.copy()) for m in bench.MODES}
+  idx = [0, 3]
+  results = [{m: (tours[i].copy(), (int(stats[i][0]), int(stats[i][1]))) for m in bench.MODES} for i in idx]
+  ok = bench.check_parity(gpu, {"indices": idx, "results": results}, "reference")
+  assert ok["ok"] and "the reference's CPU 2-opt" in ok["text"]
+  results[1]["best"] = (tours[3].copy(), (int(stats[3][0]), int(stats[3][1]) + 1))
+  assert not bench.check_parity(gpu, {"indices": idx, "results": results}, "reference")["ok"]
+  # both arms hash the same refinements to the same digest
+  dev = [{m: (tours[i],) for m in bench.MODES} for i in idx]
+  assert bench.refined_digest(dev) == bench.refined_digest([{m: (tours[i], (0, 0)) for m in bench.MODES} for i in idx])
+
+
+@pytest.mark.timeout(300)
+def test_reference_worker_equals_the_oracle_port():
+  """The installed reference's CPU 2-opt and the oracle port refine the same tour to the
+  same local optimum with the same pass and pair counts (both modes, k = 20)."""
+  import numpy as np
+
+  sys.path.insert(0, ROOT)
+  from baseline import reference_arm
+
+  if reference_arm.import_root() is None:
+    pytest.skip("the reference is not installed")
+  from oracle import distances, two_opt
+  from tsp_gpu_clean_b200 import instances
+
+  coords = instances.clustered_instance(300, 8, 30.0, 77)
+  tour = instances.random_tours(300, 1, 78)[0]
+  out, secs = reference_arm.two_opt_worker((coords, tour, ("best", "first"), 20))
+  D = distances.euc2d_matrix(coords)
+  cand = distances.candidate_list(20, coords=coords)
+  for mode in ("best", "first"):
+    t, st = two_opt.improve_batch(tour[None, :], D, cand, mode, 10**9)
+    assert np.array_equal(out[mode][0], t[0]), mode
+    assert out[mode][1] == (int(st[0][0]), int(st[0][1])), mode
+  assert secs > 0

@@ -26,14 +26,17 @@ matrix: their distances are rebuilt from FP64 coordinates in every kernel.
 
 Scheduling: instances are grouped into size buckets; each bucket gets its own offspring
 launch and its own persistent elite 2-opt launch (CTA size picked by `BatchAutotuner`).
-One captured graph holds the whole generation for every run and is replayed in chunks
-between host checks.
+One captured graph holds the whole generation for every run (offspring, survival rank
+with the elite-edge tie check, survivor gather, elite 2-opt, tracking) and is replayed in
+chunks between host checks.
 
 Elite-edge ties (the elite set then follows NumPy's unstable argsort): when every tied
 row is converged, each argsort choice refines only rows that do not change, so the run
 goes on on the device. Otherwise the run pauses; at the next check the host takes
-`np.argsort` of its fitness, and the run finishes that generation at the start of the
-next replay.
+`np.argsort` of its fitness, and the run finishes that generation in the RESUME phase
+(its own 2-opt and tracking launches) at the start of the next replay. Only that first
+replay after a host resume carries the phase: its graph is captured when a run first
+pauses.
 """
 
 from __future__ import annotations
@@ -41,6 +44,7 @@ from __future__ import annotations
 import ctypes
 import math
 import time
+import weakref
 from dataclasses import dataclass, field
 from typing import Any, Sequence
 
@@ -61,23 +65,47 @@ DEVICE_TAPE_MIN_RUNS = 32
 OFFSPRING_THREADS = (64, 128, 256)
 
 
-def capture_graph(enqueue) -> "torch.cuda.CUDAGraph":
-  """A CUDA graph of the launches `enqueue()` makes, captured on a side stream with the
-  plain begin/end calls (the `torch.cuda.graph` context manager also runs a full Python
-  garbage collection and empties the allocator cache on entry, which costs up to a second
-  in a long-lived process)."""
+class LaunchGraph:
+  """An executable CUDA graph of this library's launches (`tspb_graph_*`), replayed on the
+  current stream. The captured launches keep their buffers' addresses: the buffers must
+  outlive the graph."""
+
+  def __init__(self, handle: int):
+    self._handle = handle
+    self._fin = weakref.finalize(self, LaunchGraph._free, handle)
+
+  @staticmethod
+  def _free(handle: int) -> None:
+    native.load_library().tspb_graph_destroy(handle)
+
+  def replay(self) -> None:
+    native.check("tspb_graph_launch", native.load_library().tspb_graph_launch(self._handle, stream_handle()))
+
+  def release(self) -> None:
+    self._fin()
+
+
+def capture_graph(enqueue) -> LaunchGraph:
+  """A CUDA graph of the launches `enqueue()` makes, captured on a side stream by the
+  library itself (`tspb_graph_capture_begin/end`). Only the library's own kernels are
+  recorded and nothing is allocated during capture, so torch's graph machinery (a private
+  allocator pool per graph, set up in `CUDAGraph.capture_begin`, which stalled the host
+  for 10-50 ms in some calls) is not involved."""
+  lib = native.load_library()
   stream = torch.cuda.Stream()
   stream.wait_stream(torch.cuda.current_stream())
-  g = torch.cuda.CUDAGraph()
+  handle = ctypes.c_void_p()
   with torch.cuda.stream(stream):
-    g.capture_begin(capture_error_mode="relaxed")
+    sh = stream_handle()
+    native.check("tspb_graph_capture_begin", lib.tspb_graph_capture_begin(sh))
     try:
       enqueue()
     finally:
-      g.capture_end()
+      rc = lib.tspb_graph_capture_end(sh, ctypes.byref(handle))
+  native.check("tspb_graph_capture_end", rc)
   torch.cuda.current_stream().wait_stream(stream)
   torch.cuda.synchronize()
-  return g
+  return LaunchGraph(handle.value)
 
 
 _DEFAULT_TUNER: BatchAutotuner | None = None
@@ -295,14 +323,16 @@ class FusedBatchSolver:
     """Rows per instance of the generation's main 2-opt phase (the tuner's work shape)."""
     return self.P if self._post_mutation else self.elite
 
-  def _generation(self) -> None:
-    """Enqueue one replay: finish RESUME runs, then one generation of every RUN run."""
+  def _generation(self, resume: bool = True) -> None:
+    """Enqueue one replay: finish RESUME runs (only the host sets that state, so `resume`
+    is needed only right after a host check that resumed runs), then one generation of
+    every RUN run."""
     lib = native.load_library()
     st = ctypes.byref(self.state)
     sh = stream_handle()
     R, U, O = native.TSPB_BATCH_PHASE_RESUME, native.TSPB_BATCH_PHASE_RUN, native.TSPB_BATCH_PHASE_OFFSPRING
     # the 2-opt kernel stores each refined row's fitness itself (no separate cost pass)
-    if self.elite:
+    if self.elite and resume:
       self._per_bucket(lambda b: self._two_opt(st, b, R))
       native.check("tspb_batch_track", lib.tspb_batch_track(st, R, sh))
       self.kernel_launches += 1
@@ -314,17 +344,25 @@ class FusedBatchSolver:
 
     self._per_bucket(children)
     native.check("tspb_batch_survival", lib.tspb_batch_survival(st, sh))
-    self.kernel_launches += 3
+    self.kernel_launches += self._survival_launches()
     if self.elite:
       self._per_bucket(lambda b: self._two_opt(st, b, U))
     native.check("tspb_batch_track", lib.tspb_batch_track(st, U, sh))
     self.kernel_launches += 1
 
-  def _launches_per_replay(self) -> int:
+  @staticmethod
+  def _survival_launches() -> int:
+    """Kernels of tspb_batch_survival: the rank (with the elite-edge tie check), then the
+    survivor gather."""
+    return 2
+
+  def _launches_per_replay(self, resume: bool = False) -> int:
     nb = len(self.buckets)
-    per = nb + 3 + 1  # offspring per bucket, survival (3 kernels), track
+    per = nb + self._survival_launches() + 1  # offspring per bucket, survival, track
     if self.elite:
-      per += 2 * nb + 1  # two 2-opt phases per bucket, resume track
+      per += nb  # the elite 2-opt per bucket
+      if resume:
+        per += nb + 1  # the RESUME phase's 2-opt per bucket and its track
     if self._post_mutation:
       per += nb  # offspring 2-opt per bucket
     return per
@@ -716,9 +754,10 @@ class FusedBatchSolver:
       native.check("tspb_batch_init", lib.tspb_batch_init(st, 0, 0, sh))
       self.kernel_launches += 1
     stats_before = self.ls_stats.sum(dim=(0, 1)).cpu().numpy()
+    t_postinit = time.perf_counter()
 
-    graph = self._capture() if (self.use_graph and G > 0) else None
-    per_replay = self._launches_per_replay()
+    # graphs[resume]: the replay with the RESUME phase is captured when a run first pauses
+    graphs = {False: self._capture(False)} if (self.use_graph and G > 0) else None
     torch.cuda.synchronize()
     t_loop = time.perf_counter()
     t_prep = t_loop - t_tuned  # post-init refinement, graph capture
@@ -734,13 +773,17 @@ class FusedBatchSolver:
     rounds, max_rounds = 0, 2 * G + 2
     chunk, remaining = min(self.chunk, max(G, 1)), G
     c = None
+    need_resume = False  # runs the host resumed wait for the next replay's RESUME phase
     while G > 0 and rounds < max_rounds:
-      for _ in range(max(1, min(chunk, remaining))):
-        if graph is not None:
-          graph.replay()
-          self.kernel_launches += per_replay
+      for q in range(max(1, min(chunk, remaining))):
+        resume = need_resume and q == 0 and self.elite > 0
+        if graphs is not None:
+          if resume not in graphs:
+            graphs[resume] = self._capture(resume, warm=False)
+          graphs[resume].replay()
+          self.kernel_launches += self._launches_per_replay(resume)
         else:
-          self._generation()
+          self._generation(resume)
         self.replays += 1
       rounds += 1
       ctl_host.copy_(self.ctl, non_blocking=True)
@@ -762,6 +805,7 @@ class FusedBatchSolver:
         chunk = max(1, chunk // 2)
       else:
         chunk = min(2 * chunk, self.chunk)
+      need_resume = bool(paused.size)
       alive = np.isin(c[:, 1], live)
       if not alive.any():
         break
@@ -808,6 +852,7 @@ class FusedBatchSolver:
                            "evaluated": int(stats_all[3])}
     self.last_timing = {"setup_s": t_setup - t_start, "setup_operands_s": t_ops, "setup_tape_s": t_tape,
                         "setup_nn_init_s": t_nn, "tune_s": t_tuned - t_setup, "postinit_capture_s": t_prep,
+                        "postinit_s": t_postinit - t_tuned, "capture_s": t_loop - t_postinit,
                         "results_s": time.perf_counter() - t_end, "loop_s": t_end - t_loop,
                         "total_s": t_end - t_start, "loop_ms_device": loop_ms,
                         "generations": int(ctl[:, 3].sum()) if G > 0 else 0, "replays": self.replays,
@@ -815,14 +860,17 @@ class FusedBatchSolver:
     return results
 
   # ------------------------------------------------------------------------ graph
-  def _capture(self):
-    # Warm every launch path outside capture with every run parked (all kernels no-op).
+  def _capture(self, resume: bool, warm: bool = True):
+    """The graph of one replay, with or without the RESUME phase. `warm` first runs every
+    launch path (the RESUME phase included) outside capture with every run parked, so all
+    kernels no-op."""
     launches = self.kernel_launches
-    saved = self.ctl.clone()
-    self.ctl[:, 1] = native.TSPB_BATCH_DONE
-    self._generation()
-    torch.cuda.synchronize()
-    self.ctl.copy_(saved)
-    g = capture_graph(self._generation)
+    if warm:
+      saved = self.ctl.clone()
+      self.ctl[:, 1] = native.TSPB_BATCH_DONE
+      self._generation(True)
+      torch.cuda.synchronize()
+      self.ctl.copy_(saved)
+    g = capture_graph(lambda: self._generation(resume))
     self.kernel_launches = launches
     return g

@@ -117,10 +117,40 @@ __global__ void __launch_bounds__(256) batch_offspring_kernel(const tspb_batch B
         (origin.same[0] && clean[origin.parent[0]]) || (origin.same[1] && clean[origin.parent[1]]) ? 1 : 0;
 }
 
+// The elite-edge tie of generation g, settled by the whole CTA right after the survival
+// sort: key[r], idx[r] (shared memory, r < P) are the survivors' fitness and source index
+// (< P: the population, else the offspring). Positions elite-1 and elite with equal fitness
+// let NumPy's unstable argsort choose the elites. The run goes on when every survivor of
+// that fitness is converged (any choice refines only rows that do not change), else it
+// pauses for the host's argsort. The survivors are gathered in the same generation whether
+// the run pauses or not (the gather serves RUN and PAUSED runs).
+__device__ void survival_tie(const tspb_batch& B, int i, int g, int parity, const double* key, const int* idx) {
+  const int P = B.P, e = B.elite;
+  if (e <= 0 || e >= P) return;  // uniform: no edge
+  const double fe = key[e - 1];
+  const bool tie = key[e] == fe;
+  bool ok = true;
+  if (tie) {
+    if (!B.clean[0]) {
+      ok = false;
+    } else {
+      const uint8_t* ca = clean_buf(B, parity) + (long long)i * P;
+      const uint8_t* cb = B.off_clean + (long long)i * P;
+      for (int r = threadIdx.x; r < P; r += blockDim.x)
+        if (key[r] == fe) ok = ok && (idx[r] < P ? ca[idx[r]] : cb[idx[r] - P]) != 0;
+    }
+  }
+  const int settled = __syncthreads_and(ok ? 1 : 0);
+  if (threadIdx.x == 0) {
+    B.ties[(long long)i * B.G + g] = tie ? 1 : 0;
+    if (tie && !settled) B.ctl[4 * i + 1] = TSPB_BATCH_PAUSED;
+  }
+}
+
 // CTA per instance: the stable order of the 2P combined fitness values (old population
 // first), i.e. (fitness, index) ascending, as the reference's lexsort keeps it; the first P
-// indices go to order[]. A bitonic sort of (fitness, index) pairs in shared memory, padded
-// with +inf to the next power of two n2.
+// indices go to order[], then the elite-edge tie. A bitonic sort of (fitness, index) pairs
+// in shared memory, padded with +inf to the next power of two n2.
 __global__ void batch_survival_rank_kernel(const tspb_batch B, int n2) {
   extern __shared__ __align__(16) unsigned char rank_sm[];
   double* key = reinterpret_cast<double*>(rank_sm);
@@ -157,6 +187,7 @@ __global__ void batch_survival_rank_kernel(const tspb_batch B, int n2) {
     }
   }
   for (int r = threadIdx.x; r < P; r += blockDim.x) B.order[(long long)i * P + r] = idx[r];
+  survival_tie(B, i, c[0], parity, key, idx);
 }
 
 // The same order with n2 / 2 threads (64 <= n2 <= 2048): thread t holds positions t and
@@ -224,16 +255,25 @@ __global__ void batch_survival_rank_reg_kernel(const tspb_batch B, int n2) {
       }
     }
   }
-  if (e0 < P) B.order[(long long)i * P + e0] = i0;  // half >= P: slot 1 is never a survivor
+  if (e0 < P) {  // half >= P: slot 1 is never a survivor
+    B.order[(long long)i * P + e0] = i0;
+    skey[e0] = k0;  // the sorted survivors for the tie check (every earlier read is behind a barrier)
+    sidx[e0] = i0;
+  }
+  __syncthreads();
+  survival_tie(B, i, c[0], parity, skey, sidx);
 }
 
 // CTA per (instance, survivor): new_pop[r] = combined[order[r]] with its fitness and
-// converged bit; the elite-edge tie flag.
+// converged bit. A run the rank kernel just paused is gathered too (the host's argsort
+// reads the survivors); a run still waiting for the host is gathered again in later
+// replays from the same unchanged order, population and offspring, which rewrites the
+// same rows.
 __global__ void __launch_bounds__(128) batch_survival_gather_kernel(const tspb_batch B) {
   const int P = B.P;
   const int i = blockIdx.x / P, r = blockIdx.x - i * P;
   const int* c = B.ctl + 4 * i;
-  if (c[1] != TSPB_BATCH_RUN) return;
+  if (c[1] != TSPB_BATCH_RUN && c[1] != TSPB_BATCH_PAUSED) return;
   const int g = c[0], parity = g & 1;
   const tspb_batch_instance I = B.inst[i];
   const int n = I.n;
@@ -258,35 +298,7 @@ __global__ void __launch_bounds__(128) batch_survival_gather_kernel(const tspb_b
       const uint8_t* cs = clean_buf(B, parity) + (long long)i * P;
       clean_buf(B, parity ^ 1)[(long long)i * P + r] = o < P ? cs[o] : B.off_clean[(long long)i * P + o - P];
     }
-    const int e = B.elite;
-    if (e > 0 && e < P && r == e) {
-      const int oe = order[e - 1];
-      const double fe = oe < P ? fit[oe] : off_fit[oe - P];
-      B.ties[(long long)i * B.G + g] = fe == f ? 1 : 0;
-    }
   }
-}
-
-// Warp per RUN instance, after the gather: an elite-edge tie pauses the run unless every
-// row of the tied group is converged. Survivors are sorted by (fitness, index), so the
-// tied group is every row whose fitness equals the elite edge's.
-__global__ void batch_pause_kernel(const tspb_batch B) {
-  const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (i >= B.num_instances) return;
-  int* c = B.ctl + 4 * i;
-  if (c[1] != TSPB_BATCH_RUN || B.ties[(long long)i * B.G + c[0]] == 0) return;  // warp-uniform
-  bool settled = false;
-  if (B.clean[0]) {
-    const int P = B.P, e = B.elite, parity = (c[0] + 1) & 1;
-    const double* f = fit_buf(B, parity) + (long long)i * P;
-    const uint8_t* cl = clean_buf(B, parity) + (long long)i * P;
-    const double fe = f[e - 1];
-    bool ok = true;
-    for (int r = lane; r < P; r += 32) ok = ok && (f[r] != fe || cl[r] != 0);
-    settled = __all_sync(FULL, ok);
-  }
-  if (!settled && lane == 0) c[1] = TSPB_BATCH_PAUSED;
 }
 
 // Persistent 2-opt over the (item, row) units of one phase. COORDS: the bucket's
@@ -672,7 +684,6 @@ extern "C" int tspb_batch_survival(const tspb_batch* b, void* stream) {
     batch_survival_rank_kernel<<<b->num_instances, rank_threads, rank_smem, st>>>(*b, n2);
   }
   batch_survival_gather_kernel<<<b->num_instances * b->P, 128, 0, st>>>(*b);
-  batch_pause_kernel<<<(b->num_instances * 32 + 127) / 128, 128, 0, st>>>(*b);
   return tspb_launch_status();
 }
 

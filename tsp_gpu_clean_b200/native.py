@@ -43,6 +43,10 @@ SIGNATURES: dict[str, tuple] = {
   "tspb_three_opt_grid_threads": (ctypes.c_int, [_i32, _i32]),
   "tspb_microbench_l2_gather": (ctypes.c_int, [_p, _i64, _i32, _i32, _p, _p]),
   "tspb_microbench_int32": (ctypes.c_int, [_i32, _i32, _i32, _p, _p]),
+  "tspb_graph_capture_begin": (ctypes.c_int, [_p]),
+  "tspb_graph_capture_end": (ctypes.c_int, [_p, ctypes.POINTER(ctypes.c_void_p)]),
+  "tspb_graph_launch": (ctypes.c_int, [_p, _p]),
+  "tspb_graph_destroy": (ctypes.c_int, [_p]),
   "tspb_two_opt_workspace_bytes": (_sz, [_i32, _i32, _i32, _i32, _i32]),
   "tspb_two_opt": (ctypes.c_int, [_p, _i32, _i32, _p, _i64, _p, _p, _p, _p, _p, _p, _i32, _i32, _i64, _i32, _p, _p, _p, _sz, _p]),
   "tspb_two_opt_gated": (ctypes.c_int, [_p, _p, _i32, _i32, _p, _i64, _p, _p, _p, _p, _p, _p, _i32, _i32, _i64, _i32, _p,
