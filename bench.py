@@ -390,9 +390,11 @@ def run_gpu(args, world: int, rank: int) -> dict:
   flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
   stream = torch.cuda.current_stream()
 
+  sym = native.TSPB_MODE_SYMMETRIC if ops.symmetric else 0  # as the strategy decides it
+
   def launch(m, counted):
     rc = lib.tspb_two_opt(ptr(work[m]), args.tours, n, ptr(dist_t), stride, ptr(coords_t), ptr(tabs.cand),
-                          ptr(tabs.cand_dist), ptr(rev_off), ptr(rev_idx), ptr(packed), k, native.MODE_CODES[m],
+                          ptr(tabs.cand_dist), ptr(rev_off), ptr(rev_idx), ptr(packed), k, native.MODE_CODES[m] | sym,
                           args.max_iter, args.threads, ptr(stats[m]) if counted else None, ptr(status), None, 0,
                           stream_handle())
     native.check("tspb_two_opt", rc)

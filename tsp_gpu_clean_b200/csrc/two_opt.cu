@@ -468,6 +468,7 @@ static size_t cached_ws_tour_bytes(int n, int mode) {
 }
 
 extern "C" size_t tspb_two_opt_workspace_bytes(int32_t num_tours, int32_t n, int32_t k, int32_t mode, int32_t block_threads) {
+  if (mode >= 0) mode &= ~TSPB_MODE_SYMMETRIC;
   (void)block_threads;
   if (num_tours <= 0 || n < 4) return 0;
   const Layout L = two_opt_layout(n, k, mode, k > 0);
@@ -488,6 +489,9 @@ static int two_opt_impl(int32_t* tours, int32_t num_tours, int32_t n, const int3
                         int64_t max_iterations, int32_t block_threads, int64_t* stats, int32_t* status,
                         const int32_t* skip, void* workspace, size_t workspace_bytes, void* stream) {
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  // coordinates rebuild EUC_2D distances, which are symmetric
+  const int symmetric = (mode & TSPB_MODE_SYMMETRIC) != 0 || dist == nullptr ? 1 : 0;
+  if (mode >= 0) mode &= ~TSPB_MODE_SYMMETRIC;
   if (num_tours < 0 || n < 0 || mode < 0 || mode > 2) return TSPB_ERR_ARG;
   if (num_tours == 0) return TSPB_OK;
   if (tours == nullptr || (dist == nullptr && coords == nullptr)) return TSPB_ERR_ARG;
@@ -528,6 +532,7 @@ static int two_opt_impl(int32_t* tours, int32_t num_tours, int32_t n, const int3
     c.arrays_in_smem = per == 0 ? 1 : 0;
     c.skip = skip;
     c.budget = watchdog_cycles();
+    c.symmetric = symmetric;
     if (has_rev && mode == TSPB_MODE_FIRST) {  // incremental restart of first mode
       c.rev_off = rev_off;
       c.rev_idx = rev_idx;

@@ -25,6 +25,7 @@ struct TwoOptArgs {
   const uint32_t* cand_packed;  // scan kernel: c | d(a, c) << 16 per entry (optional)
   const int32_t* skip;          // optional device flag: non-zero makes the launch a no-op
   long long budget;             // watchdog: SM cycles a tour may run (watchdog_cycles())
+  int symmetric;                // scan kernel: symmetric distances (TSPB_MODE_SYMMETRIC)
 };
 
 // Order-preserving u64 key: negative int32 gain in the high word, scan index low.

@@ -38,6 +38,7 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value) two_op
   T.rev_off = A.rev_off;
   T.rev_idx = A.rev_idx;
   T.budget = A.budget;
+  T.symmetric = A.symmetric;
   scan_tour<MODE, THREADS, U, LAYOUT, false, COUNT>(T, S);
 }
 

@@ -101,6 +101,7 @@ struct ScanTour {
   const int32_t* rev_idx = nullptr;  // flat entries a * k + r grouped by candidate node
   double* cost = nullptr;  // optional: the refined tour's length (exact int64 sum of eout, as float64)
   long long budget = BUDGET_CYCLES;  // watchdog: SM cycles before the tour ends with TSPB_ERR_BUDGET
+  int symmetric = 0;  // 1: d(a, b) == d(b, a); a move's out-edges come from the old ones (below)
 };
 
 // k-NN table layouts of scan_tour: plain int32 candidates (+ optional distances), packed
@@ -599,10 +600,44 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
       }
     }
     __syncthreads();
-    for (int p = bi + tid; p <= bj; p += THREADS) {
-      const int x = tour[p], y = tour[p + 1 == n ? 0 : p + 1];
-      succ[x] = y;
-      eout[x] = ds(x, y);
+    if (T.symmetric) {
+      // Inside the reversed window [lo, hi] a node's new successor is its old predecessor,
+      // so its new out-edge is that predecessor's old one (the same edge, read the other
+      // way). Only the two edges the move creates come from the distance source. Chunks
+      // run by increasing position: a chunk reads the old out-edges of positions p + 1
+      // before its barrier and writes those of positions p after it, and later chunks read
+      // only higher positions than any earlier chunk wrote.
+      const int lo = bi + 1, hi = bj;
+      for (int base = lo; base < hi; base += THREADS) {
+        const int p = base + tid;
+        int x = -1, y = 0, e = 0;
+        if (p < hi) {
+          x = tour[p];
+          y = tour[p + 1];
+          e = eout[y];
+        }
+        __syncthreads();
+        if (x >= 0) {
+          succ[x] = y;
+          eout[x] = e;
+        }
+      }
+      if (tid == 0) {  // the edge (tour[bi], tour[lo]) the move creates
+        const int x = tour[bi], y = tour[lo];
+        succ[x] = y;
+        eout[x] = ds(x, y);
+      }
+      if (tid == THREADS - 1) {  // and (tour[hi], tour[hi + 1]), from another warp
+        const int x = tour[hi], y = tour[hi + 1 == n ? 0 : hi + 1];
+        succ[x] = y;
+        eout[x] = ds(x, y);
+      }
+    } else {
+      for (int p = bi + tid; p <= bj; p += THREADS) {
+        const int x = tour[p], y = tour[p + 1 == n ? 0 : p + 1];
+        succ[x] = y;
+        eout[x] = ds(x, y);
+      }
     }
     __syncthreads();
     ++moves;

@@ -212,6 +212,7 @@ class DeviceOperands:
     self.h2d_bytes = 0
     self._dist = None
     self._coords = None
+    self._symmetric = None
     # contexts of one Problem object (repetitions of a run) share its device data
     self._shared = _problem_cache(context)
     self._cand: dict[int, tuple] = self._shared.setdefault("cand", {}) if self._shared is not None else {}
@@ -291,6 +292,24 @@ class DeviceOperands:
       self._dist = device_tensor(D, torch.int32)
       self.h2d_bytes += D.nbytes
     return self._dist
+
+  @property
+  def symmetric(self) -> bool:
+    """d(a, b) == d(b, a) for every pair (the 2-opt's TSPB_MODE_SYMMETRIC). EUC_2D from
+    coordinates is symmetric by its formula (dx and -dx square alike); any other matrix is
+    compared with its transpose on the device once."""
+    if self._symmetric is None and self._shared is not None:
+      self._symmetric = self._shared.get("symmetric")
+    if self._symmetric is None:
+      if self._euc2d_on_device():
+        sym = True
+      else:
+        d = self.dist()
+        sym = bool(d.shape[0] == d.shape[1] and torch.equal(d, d.t()))
+      self._symmetric = sym
+      if self._shared is not None:
+        self._shared["symmetric"] = sym
+    return self._symmetric
 
   def _tsplib_on_device(self) -> bool:
     from .native import EDGE_TYPE_CODES

@@ -169,7 +169,7 @@ class FusedMemeticSolver:
   def _two_opt(self, rows_ptr, num, skip=None):
     ls = self.ls
     lib = native.load_library()
-    mode = native.MODE_CODES[ls.mode]
+    mode = native.MODE_CODES[ls.mode] | (native.TSPB_MODE_SYMMETRIC if self.symmetric else 0)
     threads = int(ls.threads) if ls.threads else auto_threads(num)
     rc = lib.tspb_two_opt_gated(ptr(skip if skip is not None else self.d_zero), rows_ptr, num, self.n, ptr(self.dist),
                                 self.stride, ptr(self.coords), ptr(self.cand), ptr(self.cand_dist), None, None,
@@ -249,6 +249,7 @@ class FusedMemeticSolver:
     pop0 = InitializationB200TourNearestNeighbor(k=self.nn_k, return_gpu=True).initialize(list(customers), P, context)
     ops = operands_for(context)
     self.dist, self.stride, self.coords = ops.distance_args(n, self.max_matrix_dimension)
+    self.symmetric = self.dist is not None and ops.symmetric
     self.cand = self.cand_dist = self.packed = None
     self.k = 0
     ls = self.ls

@@ -85,7 +85,8 @@ def two_opt_table(inst: InstanceTensors, tours: "torch.Tensor", table: "torch.Te
     use_packed = False
   native.check("tspb_two_opt", lib.tspb_two_opt(
     ptr(t), num, n, ptr(inst.dist), n if inst.dist is not None else 0, ptr(inst.coords) if inst.dist is None else None,
-    ptr(table), ptr(cd), None, None, ptr(packed) if use_packed else None, k, native.MODE_CODES[mode], int(max_iterations),
+    ptr(table), ptr(cd), None, None, ptr(packed) if use_packed else None, k,
+    native.MODE_CODES[mode] | native.TSPB_MODE_SYMMETRIC, int(max_iterations),  # EUC_2D: symmetric
     threads, ptr(stats), ptr(status), ptr(ws), ws_bytes, stream_handle()))
   if int(status.max().item()) != 0:
     raise RuntimeError("2-opt rejected a start tour")

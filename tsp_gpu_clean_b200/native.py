@@ -27,6 +27,8 @@ TSPB_ERR_BUDGET = 7
 TSPB_ERR_DEVICE_MEMORY = 8
 
 MODE_CODES = {"best": 0, "batch": 0, "first": 1, "multi_move": 2}
+#: OR-ed into a 2-opt mode code: the distances are symmetric (include/tspb.h)
+TSPB_MODE_SYMMETRIC = 0x100
 
 _p = ctypes.c_void_p
 _i32 = ctypes.c_int32
@@ -123,6 +125,7 @@ TSPB_BATCH_COORDS = 1
 TSPB_BATCH_GROUPED = 2
 TSPB_BATCH_INCREMENTAL = 4
 TSPB_BATCH_PAIR = 8
+TSPB_BATCH_SYMMETRIC = 16
 
 
 class Pcg64(ctypes.Structure):

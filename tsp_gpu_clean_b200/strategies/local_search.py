@@ -134,6 +134,8 @@ class LocalSearchB200TourTwoOpt(StrategyBase):
       d_tours = self._stager.upload(host, torch.int32)
       self.h2d_bytes += host.nbytes
     mode = native.MODE_CODES[self.mode]
+    if dist is not None and ops.symmetric:
+      mode |= native.TSPB_MODE_SYMMETRIC  # a move's out-edges from the old ones (include/tspb.h)
     threads = int(self.threads_per_block) if self.threads_per_block else auto_threads(num)
     ws_bytes = native.load_library().tspb_two_opt_workspace_bytes(num, n, k, mode, threads)
     ws = self._workspace.get(int(ws_bytes))
