@@ -67,8 +67,8 @@ L2_FLUSH_BYTES = 256 << 20
 #: DRAM bytes read + written scaled to a 1024-tour launch (the tours' 4 KB each is the part
 #: that grows). A gain is computed only for entries whose lower bound could improve.
 NCU_PER_GAIN: dict[str, dict[str, float]] = {
-  "first": {"inst": 8.327, "lts_bytes": 45.25, "dram_bytes_per_launch": 8_298_496},
-  "best": {"inst": 9.030, "lts_bytes": 33.36, "dram_bytes_per_launch": 8_215_040},
+  "first": {"inst": 8.337, "lts_bytes": 32.52, "dram_bytes_per_launch": 8_486_144},
+  "best": {"inst": 9.083, "lts_bytes": 31.95, "dram_bytes_per_launch": 8_617_472},
 }
 #: CPU parity sample: tours of the timed batch refined by the oracle (at least this many)
 PARITY_TOURS = 16

@@ -39,11 +39,12 @@ extern "C" {
 #define TSPB_MODE_FIRST 1      /* first improving move in scan order */
 #define TSPB_MODE_MULTI_MOVE 2 /* every disjoint improving move, steepest first */
 /* OR-ed into a 2-opt mode: the distances are symmetric (d(a, b) == d(b, a) for every pair),
- * as every coordinate-built TSPLIB type is. After a move the candidate scan then takes each
- * reversed node's new out-edge from its old predecessor's (the same edge) and reads only the
- * two new edges from the distance source. Without it every out-edge of the reversed window
- * is read again, which is exact for asymmetric matrices too. Launches that rebuild
- * distances from coordinates (no matrix) are symmetric without it. */
+ * as EUC_2D from coordinates is. After a move that reverses a window wider than the CTA,
+ * the candidate scan then takes each reversed node's new out-edge from its old
+ * predecessor's (the same edge) and reads only the two new edges from the distance source.
+ * Without it every out-edge of the reversed window is read again, which is exact for
+ * asymmetric matrices too. Launches that rebuild distances from coordinates (no matrix)
+ * are symmetric without it. Results are the same either way on symmetric distances. */
 #define TSPB_MODE_SYMMETRIC 0x100
 
 /* Library version and build facts. */
@@ -571,8 +572,6 @@ int tspb_batch_survival(const tspb_batch* b, void* stream);
  * Same results; for phases with fewer units than SMs (elites of a few runs). threads counts
  * per CTA, and tspb_batch_two_opt_occupancy then reports co-resident CTAs of such pairs. */
 #define TSPB_BATCH_PAIR 8
-/* every item's distances are symmetric (TSPB_MODE_SYMMETRIC); implied by COORDS */
-#define TSPB_BATCH_SYMMETRIC 16
 /* 2-opt over the (item, row) units of one phase: persistent CTAs (ctas <= 0: every CTA
  * that fits) take units from the device counter `queue` (zeroed by this call) in item
  * order; put the largest instances first. `flags` (TSPB_BATCH_*) state what holds for

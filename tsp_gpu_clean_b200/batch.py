@@ -132,7 +132,6 @@ class Bucket:
   can_rebuild: bool = False  # every item has coordinates: the tuner may pick them over the matrix
   incremental: bool = False  # the 2-opt runs with the reverse k-NN index (TSPB_BATCH_INCREMENTAL)
   pair: bool = False  # every row is refined by a two-CTA cluster (TSPB_BATCH_PAIR, best mode)
-  symmetric: bool = False  # every item's distances are symmetric (TSPB_BATCH_SYMMETRIC)
   two_opt_threads: int = 128
   offspring_threads: int = 128
   d_items: Any = None
@@ -283,8 +282,7 @@ class FusedBatchSolver:
   def _flags(bucket: Bucket) -> int:
     return ((native.TSPB_BATCH_COORDS if bucket.coords else 0) | (native.TSPB_BATCH_GROUPED if bucket.grouped else 0)
             | (native.TSPB_BATCH_INCREMENTAL if bucket.incremental else 0)
-            | (native.TSPB_BATCH_PAIR if bucket.pair else 0)
-            | (native.TSPB_BATCH_SYMMETRIC if bucket.symmetric else 0))
+            | (native.TSPB_BATCH_PAIR if bucket.pair else 0))
 
   def _two_opt(self, st_ref, bucket: Bucket, phase: int, threads: int | None = None) -> None:
     rc = native.load_library().tspb_batch_two_opt(
@@ -673,7 +671,6 @@ class FusedBatchSolver:
 
     self._keep = []
     coords_flags = []
-    symmetric = []
     rebuildable = []
     t_ops = t_tape = 0.0
     all_tabs = []
@@ -714,7 +711,6 @@ class FusedBatchSolver:
       opt = optimal_cost[i] if isinstance(optimal_cost, (list, tuple, np.ndarray)) else optimal_cost
       inst.optimal = float(opt) if opt is not None and opt > 0 else 0.0
       coords_flags.append(dist is None)
-      symmetric.append(dist is None or ops.symmetric)
     t0 = time.perf_counter()
     check_packed(all_tabs)  # every instance's pack-overflow flag in one sync
     bad = [i for i, t in enumerate(all_tabs) if t.packed is None]
@@ -740,7 +736,6 @@ class FusedBatchSolver:
     for b in self.buckets:
       b.grouped = all(h_inst[i].k % 4 == 0 and h_inst[i].cand_packed % 16 == 0 for i in b.items)
       b.can_rebuild = all(rebuildable[i] for i in b.items)
-      b.symmetric = all(symmetric[i] for i in b.items)
       b.d_items = torch.tensor(b.items, dtype=torch.int32, device=dev)
       b.queue = torch.zeros(1, dtype=torch.int32, device=dev)
 

@@ -313,8 +313,7 @@ __global__ void __launch_bounds__(128) batch_survival_gather_kernel(const tspb_b
 template <int MODE, int THREADS, int U, bool COORDS, int LAYOUT, bool REV = false, int CL = 1>
 __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value)
     batch_two_opt_kernel(const tspb_batch B, const int32_t* __restrict__ items, int num_items, int rows, int phase,
-                         long long max_iter, int max_n, unsigned* __restrict__ queue, long long budget,
-                         int symmetric) {
+                         long long max_iter, int max_n, unsigned* __restrict__ queue, long long budget) {
   extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ ScanSmem S;
   __shared__ unsigned s_unit;
@@ -381,13 +380,12 @@ __global__ void __launch_bounds__(THREADS, ScanMinBlocks<THREADS>::value)
     T.rev_off = REV ? I.rev_off : nullptr;
     T.rev_idx = REV ? I.rev_idx : nullptr;
     T.budget = budget;
-    T.symmetric = COORDS || symmetric;  // coordinates rebuild EUC_2D distances (symmetric)
     // the refined row's fitness (fit, or off_fit for children); POSTINIT leaves fitness
     // to tspb_batch_init (the tuner's probes refine scratch rows there)
     T.cost = phase == TSPB_BATCH_PHASE_POSTINIT
                  ? nullptr
                  : (offspring ? B.off_fit : fit_buf(B, parity)) + (long long)i * B.P + row;
-    scan_tour<MODE, THREADS, U, LAYOUT, REV && MODE == TSPB_MODE_BEST, true, CL>(T, S);
+    scan_tour<MODE, THREADS, U, LAYOUT, REV && MODE == TSPB_MODE_BEST, true, CL, false>(T, S);
   }
 }
 
@@ -474,8 +472,7 @@ static int batch_two_opt_launch(const tspb_batch& b, const int32_t* items, int n
                                 cudaStream_t st) {
   const bool coords = flags & TSPB_BATCH_COORDS, grouped = flags & TSPB_BATCH_GROUPED;
   const bool rev = flags & TSPB_BATCH_INCREMENTAL;
-  const int symmetric = (flags & TSPB_BATCH_SYMMETRIC) ? 1 : 0;
-  using Kern = void (*)(const tspb_batch, const int32_t*, int, int, int, long long, int, unsigned*, long long, int);
+  using Kern = void (*)(const tspb_batch, const int32_t*, int, int, int, long long, int, unsigned*, long long);
   Kern kern = coords ? (grouped ? batch_two_opt_kernel<MODE, THREADS, U, true, SCAN_GROUPED>
                                 : batch_two_opt_kernel<MODE, THREADS, U, true, SCAN_PACKED>)
                      : (grouped ? batch_two_opt_kernel<MODE, THREADS, U, false, SCAN_GROUPED>
@@ -522,7 +519,7 @@ static int batch_two_opt_launch(const tspb_batch& b, const int32_t* items, int n
       TSPB_CUDA_CHECK(cudaMemsetAsync(queue, 0, sizeof(unsigned), st));
       cfg.gridDim = dim3((unsigned)(2 * pairs));
       TSPB_CUDA_CHECK(cudaLaunchKernelEx(&cfg, pk, b, items, num_items, rows, phase, max_iter, max_n, queue,
-                                         watchdog_cycles(), symmetric));
+                                         watchdog_cycles()));
       return tspb_launch_status();
     } else {
       return TSPB_ERR_ARG;
@@ -543,8 +540,7 @@ static int batch_two_opt_launch(const tspb_batch& b, const int32_t* items, int n
   const int pct = carveout_for(per_sm_used < per_sm ? per_sm_used : per_sm, smem);
   if (pct > 0) TSPB_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
   TSPB_CUDA_CHECK(cudaMemsetAsync(queue, 0, sizeof(unsigned), st));
-  kern<<<(int)grid, THREADS, smem, st>>>(b, items, num_items, rows, phase, max_iter, max_n, queue, watchdog_cycles(),
-                                         symmetric);
+  kern<<<(int)grid, THREADS, smem, st>>>(b, items, num_items, rows, phase, max_iter, max_n, queue, watchdog_cycles());
   return tspb_launch_status();
 }
 
@@ -706,9 +702,7 @@ extern "C" int tspb_batch_two_opt(const tspb_batch* b, const int32_t* items, int
                                   int32_t flags, int32_t phase, int32_t mode, int64_t max_iterations, int32_t threads,
                                   int32_t ctas, uint32_t* queue, void* stream) {
   if (!batch_ok(b) || num_items < 0 || max_n < 4 || !queue) return TSPB_ERR_ARG;
-  if (flags & ~(TSPB_BATCH_COORDS | TSPB_BATCH_GROUPED | TSPB_BATCH_INCREMENTAL | TSPB_BATCH_PAIR |
-                TSPB_BATCH_SYMMETRIC))
-    return TSPB_ERR_ARG;
+  if (flags & ~(TSPB_BATCH_COORDS | TSPB_BATCH_GROUPED | TSPB_BATCH_INCREMENTAL | TSPB_BATCH_PAIR)) return TSPB_ERR_ARG;
   if ((flags & TSPB_BATCH_PAIR) &&
       (mode != TSPB_MODE_BEST || !(flags & TSPB_BATCH_GROUPED) || (flags & TSPB_BATCH_INCREMENTAL)))
     return TSPB_ERR_ARG;

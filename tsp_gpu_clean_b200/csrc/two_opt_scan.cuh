@@ -135,7 +135,11 @@ __device__ __forceinline__ void load_words(const uint32_t* p, uint32_t (&w)[U]) 
 // and refreshing them after a move visits every candidate of every row in the reversed
 // window, so a caller that passes no stats runs the COUNT = false instance (or, with
 // COUNT = true, skips the refresh at run time): same moves, same tours.
-template <int MODE, int THREADS, int U, int LAYOUT, bool INC = false, bool COUNT = true, int CL = 1>
+//
+// SYM: the symmetric-distance refresh after a move is compiled in (used when T.symmetric
+// is set). The batch engine compiles it out: its large CTAs cover most windows in one round
+// of distance reads, and the extra code measured slower there.
+template <int MODE, int THREADS, int U, int LAYOUT, bool INC = false, bool COUNT = true, int CL = 1, bool SYM = true>
 __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
   constexpr bool PACKED = LAYOUT != SCAN_PLAIN;
   constexpr bool GROUPED = LAYOUT == SCAN_GROUPED;
@@ -600,13 +604,15 @@ __device__ __forceinline__ void scan_tour(const ScanTour T, ScanSmem& S) {
       }
     }
     __syncthreads();
-    if (T.symmetric) {
+    if (SYM && T.symmetric && bj - bi >= THREADS) {
       // Inside the reversed window [lo, hi] a node's new successor is its old predecessor,
       // so its new out-edge is that predecessor's old one (the same edge, read the other
       // way). Only the two edges the move creates come from the distance source. Chunks
       // run by increasing position: a chunk reads the old out-edges of positions p + 1
       // before its barrier and writes those of positions p after it, and later chunks read
-      // only higher positions than any earlier chunk wrote.
+      // only higher positions than any earlier chunk wrote. A window that one round of
+      // distance reads covers (bj - bi < THREADS) keeps that round: a chunk's barrier
+      // would cost more than the reads it saves.
       const int lo = bi + 1, hi = bj;
       for (int base = lo; base < hi; base += THREADS) {
         const int p = base + tid;

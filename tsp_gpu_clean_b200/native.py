@@ -125,7 +125,6 @@ TSPB_BATCH_COORDS = 1
 TSPB_BATCH_GROUPED = 2
 TSPB_BATCH_INCREMENTAL = 4
 TSPB_BATCH_PAIR = 8
-TSPB_BATCH_SYMMETRIC = 16
 
 
 class Pcg64(ctypes.Structure):
