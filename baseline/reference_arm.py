@@ -112,7 +112,8 @@ def two_opt_worker(args):
   return out, secs
 
 
-def ga_gens_per_s(coords, population: int, elite: int, post_init: bool, sample_gens: int, options: dict) -> dict:
+def ga_gens_per_s(coords, population: int, elite: int, post_init: bool, sample_gens: int, options: dict,
+                  seed: int = 42) -> dict:
   """Generations/s of the reference's own `GeneticAlgorithm.evolve`
   (src/algorithms/metaheuristics/genetic_algorithm.py:789-965) with its CPU strategies, on
   one core: `options` picks the configuration (`crossover` "pmx"/"ox", `mutation`
@@ -120,7 +121,7 @@ def ga_gens_per_s(coords, population: int, elite: int, post_init: bool, sample_g
   k = 20 x 10 through `PostInitLocalSearchStep` / `EliteOnlyLocalSearchStep`
   (src/algorithms/pipeline_steps.py:103-195) as configured. The loop time is a run of
   `sample_gens` generations minus a run of none (initialisation and the post-init
-  refinement), so it counts generations only."""
+  refinement), so it counts generations only. `seed` seeds the context and every strategy."""
   setup()
   from algorithms import GeneticAlgorithm
   from algorithms.pipeline_steps import EliteOnlyLocalSearchStep, PostInitLocalSearchStep
@@ -142,7 +143,7 @@ def ga_gens_per_s(coords, population: int, elite: int, post_init: bool, sample_g
                     coordinates=np.asarray(coords, dtype=np.float64), distances=None)
 
   def run(gens: int):
-    ctx = ProblemContext(problem, xp=np, seed=42)
+    ctx = ProblemContext(problem, xp=np, seed=seed)
     ctx.get_cpu_distances()
     ctx.get_cpu_candidate_list(20)
     ctx.get_cpu_candidate_list(5)
@@ -153,12 +154,12 @@ def ga_gens_per_s(coords, population: int, elite: int, post_init: bool, sample_g
       steps.append(PostInitLocalSearchStep(local_search=ls, evaluation=ev))
     if elite:
       steps.append(EliteOnlyLocalSearchStep(local_search=ls, evaluation=ev, elite_count=elite))
-    init = (InitializationCPUPermRandom(seed=42) if options["init"] == "random"
-            else InitializationCPUTourNearestNeighbor(k=5, seed=42))
-    xo = CrossoverCPUPermOrder(seed=42) if options["crossover"] == "ox" else CrossoverCPUPermPartiallyMapped(seed=42)
-    mut = MutationCPUPermSwap(seed=42) if options["mutation"] == "swap" else MutationCPUPermInversion(seed=42)
-    ga = GeneticAlgorithm(population_size=population, mutation_rate=options["rate"], seed=42, initialization=init,
-                          selection=SelectionCPUTournament(k=5, seed=42), crossover=xo, mutation=mut,
+    init = (InitializationCPUPermRandom(seed=seed) if options["init"] == "random"
+            else InitializationCPUTourNearestNeighbor(k=5, seed=seed))
+    xo = CrossoverCPUPermOrder(seed=seed) if options["crossover"] == "ox" else CrossoverCPUPermPartiallyMapped(seed=seed)
+    mut = MutationCPUPermSwap(seed=seed) if options["mutation"] == "swap" else MutationCPUPermInversion(seed=seed)
+    ga = GeneticAlgorithm(population_size=population, mutation_rate=options["rate"], seed=seed, initialization=init,
+                          selection=SelectionCPUTournament(k=5, seed=seed), crossover=xo, mutation=mut,
                           local_search=ls, evaluation=ev, local_search_stage=options["stage"],
                           pipeline=steps or None)
     t0 = time.perf_counter()

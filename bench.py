@@ -719,8 +719,14 @@ def _uneven_inputs(count: int, pool=None, seed: int = UNEVEN_SEED):
 
 
 def _uneven_cpu_worker(args):
-  """Oracle GA generations/s on one instance of the batch (init excluded)."""
+  """GA generations/s on one instance of the batch (init excluded): the reference's own
+  GeneticAlgorithm.evolve with its CPU strategies when it is installed, else the oracle GA."""
   coords, cache, seed, gens = args
+  if cpu_path()[0] == "reference":
+    from baseline import reference_arm
+
+    r = reference_arm.ga_gens_per_s(coords, 64, 8, True, gens, dict(GA_DEFAULT_OPTIONS), seed=seed)
+    return gens, r["loop_s"], len(coords)
   from oracle import distances as odist
   from oracle import ga as oga
 
@@ -736,8 +742,9 @@ def _uneven_cpu_worker(args):
 
 
 def uneven_cpu_sample(pool, workers: int, coords, caches, gens: int) -> dict:
-  """Aggregate oracle generations/s over a size-stratified sample of the batch, one
-  instance per process (evenly spaced instances in size order)."""
+  """Aggregate CPU generations/s (the reference's GA, else the oracle's) over a
+  size-stratified sample of the batch, one instance per process (evenly spaced instances
+  in size order)."""
   order = sorted(range(len(coords)), key=lambda i: len(coords[i]))
   step = max(1, len(order) // workers)
   pick = [order[min(j * step + step // 2, len(order) - 1)] for j in range(min(workers, len(order)))]
@@ -746,7 +753,8 @@ def uneven_cpu_sample(pool, workers: int, coords, caches, gens: int) -> dict:
   wall = time.perf_counter() - t0
   # each process runs one GA at a time; the aggregate is the sum of the per-process rates
   value = sum(g / t for g, t, _ in res)
-  return {"value": value, "instances": len(pick), "sizes": [n for _, _, n in res], "wall_s": wall, "gens": gens}
+  return {"value": value, "instances": len(pick), "sizes": [n for _, _, n in res], "wall_s": wall, "gens": gens,
+          "kind": cpu_path()[0]}
 
 
 def run_uneven_bench(args) -> dict:
@@ -849,7 +857,7 @@ def main_uneven(args) -> int:
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * count * G / value, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "int32", "data": "synthetic (seeded)", "impl": "reference", "config": config,
-            "cpu_baseline": {"value": value, "unit": "generations/s", "cores": workers, "kind": "port",
+            "cpu_baseline": {"value": value, "unit": "generations/s", "cores": workers, "kind": vals[0]["kind"],
                              "sample": f"{vals[0]['instances']} size-stratified instances (n = {vals[0]['sizes']}), "
                                        f"{sample_gens} generations each, one process per instance"},
             "e2e": {"value": value, "unit": "generations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -877,7 +885,7 @@ def main_uneven(args) -> int:
     cpu = uneven_cpu_sample(pool, workers, coords, caches, sample_gens)
     pool.close()
     pool.join()
-    line["cpu_baseline"] = {"value": cpu["value"], "unit": "generations/s", "cores": workers, "kind": "port",
+    line["cpu_baseline"] = {"value": cpu["value"], "unit": "generations/s", "cores": workers, "kind": cpu["kind"],
                             "sample": f"{cpu['instances']} size-stratified instances (n = {cpu['sizes']}), "
                                       f"{sample_gens} generations each, one process per instance, {cpu['wall_s']:.1f} s"}
   print(json.dumps(line))
