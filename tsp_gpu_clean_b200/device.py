@@ -37,9 +37,20 @@ def is_device_array(x: Any) -> bool:
   return torch is not None and isinstance(x, torch.Tensor) and x.is_cuda
 
 
+_RAW_STREAM = getattr(torch._C, "_cuda_getCurrentRawStream", None) if torch is not None else None
+_CUR_DEVICE = getattr(torch._C, "_cuda_getDevice", None) if torch is not None else None
+
+
 def stream_handle(stream=None) -> ctypes.c_void_p:
-  s = stream if stream is not None else torch.cuda.current_stream()
-  return ctypes.c_void_p(s.cuda_stream)
+  """The cudaStream_t of `stream`, else of the current stream. The current stream's handle
+  is read from torch's raw accessor when it has one: `torch.cuda.current_stream()` builds a
+  Stream object and resolves the device each call, which cost a few microseconds in every
+  replay of the GA engines' graphs."""
+  if stream is not None:
+    return ctypes.c_void_p(stream.cuda_stream)
+  if _RAW_STREAM is not None and _CUR_DEVICE is not None and torch.cuda.is_initialized():
+    return ctypes.c_void_p(_RAW_STREAM(_CUR_DEVICE()))
+  return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
 def ptr(t) -> ctypes.c_void_p | None:
