@@ -75,15 +75,6 @@ PARITY_TOURS = 16
 GA_SUB_WORKLOAD = "ga1000"
 
 
-def _peaks() -> dict:
-  path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-  if os.path.exists(path):
-    with open(path) as fh:
-      d = json.load(fh)
-    return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
-  return {"hbm_gbs": 6650.0, "source": "fallback"}
-
-
 # ----------------------------------------------------------------------------------- CPU
 def _cpu_worker(args):
   """Refine one tour in best then first mode with the oracle.
@@ -1063,6 +1054,10 @@ def run_learned_bench(args) -> dict:
 OR_OPT_PASSES = 50
 OR_OPT_SEGMENT = 3
 OR_OPT_BYTES_PER_ENTRY = 12  # candidate id + d(x, c) from the k-NN tables, one gathered d(y, e)
+#: Per valid entry the Or-opt kernel evaluated (1024 tours, 128-thread CTAs), from one ncu
+#: capture of the same launch on the first 256 tours: warp instructions executed and L2
+#: sector bytes, and DRAM bytes scaled to a 1024-tour launch (the tours' 4 KB each grows).
+OR_OPT_NCU_PER_ENTRY: dict | None = {"inst": 4.032, "lts_bytes": 32.51, "dram_bytes_per_launch": 8_488_960}
 OR_OPT_CPU_TOURS = 6
 OR_OPT_THREADS = 128  # fastest of 128 / 256 / 512 threads per CTA here
 
@@ -1123,6 +1118,9 @@ def main_or_opt(args) -> int:
   world, rank = _init_ranks()  # this rank's GPU and, under torchrun, the NCCL group
   build_library()
   lib = native.load_library()
+  from tsp_gpu_clean_b200 import roofline
+
+  peaks = roofline.measure_peaks()  # the kernel's ceilings on this device, before the timed region
   ops = operands_for(ctx)
   dist_t, stride, _ = ops.distance_args(n)
   tabs = ops.candidates(K_CAND, cand_np, n)
@@ -1185,12 +1183,27 @@ def main_or_opt(args) -> int:
                   "d2h_bytes_per_step": int(tours_np.nbytes)},
           "gpu_launches": launches,
           "detail": {"e2e_walls_s": [round(w, 4) for w in walls], "e2e_gc": gcw.summary()}}
-  per_launch = evaluated / len(ms) * OR_OPT_BYTES_PER_ENTRY
-  peaks = _peaks()
-  achieved = per_launch / (sum(ms) / len(ms) / 1e3) / 1e9
-  line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                      "frac": achieved / peaks["hbm_gbs"], "traffic": None,
-                      "note": f"{OR_OPT_BYTES_PER_ENTRY} B per valid entry; peak {peaks['source']}"}
+  line["detail"]["evaluated_per_step"] = evaluated // len(ms)
+  # like the 2-opt scan, the kernel works on an L2-resident matrix and shared-memory tour
+  # state: its ceilings are the L2 gather rate and the INT32 issue rate, measured here
+  eps = evaluated / (sum(ms) / 1e3)
+  per = OR_OPT_NCU_PER_ENTRY
+  if per is not None:
+    int_ach, l2_ach = eps * per["inst"] * 32 / 1e12, eps * per["lts_bytes"] / 1e9
+    basis = (f"ncu per valid entry: {per['inst']:.2f} warp instructions, {per['lts_bytes']:.2f} L2 sector bytes")
+  else:
+    int_ach, l2_ach = eps * ALG_OPS_PER_DELTA / 1e12, eps * 32 / 1e9
+    basis = f"no ncu figure: one 32-byte L2 sector and {ALG_OPS_PER_DELTA} integer ops per valid entry"
+  i32 = {"achieved": int_ach, "peak": peaks["int32_tops"], "unit": "TOP/s", "frac": int_ach / peaks["int32_tops"]}
+  l2 = {"achieved": l2_ach, "peak": peaks["l2_sector_gbs"], "unit": "GB/s", "frac": l2_ach / peaks["l2_sector_gbs"]}
+  top = i32 if i32["frac"] >= l2["frac"] else l2
+  line["roofline"] = {"bound": "int32" if top is i32 else "l2", "achieved": top["achieved"], "peak": top["peak"],
+                      "unit": top["unit"], "frac": top["frac"],
+                      "traffic": per.get("dram_bytes_per_launch") if per is not None else None,
+                      "kernel": "or_opt_kernel", "peak_source": "measured in this run: " + peaks["method"],
+                      "basis": basis, "int32": i32, "l2": l2,
+                      "algorithmic": {"gbs": eps * OR_OPT_BYTES_PER_ENTRY / 1e9,
+                                      "basis": f"{OR_OPT_BYTES_PER_ENTRY} B per valid entry"}}
   if world == 1 and not args.no_cpu_baseline:
     cpu = _or_opt_cpu_sample(coords, cand_np, tours_np)
     for t, o in enumerate(cpu["outs"]):

@@ -69,3 +69,18 @@ def test_argument_checks(lib):
   assert lib.tspb_graph_capture_end(None, ctypes.byref(out)) == native.TSPB_ERR_ARG
   assert lib.tspb_graph_launch(None, None) == native.TSPB_ERR_ARG
   assert lib.tspb_graph_destroy(None) == native.TSPB_OK
+
+
+def test_stream_handle_follows_the_current_stream(lib):
+  """The raw current-stream handle the launches use is torch's current stream, inside and
+  outside a stream context (graph capture relies on it)."""
+  import torch
+
+  from tsp_gpu_clean_b200.device import stream_handle
+
+  assert stream_handle().value == (torch.cuda.current_stream().cuda_stream or None)
+  side = torch.cuda.Stream()
+  with torch.cuda.stream(side):
+    assert stream_handle().value == side.cuda_stream
+  assert stream_handle(side).value == side.cuda_stream
+  assert stream_handle().value == (torch.cuda.current_stream().cuda_stream or None)
