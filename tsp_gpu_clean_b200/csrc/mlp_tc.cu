@@ -42,8 +42,9 @@ constexpr int TMEM_COLS = 256;  // D, G2, GX, G1: 64 FP32 columns each
 constexpr int COL_D = 0, COL_G2 = 64, COL_GX = 128, COL_G1 = 192;
 
 // shared-memory layout (bytes)
-constexpr int S_X = 0;              // X: units (edge, fb), fb 0..7 (2..7 zero), 2048 B per block
-constexpr int S_W1T = S_X + 16384;  // W1 as N = hidden, K = feature: units (i, fb), 1024 B per block
+constexpr int S_X = 0;              // X: units (edge, fb), fb 0..7 (2..7 zero), 2048 B per block; two slots
+constexpr int X_SLOT = 16384;       // tile t uses slot t % 2 (its column sums may still read it during t + 1)
+constexpr int S_W1T = S_X + 2 * X_SLOT;  // W1 as N = hidden, K = feature: units (i, fb), 1024 B per block
 constexpr int S_W2T = S_W1T + 2048;  // W2 as N = j, K = i: units (j, ib)
 constexpr int S_W2 = S_W2T + 8192;   // W2 as N = i, K = j: units (i, jb)
 constexpr int S_H1 = S_W2 + 8192;    // h1: units (edge, ib)
@@ -195,8 +196,9 @@ __global__ void __launch_bounds__(ROWS, 1)
     u.w = pack2(w[6], w[7]);
     *reinterpret_cast<uint4*>(sm + S_W2 + r * 16 + b * 1024) = u;
   }
-  for (int q = tid; q < 6 * ROWS; q += ROWS)  // X blocks 2..7: the zero rows 16..63 of X^T
-    *reinterpret_cast<uint4*>(sm + S_X + (q % ROWS) * 16 + (2 + q / ROWS) * 2048) = make_uint4(0, 0, 0, 0);
+  for (int q = tid; q < 12 * ROWS; q += ROWS)  // X blocks 2..7 of both slots: the zero rows 16..63 of X^T
+    *reinterpret_cast<uint4*>(sm + S_X + (q / (6 * ROWS)) * X_SLOT + (q % ROWS) * 16 + (2 + (q / ROWS) % 6) * 2048) =
+        make_uint4(0, 0, 0, 0);
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(1) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -243,14 +245,15 @@ __global__ void __launch_bounds__(ROWS, 1)
       u1 = __ldg(X4 + 2 * e + 1);
     }
     u1.w = (u1.w & 0xFFFFu) | (0x3F80u << 16);  // feature 15 = 1: the rows of X^T dH at index 15 sum dH
-    *reinterpret_cast<uint4*>(sm + S_X + tid * 16) = u0;
-    *reinterpret_cast<uint4*>(sm + S_X + tid * 16 + 2048) = u1;
+    const int sx = S_X + (iter & 1) * X_SLOT;  // the previous tile's column sums may still read the other slot
+    *reinterpret_cast<uint4*>(sm + sx + tid * 16) = u0;
+    *reinterpret_cast<uint4*>(sm + sx + tid * 16 + 2048) = u1;
     const float yv = valid ? __ldg(y + e) : 0.f;
     publish();
     // h1 = bf16(relu(X W1 + b1))
     if (tid == 0) {
-      mma(tmem + COL_D, sdesc(base + S_X, 2048, 128), sdesc(base + S_W1T, 1024, 128), ID_ROWS, 0);
-      commit(bar);
+      mma(tmem + COL_D, sdesc(base + sx, 2048, 128), sdesc(base + S_W1T, 1024, 128), ID_ROWS, 0);
+      commit(bar);  // also the previous tile's column sums, issued before this MMA
     }
     wait_mma();
     if (!ok) break;
@@ -290,21 +293,23 @@ __global__ void __launch_bounds__(ROWS, 1)
     }
     store_row(sm, S_DH2, tid, v);
     publish();
-    // dh1 = dh2 W2^T (masked below); dW2 += h1^T dh2; db2 (row 15 of X^T dh2)
+    // dh1 = dh2 W2^T (masked below), committed alone; then dW2 += h1^T dh2 and db2 (row 15
+    // of X^T dh2), which run on while the threads mask dh1. Nothing rewrites h1, dh2 or this
+    // X slot before the next tile's first commit, which also covers these sums.
     if (tid == 0) {
 #pragma unroll
       for (int s = 0; s < 4; ++s)
         mma(tmem + COL_D, sdesc(base + S_DH2 + s * 4096, 2048, 128), sdesc(base + S_W2 + s * 2048, 1024, 128), ID_ROWS,
             s > 0 ? 1u : 0u);
+      commit(bar);
 #pragma unroll
       for (int s = 0; s < 8; ++s)
         mma(tmem + COL_G2, sdesc(base + S_H1 + s * 256, 128, 2048), sdesc(base + S_DH2 + s * 256, 128, 2048), ID_SUMS,
             (iter > 0 || s > 0) ? 1u : 0u);
 #pragma unroll
       for (int s = 0; s < 8; ++s)
-        mma(tmem + COL_GX, sdesc(base + S_X + s * 256, 128, 2048), sdesc(base + S_DH2 + s * 256, 128, 2048), ID_SUMS,
+        mma(tmem + COL_GX, sdesc(base + sx + s * 256, 128, 2048), sdesc(base + S_DH2 + s * 256, 128, 2048), ID_SUMS,
             (iter > 0 || s > 0) ? 1u : 0u);
-      commit(bar);
     }
     // dw3 and db3 in FP32 while the tensor cores run
     if (tid < 64) {
@@ -334,16 +339,19 @@ __global__ void __launch_bounds__(ROWS, 1)
     }
     store_row(sm, S_DH1, tid, v);
     publish();
-    // dW1 (rows 0..4) and db1 (row 15) += X^T dh1
+    // dW1 (rows 0..4) and db1 (row 15) += X^T dh1: not waited for here. The next tile loads
+    // its X into the other slot meanwhile, and its first commit covers these MMAs before it
+    // rewrites dh1.
     if (tid == 0) {
 #pragma unroll
       for (int s = 0; s < 8; ++s)
-        mma(tmem + COL_G1, sdesc(base + S_X + s * 256, 128, 2048), sdesc(base + S_DH1 + s * 256, 128, 2048), ID_SUMS,
+        mma(tmem + COL_G1, sdesc(base + sx + s * 256, 128, 2048), sdesc(base + S_DH1 + s * 256, 128, 2048), ID_SUMS,
             (iter > 0 || s > 0) ? 1u : 0u);
-      commit(bar);
     }
+  }
+  if (ok && iter > 0) {  // the last tile's column sums
+    if (tid == 0) commit(bar);
     wait_mma();
-    if (!ok) break;
   }
 
   fence_before();
