@@ -133,3 +133,42 @@ def test_reference_worker_equals_the_oracle_port():
     assert np.array_equal(out[mode][0], t[0]), mode
     assert out[mode][1] == (int(st[0][0]), int(st[0][1])), mode
   assert secs > 0
+
+
+@pytest.mark.timeout(300)
+def test_reference_ga_timing_runs_the_same_ga_as_the_oracle():
+  """The GA the CPU baseline times (the installed reference's GeneticAlgorithm.evolve with
+  its CPU strategies) and the oracle GA give the same best-fitness history on the 100-city
+  workload and on the Chapter-4 configuration."""
+  sys.path.insert(0, ROOT)
+  from baseline import reference_arm
+
+  if reference_arm.import_root() is None:
+    pytest.skip("the reference is not installed")
+  import bench
+  from tsp_gpu_clean_b200 import instances
+
+  for name in ("ga100", "chapter4"):
+    n, P, G, elite, post_init, seed, _ = bench.GA_WORKLOADS[name]
+    o = bench.ga_options(name)
+    ref = reference_arm.ga_gens_per_s(instances.uniform_instance(n, seed), P, elite, post_init, 2, o)
+    assert ref["value"] > 0
+    from oracle import distances as odist
+    from oracle import ga as oga
+
+    coords = instances.uniform_instance(n, seed)
+    cache = {}
+
+    def provider(k, coords=coords, cache=cache):
+      if k not in cache:
+        cache[k] = odist.candidate_list(k, coords=coords)
+      return cache[k]
+
+    cfg = oga.GAConfig(population_size=P, mutation_rate=o["rate"], nn_k=5, tournament_k=5,
+                       local_search=oga.LocalSearchSpec("best", 10, 20), post_init=post_init,
+                       elite_count=elite or None, local_search_stage=o["stage"], crossover=o["crossover"],
+                       mutation=o["mutation"], init=o["init"])
+    import numpy as np
+
+    res = oga.OracleGA(odist.euc2d_matrix(coords), provider, cfg, np.random.default_rng(42)).evolve(2, patience=10**9)
+    assert ref["history"] == [float(v) for v in res[3]["convergence_history"]], name
