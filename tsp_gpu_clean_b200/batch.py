@@ -765,6 +765,13 @@ class FusedBatchSolver:
     ev_end = torch.cuda.Event(enable_timing=True)
     ev_start.record()
     ctl_host = torch.empty((self.I, 4), dtype=torch.int32, pin_memory=True)
+    # each round's snapshot also carries both fitness buffers, so a paused run's fitness
+    # needs no further read; the host's answers go back through pinned buffers without a
+    # sync (the next round's snapshot is ordered after them)
+    fit_host = torch.empty((2, self.I, P), dtype=torch.float64, pin_memory=True)
+    ctl_up = torch.empty((self.I, 4), dtype=torch.int32, pin_memory=True)
+    he_up = torch.zeros((self.I, max(self.elite, 1)), dtype=torch.int32, pin_memory=True)
+    he_host = he_up.numpy()
     ready = torch.cuda.Event()
     host_elite_gens = np.zeros(self.I, dtype=np.int64)
     live = (native.TSPB_BATCH_RUN, native.TSPB_BATCH_PAUSED, native.TSPB_BATCH_RESUME)
@@ -787,20 +794,21 @@ class FusedBatchSolver:
         self.replays += 1
       rounds += 1
       ctl_host.copy_(self.ctl, non_blocking=True)
+      fit_host[0].copy_(self.fit[0], non_blocking=True)
+      fit_host[1].copy_(self.fit[1], non_blocking=True)
       ready.record()
       ready.synchronize()
       c = ctl_host.numpy()
       paused = np.nonzero(c[:, 1] == native.TSPB_BATCH_PAUSED)[0]
       if paused.size:
         parity = (c[paused, 0] + 1) & 1
-        fits = torch.stack(self.fit)[torch.from_numpy(parity).long().cuda(), torch.from_numpy(paused).long().cuda()]
-        rows = elite_rows(fits.cpu().numpy(), self.elite)  # pipeline_steps.py:163
-        he = self.host_elites.cpu().numpy()
-        he[paused] = rows
-        self.host_elites.copy_(torch.from_numpy(he))
+        fits = fit_host.numpy()[parity, paused]
+        he_host[paused] = elite_rows(fits, self.elite)  # pipeline_steps.py:163
+        self.host_elites.copy_(he_up, non_blocking=True)
         c = c.copy()
         c[paused, 1] = native.TSPB_BATCH_RESUME
-        self.ctl.copy_(torch.from_numpy(c))
+        ctl_up.numpy()[...] = c
+        self.ctl.copy_(ctl_up, non_blocking=True)
         host_elite_gens[paused] += 1
         chunk = max(1, chunk // 2)
       else:
