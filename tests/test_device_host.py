@@ -81,3 +81,35 @@ def test_check_free_logic_against_fake_allocator_counters(monkeypatch):
   device.check_free(1000, "no allocator yet")
   with pytest.raises(VRAMInsufficientError):
     device.check_free(1001, "no allocator yet, too large")
+
+
+def test_checked_budget_covers_the_allocations_inside_it(monkeypatch):
+  """One check for a batch's total: the check_free calls inside the block draw on it without
+  querying the allocator; beyond it, or after the block, they query again."""
+  import pytest
+  import torch
+
+  from tsp_gpu_clean_b200 import device
+  from tsp_gpu_clean_b200.errors import VRAMInsufficientError
+
+  calls = {"stats": 0}
+
+  def fake_stats(*a):
+    calls["stats"] += 1
+    return {"reserved_bytes": {"all": {"current": 0}}, "allocated_bytes": {"all": {"current": 0}}}
+
+  monkeypatch.setattr(torch.cuda, "memory_stats_as_nested_dict", fake_stats)
+  monkeypatch.setattr(torch.cuda, "mem_get_info", lambda *a: (1000, 10**6))
+  with device.checked_budget(900, "batch"):
+    assert calls["stats"] == 1
+    device.check_free(600, "first matrix")
+    device.check_free(300, "second matrix")
+    assert calls["stats"] == 1  # drawn from the checked total
+    device.check_free(50, "beyond the total")
+    assert calls["stats"] == 2
+  device.check_free(10, "after the block")
+  assert calls["stats"] == 3
+  with pytest.raises(VRAMInsufficientError):
+    with device.checked_budget(2000, "too large"):
+      pass
+  assert device._CHECKED[0] == 0

@@ -52,7 +52,8 @@ import numpy as np
 
 from . import native
 from .autotune import BatchAutotuner
-from .device import candidate_list, check_packed, operands_for, ptr, require_gpu, stream_handle, torch
+from .device import (candidate_list, check_packed, checked_budget, operands_for, ptr, require_gpu, stream_handle, torch,
+                     upload_coordinates)
 from .fused import LocalSearchConfig, draw_generation_tape
 from .problem import resolve_rng
 from .strategies.initialization import draw_row_seeds
@@ -679,38 +680,54 @@ class FusedBatchSolver:
     # every generator's next draws are its generations' tape: a few runs draw it on the
     # host, in a thread (the C++ draw releases the GIL) while the operands are built here
     tape_job = self._start_host_tapes(rngs, ns)
-    for i, (ctx, n, rng) in enumerate(zip(contexts, ns, rngs)):
-      if self.init == "nn":
-        nn_tables.append(np.ascontiguousarray(candidate_list(ctx, self.nn_k), dtype=np.int32))
-      t0 = time.perf_counter()
-      ops = operands_for(ctx)
-      dist, stride, coords = ops.distance_args(n, self.max_matrix_dimension)
-      tabs = ops.candidates(k, candidate_list(ctx, k), n, self.max_matrix_dimension)
-      if tabs.packed_words is None:
-        raise ValueError(f"instance {i}: k-NN table does not pack into 16-bit ids and distances")
-      all_tabs.append(tabs)
-      t_ops += time.perf_counter() - t0
-      self._keep.append((dist, coords, tabs))
-      inst = h_inst[i]
-      inst.n = n
-      inst.k = tabs.k
-      inst.pop_offset = self.pop_offsets[i]
-      inst.node_offset = int(prefix[i])
-      inst.dist = dist.data_ptr() if dist is not None else None
-      inst.dist_stride = int(stride)
-      has_xy = ops._euc2d_on_device() or coords is not None
-      xy = coords if coords is not None else (ops.coords() if has_xy else None)
-      inst.coords = xy.data_ptr() if xy is not None else None
-      rebuildable.append(xy is not None)
-      self._keep.append(xy)
-      inst.cand_packed = tabs.packed_words.data_ptr()
-      inst.rev_off = tabs.rev_off.data_ptr()
-      inst.rev_idx = tabs.rev_idx.data_ptr()
-      pat = patience[i] if isinstance(patience, (list, tuple, np.ndarray)) else patience
-      inst.patience = int(pat) if pat is not None else int(2 * math.sqrt(n))
-      opt = optimal_cost[i] if isinstance(optimal_cost, (list, tuple, np.ndarray)) else optimal_cost
-      inst.optimal = float(opt) if opt is not None and opt > 0 else 0.0
-      coords_flags.append(dist is None)
+    t0 = time.perf_counter()
+    # all coordinates in one upload, and one free-memory check for all the matrices to build
+    all_ops = [operands_for(ctx) for ctx in contexts]
+    upload_coordinates([o for o in all_ops if o._euc2d_on_device()])
+    need, seen = 0, set()
+    for o, n in zip(all_ops, ns):
+      key = id(o._shared) if o._shared is not None else id(o)  # contexts of one Problem share a matrix
+      if key not in seen and not o.use_coords(n, self.max_matrix_dimension) and not o.has_dist():
+        need += n * n * 4
+      seen.add(key)
+    budget = checked_budget(need, f"distance matrices of {self.I} instances")
+    budget.__enter__()
+    t_ops += time.perf_counter() - t0
+    try:
+      for i, (ctx, n, rng) in enumerate(zip(contexts, ns, rngs)):
+        if self.init == "nn":
+          nn_tables.append(np.ascontiguousarray(candidate_list(ctx, self.nn_k), dtype=np.int32))
+        t0 = time.perf_counter()
+        ops = operands_for(ctx)
+        dist, stride, coords = ops.distance_args(n, self.max_matrix_dimension)
+        tabs = ops.candidates(k, candidate_list(ctx, k), n, self.max_matrix_dimension)
+        if tabs.packed_words is None:
+          raise ValueError(f"instance {i}: k-NN table does not pack into 16-bit ids and distances")
+        all_tabs.append(tabs)
+        t_ops += time.perf_counter() - t0
+        self._keep.append((dist, coords, tabs))
+        inst = h_inst[i]
+        inst.n = n
+        inst.k = tabs.k
+        inst.pop_offset = self.pop_offsets[i]
+        inst.node_offset = int(prefix[i])
+        inst.dist = dist.data_ptr() if dist is not None else None
+        inst.dist_stride = int(stride)
+        has_xy = ops._euc2d_on_device() or coords is not None
+        xy = coords if coords is not None else (ops.coords() if has_xy else None)
+        inst.coords = xy.data_ptr() if xy is not None else None
+        rebuildable.append(xy is not None)
+        self._keep.append(xy)
+        inst.cand_packed = tabs.packed_words.data_ptr()
+        inst.rev_off = tabs.rev_off.data_ptr()
+        inst.rev_idx = tabs.rev_idx.data_ptr()
+        pat = patience[i] if isinstance(patience, (list, tuple, np.ndarray)) else patience
+        inst.patience = int(pat) if pat is not None else int(2 * math.sqrt(n))
+        opt = optimal_cost[i] if isinstance(optimal_cost, (list, tuple, np.ndarray)) else optimal_cost
+        inst.optimal = float(opt) if opt is not None and opt > 0 else 0.0
+        coords_flags.append(dist is None)
+    finally:
+      budget.__exit__(None, None, None)
     t0 = time.perf_counter()
     check_packed(all_tabs)  # every instance's pack-overflow flag in one sync
     bad = [i for i, t in enumerate(all_tabs) if t.packed is None]

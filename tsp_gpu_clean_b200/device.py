@@ -6,6 +6,7 @@ computation on the path runs in libtspb.so kernels.
 
 from __future__ import annotations
 
+import contextlib
 import ctypes
 import weakref
 from typing import Any
@@ -95,10 +96,30 @@ def auto_threads(num_tours: int) -> int:
   return 128
 
 
+# bytes that a caller has already checked for the allocations that follow (checked_budget)
+_CHECKED = [0]
+
+
+@contextlib.contextmanager
+def checked_budget(required_bytes: int, what: str):
+  """Check once for the total of many allocations (a batch's distance matrices); the
+  check_free calls inside the block draw on that total instead of querying each time."""
+  check_free(required_bytes, what)
+  prev = _CHECKED[0]
+  _CHECKED[0] = prev + int(required_bytes)
+  try:
+    yield
+  finally:
+    _CHECKED[0] = prev
+
+
 def check_free(required_bytes: int, what: str) -> None:
   """Raise VRAMInsufficientError before an allocation that cannot succeed. Memory that
   torch's caching allocator already holds unused is counted first (host-side counters);
   the driver is asked for free memory only when that does not cover the request."""
+  if _CHECKED[0] >= required_bytes:
+    _CHECKED[0] -= required_bytes
+    return
   # the nested form skips the flattening that torch.cuda.memory_reserved/allocated do on
   # every call (tens of microseconds each, paid per instance of a large batch)
   stats = torch.cuda.memory_stats_as_nested_dict()
@@ -235,23 +256,37 @@ class DeviceOperands:
       raise RuntimeError("the problem context of these device operands no longer exists")
     return ctx
 
+  def host_coords(self) -> np.ndarray:
+    """The context's (n, 2) float64 coordinates, checked for the device's EUC_2D rebuild."""
+    c = self.context.get_cpu_coordinates()
+    if c is None:
+      raise ValueError("problem has no coordinates for on-the-fly distances")
+    c = np.ascontiguousarray(c, dtype=np.float64)
+    if c.ndim != 2 or c.shape[1] != 2:
+      raise ValueError("on-the-fly distances need (n, 2) EUC_2D coordinates")
+    span = float(np.abs(c).max()) if c.size else 0.0
+    if span * 2.0 * 1.5 >= MAX_DISTANCE:
+      raise ValueError("coordinates too large for exact int32 gains")
+    return c
+
+  def has_coords(self) -> bool:
+    return self._coords is not None or (self._shared is not None and "coords" in self._shared)
+
+  def has_dist(self) -> bool:
+    return self._dist is not None or (self._shared is not None and "dist" in self._shared)
+
+  def set_coords(self, t) -> None:
+    """Adopt device coordinates uploaded by the caller (a view of a batch upload)."""
+    self._coords = t
+    self.h2d_bytes += t.numel() * 8
+    if self._shared is not None:
+      self._shared["coords"] = t
+
   def coords(self):
     if self._coords is None and self._shared is not None:
       self._coords = self._shared.get("coords")
     if self._coords is None:
-      c = self.context.get_cpu_coordinates()
-      if c is None:
-        raise ValueError("problem has no coordinates for on-the-fly distances")
-      c = np.ascontiguousarray(c, dtype=np.float64)
-      if c.ndim != 2 or c.shape[1] != 2:
-        raise ValueError("on-the-fly distances need (n, 2) EUC_2D coordinates")
-      span = float(np.abs(c).max()) if c.size else 0.0
-      if span * 2.0 * 1.5 >= MAX_DISTANCE:
-        raise ValueError("coordinates too large for exact int32 gains")
-      self._coords = device_tensor(c, torch.float64)
-      self.h2d_bytes += self._coords.numel() * 8
-      if self._shared is not None:
-        self._shared["coords"] = self._coords
+      self.set_coords(device_tensor(self.host_coords(), torch.float64))
     return self._coords
 
   def dist(self):
@@ -384,6 +419,35 @@ class DeviceOperands:
     tables = CandidateTables(d_cand, d_cd, rev_off, rev_idx, packed, overflow)
     self._cand[key] = (table, tables)
     return tables
+
+
+def upload_coordinates(ops_list) -> None:
+  """One H2D copy for the coordinates of every operand set in `ops_list` that has none on
+  the device yet; each adopts a view of the upload (offsets of 16 bytes per city, so every
+  view stays aligned for the kernels' double2 loads). Operand sets that share a problem's
+  data are uploaded once."""
+  todo, seen = [], set()
+  for o in ops_list:
+    key = id(o._shared) if o._shared is not None else id(o)
+    if o.has_coords() or key in seen:
+      continue
+    seen.add(key)
+    todo.append(o)
+  if not todo:
+    return
+  hosts = [o.host_coords() for o in todo]
+  total = sum(len(h) for h in hosts)
+  buf = torch.empty((max(total, 1), 2), dtype=torch.float64, pin_memory=True)
+  arr = buf.numpy()
+  off = 0
+  for h in hosts:
+    arr[off:off + len(h)] = h
+    off += len(h)
+  dev = buf.to("cuda", non_blocking=True)  # the caching host allocator holds buf until the copy has run
+  off = 0
+  for o, h in zip(todo, hosts):
+    o.set_coords(dev[off:off + len(h)])
+    off += len(h)
 
 
 def _host_knn_rows(context, rows: np.ndarray, k_eff: int, dist=None) -> np.ndarray:
