@@ -763,7 +763,7 @@ class FusedBatchSolver:
     self._tune()
     torch.cuda.synchronize()
     t_tuned = time.perf_counter()
-    self.kernel_launches = 1
+    self.kernel_launches = 2  # tspb_batch_init: the rows' fitness, then the initial best
     initial_best = self.best_cost.cpu().numpy().copy()
     if self.post_init and G > 0:
       for b in self.buckets:

@@ -50,21 +50,27 @@ __device__ __forceinline__ int phase_state(int phase) {
   return phase == TSPB_BATCH_PHASE_RESUME ? TSPB_BATCH_RESUME : TSPB_BATCH_RUN;
 }
 
-// CTA per instance: fitness of every row of pop[parity]; optionally the initial best.
-__global__ void __launch_bounds__(256) batch_init_kernel(const tspb_batch B, int parity, int set_best) {
+// Warp per row of pop[parity], INIT_ROWS rows per CTA, blockIdx.x the instance: every
+// row's fitness. One CTA per instance would walk P tours with 8 warps, which for one run
+// of 512 tours of 2000 cities took milliseconds on a single SM.
+constexpr int INIT_ROWS = 8;
+__global__ void __launch_bounds__(32 * INIT_ROWS) batch_fitness_kernel(const tspb_batch B, int parity) {
+  const int i = blockIdx.x, P = B.P;
+  const int r = blockIdx.y * INIT_ROWS + (threadIdx.x >> 5);
+  if (r >= P) return;  // warp-uniform
+  const tspb_batch_instance I = B.inst[i];
+  const double f = warp_tour_length(pop_buf(B, parity) + I.pop_offset + (long long)r * I.n, I.n, inst_ds(I));
+  if ((threadIdx.x & 31) == 0) fit_buf(B, parity)[(long long)i * P + r] = f;
+}
+
+// CTA per instance, after batch_fitness_kernel: the initial best (first minimum), the
+// history's first entry and the control block.
+__global__ void __launch_bounds__(256) batch_init_kernel(const tspb_batch B, int parity) {
   const int i = blockIdx.x;
   const tspb_batch_instance I = B.inst[i];
-  const DistSrc ds = inst_ds(I);
   const int P = B.P, n = I.n;
   const int32_t* pop = pop_buf(B, parity) + I.pop_offset;
   double* fit = fit_buf(B, parity) + (long long)i * P;
-  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int r = warp; r < P; r += nw) {
-    const double f = warp_tour_length(pop + (long long)r * n, n, ds);
-    if ((threadIdx.x & 31) == 0) fit[r] = f;
-  }
-  if (!set_best) return;
-  __syncthreads();
   __shared__ int best_row;
   if (threadIdx.x == 0) {
     int b = 0;
@@ -647,7 +653,12 @@ static bool tape_ok(const tspb_batch* b) {
 extern "C" int tspb_batch_init(const tspb_batch* b, int32_t parity, int32_t set_best, void* stream) {
   if (!batch_ok(b) || (parity != 0 && parity != 1)) return TSPB_ERR_ARG;
   if (b->num_instances == 0) return TSPB_OK;
-  batch_init_kernel<<<b->num_instances, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(*b, parity, set_best);
+  const int row_blocks = (b->P + INIT_ROWS - 1) / INIT_ROWS;
+  if (row_blocks > 65535) return TSPB_ERR_UNSUPPORTED;  // row blocks index grid.y
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const dim3 grid((unsigned)b->num_instances, (unsigned)row_blocks);
+  batch_fitness_kernel<<<grid, 32 * INIT_ROWS, 0, st>>>(*b, parity);
+  if (set_best) batch_init_kernel<<<b->num_instances, 256, 0, st>>>(*b, parity);
   return tspb_launch_status();
 }
 
