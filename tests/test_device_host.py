@@ -112,4 +112,4 @@ def test_checked_budget_covers_the_allocations_inside_it(monkeypatch):
   with pytest.raises(VRAMInsufficientError):
     with device.checked_budget(2000, "too large"):
       pass
-  assert device._CHECKED[0] == 0
+  assert device._checked() == 0

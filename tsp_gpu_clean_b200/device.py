@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import contextlib
 import ctypes
+import threading
 import weakref
 from typing import Any
 
@@ -96,29 +97,34 @@ def auto_threads(num_tours: int) -> int:
   return 128
 
 
-# bytes that a caller has already checked for the allocations that follow (checked_budget)
-_CHECKED = [0]
+# bytes that this thread has already checked for the allocations that follow (checked_budget)
+_CHECKED = threading.local()
+
+
+def _checked() -> int:
+  return getattr(_CHECKED, "bytes", 0)
 
 
 @contextlib.contextmanager
 def checked_budget(required_bytes: int, what: str):
   """Check once for the total of many allocations (a batch's distance matrices); the
-  check_free calls inside the block draw on that total instead of querying each time."""
+  check_free calls inside the block, on the same thread, draw on that total instead of
+  querying each time."""
   check_free(required_bytes, what)
-  prev = _CHECKED[0]
-  _CHECKED[0] = prev + int(required_bytes)
+  prev = _checked()
+  _CHECKED.bytes = prev + int(required_bytes)
   try:
     yield
   finally:
-    _CHECKED[0] = prev
+    _CHECKED.bytes = prev
 
 
 def check_free(required_bytes: int, what: str) -> None:
   """Raise VRAMInsufficientError before an allocation that cannot succeed. Memory that
   torch's caching allocator already holds unused is counted first (host-side counters);
   the driver is asked for free memory only when that does not cover the request."""
-  if _CHECKED[0] >= required_bytes:
-    _CHECKED[0] -= required_bytes
+  if _checked() >= required_bytes:
+    _CHECKED.bytes = _checked() - required_bytes
     return
   # the nested form skips the flattening that torch.cuda.memory_reserved/allocated do on
   # every call (tens of microseconds each, paid per instance of a large batch)
